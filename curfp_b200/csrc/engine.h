@@ -1,0 +1,95 @@
+// engine.h — the primitive operations every RFP routine is planned onto, and
+// the recursive dense-triangular algorithms (potrf / trsm / trmm / trtri /
+// lauum) written against them.
+//
+// The planner (plan.cpp) only manipulates views and calls an Exec.  The
+// product library binds it to the CUDA executor (exec_cuda.cu), which launches
+// the sm_100a kernels on the handle's stream.  The host-logic tests bind the
+// same planner source to a CPU executor so that view arithmetic, recursion
+// splits and masks are checked without a GPU.
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+#include "rfp.h"
+
+namespace rfp {
+
+// C(m x n) := alpha * (A(m x k) B(k x n) + A2(m x k2) B2(k2 x n)) + beta * C
+// beta == 0 means C is not read.  k2 == 0 disables the second product.
+struct GemmProb {
+  View A, B, A2, B2, C;
+  int m, n, k, k2;
+  float alpha, beta;
+  int c_lower;  // write only C(i,j) with i >= j (tiles above the diagonal skipped)
+  int a_lower;  // treat A(i,kk) as 0 for kk > i (product 1 only)
+  int inplace;  // C aliases B: the executor must read all of B's column block
+                // before writing it (the planner guarantees m <= inplace_rows())
+  int math;     // 0 = FP32 FMA, 1 = split-BF16 tensor cores (engine may ignore
+                // for small problems)
+};
+
+constexpr int kMaxBatch = 4;
+
+// Block sizes of the recursive algorithms.
+constexpr int kPotrfTile = 64;   // diagonal Cholesky tiles
+constexpr int kTrsmLeaf = 64;    // TRSM diagonal blocks (inverted, then multiplied)
+constexpr int kTriTile = 64;     // trtri / lauum tiles
+constexpr int kTrmmLeaf = 64;    // TRMM leaves (masked in-place multiply)
+
+class Exec {
+ public:
+  virtual ~Exec() {}
+  // Independent problems, executed as one launch where possible.
+  virtual int gemm(const GemmProb* p, int count) = 0;
+  // In-place Cholesky of the lower triangle of L (n <= kPotrfTile).  On the
+  // first non-positive (or NaN) pivot at local column j the device info word
+  // becomes min(info, info_base + j + 1) and the tile stops.
+  virtual int potrf_tile(View L, int n, int info_base) = 0;
+  // Inverses of the diagonal nb x nb blocks of lower L (n x n): block b is
+  // written to W + b*nb*nb, column-major with ld nb, zeros above the diagonal.
+  virtual int trtri_blocks(View L, int n, int nb, float* W) = 0;
+  // In-place inverse of lower L (n <= kTriTile).
+  virtual int trtri_tile(View L, int n) = 0;
+  // In-place L := L^T L (lower triangle; n <= kTriTile).
+  virtual int lauum_tile(View L, int n) = 0;
+  // Scratch of at least nfloats, valid until the next workspace() call.
+  virtual float* workspace(size_t nfloats) = 0;
+  // Largest m of an in-place GEMM.
+  virtual int inplace_rows() const = 0;
+};
+
+namespace plan {
+
+// L X = alpha B (L n x n lower, non-unit; B n x m), X overwrites B.
+int trsm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math = 0);
+// op(T) X = alpha B (left) or X op(T) = alpha B (right); B is rows x cols.
+int trsm(Exec& ex, int left, int lower, int trans, View T, View B, int rows,
+         int cols, float alpha, int math = 0);
+// B := alpha L B (L lower n x n, B n x m).
+int trmm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math = 0);
+// B := alpha op(T) B (left) or alpha B op(T) (right).
+int trmm(Exec& ex, int left, int lower, int trans, View T, View B, int rows,
+         int cols, float alpha, int math = 0);
+// In-place lower Cholesky; info_base is added to local failure columns.
+int potrf_lower(Exec& ex, View A, int n, int info_base, int math = 0);
+// In-place inverse of a lower triangular matrix.
+int trtri_lower(Exec& ex, View L, int n, int math = 0);
+// In-place L := L^T L (lower part).
+int lauum_lower(Exec& ex, View L, int n, int math = 0);
+
+// RFP routines (logical level, all 8 variants through rfp::geometry).
+// transr: 0 = N, 1 = T; lower: 1 = L, 0 = U; trans: 0 = N, 1 = T.
+int ssfrk(Exec& ex, int transr, int lower, int trans, int n, int k,
+          float alpha, const float* A, int lda, float beta, float* C,
+          int math = 0);
+int ssfr2k(Exec& ex, int transr, int lower, int trans, int n, int k,
+           float alpha, const float* A, int lda, const float* B, int ldb,
+           float beta, float* C);
+int spftrf(Exec& ex, int transr, int lower, int n, float* A, int math = 0);
+int spftrs(Exec& ex, int transr, int lower, int n, int nrhs, const float* A,
+           float* B, int ldb);
+int spftri(Exec& ex, int transr, int lower, int n, float* A);
+
+}  // namespace plan
+}  // namespace rfp

@@ -1,0 +1,117 @@
+// exec_cuda.cu — CUDA executor: turns planner primitives into sm_100a kernel
+// launches on the handle's stream.
+#include <climits>
+#include <cstdint>
+
+#include "context.h"
+#include "k_gemm.cuh"
+#include "k_tile.cuh"
+
+namespace rfp {
+
+void* grow_buffer(curfpContext* ctx, void** buf, size_t* cur, size_t bytes) {
+  if (*buf && *cur >= bytes) return *buf;
+  if (*buf) {
+    cudaFreeAsync(*buf, ctx->stream);
+    *buf = nullptr;
+    *cur = 0;
+  }
+  size_t want = bytes < 256 ? 256 : bytes;
+  void* p = nullptr;
+  if (cudaMallocAsync(&p, want, ctx->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  *buf = p;
+  *cur = want;
+  return p;
+}
+
+float* CudaExec::workspace(size_t nfloats) {
+  return static_cast<float*>(
+      grow_buffer(ctx_, &ctx_->ws, &ctx_->ws_bytes, nfloats * sizeof(float)));
+}
+
+namespace {
+
+template <int BM, int BN>
+int launch_gemm(const GemmProb* p, int count, const int* abort_flag,
+                cudaStream_t st) {
+  kgemm::Batch b{};
+  int tiles = 0, cnt = 0;
+  for (int i = 0; i < count; ++i) {
+    const GemmProb& g = p[i];
+    if (g.m <= 0 || g.n <= 0) continue;
+    kgemm::Prob& q = b.p[cnt];
+    q.A = g.A.p; q.a_rs = g.A.rs; q.a_cs = g.A.cs;
+    q.B = g.B.p; q.b_rs = g.B.rs; q.b_cs = g.B.cs;
+    q.A2 = g.A2.p; q.a2_rs = g.A2.rs; q.a2_cs = g.A2.cs;
+    q.B2 = g.B2.p; q.b2_rs = g.B2.rs; q.b2_cs = g.B2.cs;
+    q.C = g.C.p; q.c_rs = g.C.rs; q.c_cs = g.C.cs;
+    q.m = g.m; q.n = g.n; q.k = g.k; q.k2 = g.k2;
+    q.alpha = g.alpha; q.beta = g.beta;
+    q.c_lower = g.c_lower; q.a_lower = g.a_lower;
+    q.tiles_m = (g.m + BM - 1) / BM;
+    q.tiles_n = (g.n + BN - 1) / BN;
+    if (g.inplace && q.tiles_m != 1) return 3;  // planner contract
+    if (g.c_lower && (q.tiles_m != q.tiles_n || BM != BN || g.m != g.n))
+      return 3;
+    q.tile_begin = tiles;
+    tiles += g.c_lower ? q.tiles_m * (q.tiles_m + 1) / 2 : q.tiles_m * q.tiles_n;
+    ++cnt;
+  }
+  if (cnt == 0) return 0;
+  b.count = cnt;
+  b.total_tiles = tiles;
+  b.abort_flag = abort_flag;
+  kgemm::sgemm_batch<BM, BN><<<tiles, kgemm::kThreads, 0, st>>>(b);
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+}  // namespace
+
+int CudaExec::gemm(const GemmProb* p, int count) {
+  if (count <= 0) return 0;
+  if (count > kMaxBatch) return 3;
+  // Tile choice: 128 x 128 when it fills the machine, else 64 x 64.
+  int64_t t128 = 0;
+  int maxm = 0;
+  for (int i = 0; i < count; ++i) {
+    int64_t tm = (p[i].m + 127) / 128, tn = (p[i].n + 127) / 128;
+    t128 += p[i].c_lower ? tm * (tm + 1) / 2 : tm * tn;
+    if (p[i].inplace && p[i].m > maxm) maxm = p[i].m;
+  }
+  if (t128 >= 2 * 148 && maxm == 0)
+    return launch_gemm<128, 128>(p, count, abort_, ctx_->stream);
+  return launch_gemm<64, 64>(p, count, abort_, ctx_->stream);
+}
+
+int CudaExec::potrf_tile(View L, int n, int info_base) {
+  if (n <= 0) return 0;
+  ktile::potrf_tile<<<1, 256, 0, ctx_->stream>>>(L, n, info_base, ctx_->d_info);
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+int CudaExec::trtri_blocks(View L, int n, int nb, float* W) {
+  if (n <= 0) return 0;
+  if (nb != ktile::T) return 3;
+  int nblk = (n + nb - 1) / nb;
+  ktile::trtri_blocks<<<nblk, ktile::T, 0, ctx_->stream>>>(L, n, W, abort_);
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+int CudaExec::trtri_tile(View L, int n) {
+  if (n <= 0) return 0;
+  if (n > ktile::T) return 3;
+  ktile::trtri_blocks<<<1, ktile::T, 0, ctx_->stream>>>(L, n, nullptr, abort_);
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+int CudaExec::lauum_tile(View L, int n) {
+  if (n <= 0) return 0;
+  if (n > ktile::T) return 3;
+  ktile::lauum_tile<<<1, 256, 0, ctx_->stream>>>(L, n);
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+}  // namespace rfp

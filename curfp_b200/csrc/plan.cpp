@@ -1,0 +1,288 @@
+// plan.cpp — recursive blocked algorithms over strided views.
+//
+// All routines reduce to one canonical form (left side, lower triangular, no
+// transpose) by view transposition and index reversal; see rfp.h.  The
+// RFP-level routines split the logical matrix at n1 exactly as the reference
+// does (T1 / S / T2: src/curfp_spftrf.cpp:254-282, src/curfp_spftrs.cpp:257-299,
+// src/curfp_ssfrk.cpp:193-209), and every dense sub-problem is then solved
+// recursively on the views.
+#include "engine.h"
+
+namespace rfp {
+namespace plan {
+
+namespace {
+
+// Split n into n1 + n2 with n1 a multiple of `blk`, n1 ~ n/2.
+inline int split(int n, int blk) {
+  int half = (n + 1) / 2;
+  int n1 = ((half + blk - 1) / blk) * blk;
+  if (n1 >= n) n1 = n - blk;  // only reached for n <= 2*blk
+  if (n1 <= 0) n1 = n / 2;
+  return n1;
+}
+
+inline GemmProb gemm_prob(View A, View B, View C, int m, int n, int k,
+                          float alpha, float beta, int math) {
+  GemmProb p{};
+  p.A = A; p.B = B; p.C = C;
+  p.A2 = A; p.B2 = B;
+  p.m = m; p.n = n; p.k = k; p.k2 = 0;
+  p.alpha = alpha; p.beta = beta;
+  p.c_lower = 0; p.a_lower = 0; p.inplace = 0;
+  p.math = math;
+  return p;
+}
+
+int trsm_rec(Exec& ex, View L, int n, View B, int m, float alpha,
+             const float* W, int blk0, int math) {
+  if (n <= 0 || m <= 0) return 0;
+  if (n <= kTrsmLeaf) {
+    View Wv{const_cast<float*>(W) + (int64_t)blk0 * kTrsmLeaf * kTrsmLeaf, 1,
+            kTrsmLeaf};
+    GemmProb p = gemm_prob(Wv, B, B, n, m, n, alpha, 0.0f, 0);
+    p.inplace = 1;
+    return ex.gemm(&p, 1);
+  }
+  int n1 = split(n, kTrsmLeaf), n2 = n - n1;
+  int rc = trsm_rec(ex, L, n1, B, m, alpha, W, blk0, math);
+  if (rc) return rc;
+  GemmProb p = gemm_prob(sub(L, n1, 0), B, sub(B, n1, 0), n2, m, n1, -1.0f,
+                         alpha, math);
+  if ((rc = ex.gemm(&p, 1))) return rc;
+  return trsm_rec(ex, sub(L, n1, n1), n2, sub(B, n1, 0), m, 1.0f, W,
+                  blk0 + n1 / kTrsmLeaf, math);
+}
+
+}  // namespace
+
+int trsm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math) {
+  if (n <= 0 || m <= 0) return 0;
+  int nblk = (n + kTrsmLeaf - 1) / kTrsmLeaf;
+  float* W = ex.workspace((size_t)nblk * kTrsmLeaf * kTrsmLeaf);
+  if (!W) return 2;
+  int rc = ex.trtri_blocks(L, n, kTrsmLeaf, W);
+  if (rc) return rc;
+  return trsm_rec(ex, L, n, B, m, alpha, W, 0, math);
+}
+
+int trsm(Exec& ex, int left, int lower, int trans, View T, View B, int rows,
+         int cols, float alpha, int math) {
+  if (!left) {  // X op(T) = B  <=>  op(T)^T X^T = B^T
+    B = tr(B);
+    int t = rows; rows = cols; cols = t;
+    trans = !trans;
+  }
+  View E = trans ? tr(T) : T;
+  int e_lower = lower ^ trans;
+  if (e_lower) return trsm_lln(ex, E, rows, B, cols, alpha, math);
+  return trsm_lln(ex, rev(E, rows, rows), rows, rev_rows(B, rows), cols,
+                  alpha, math);
+}
+
+int trmm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math) {
+  if (n <= 0 || m <= 0) return 0;
+  int leaf = kTrmmLeaf < ex.inplace_rows() ? kTrmmLeaf : ex.inplace_rows();
+  if (n <= leaf) {
+    GemmProb p = gemm_prob(L, B, B, n, m, n, alpha, 0.0f, 0);
+    p.a_lower = 1;
+    p.inplace = 1;
+    return ex.gemm(&p, 1);
+  }
+  int n1 = split(n, leaf), n2 = n - n1;
+  int rc = trmm_lln(ex, sub(L, n1, n1), n2, sub(B, n1, 0), m, alpha, math);
+  if (rc) return rc;
+  GemmProb p = gemm_prob(sub(L, n1, 0), B, sub(B, n1, 0), n2, m, n1, alpha,
+                         1.0f, math);
+  if ((rc = ex.gemm(&p, 1))) return rc;
+  return trmm_lln(ex, L, n1, B, m, alpha, math);
+}
+
+int trmm(Exec& ex, int left, int lower, int trans, View T, View B, int rows,
+         int cols, float alpha, int math) {
+  if (!left) {  // B op(T)  <=>  (op(T)^T B^T)^T
+    B = tr(B);
+    int t = rows; rows = cols; cols = t;
+    trans = !trans;
+  }
+  View E = trans ? tr(T) : T;
+  int e_lower = lower ^ trans;
+  if (e_lower) return trmm_lln(ex, E, rows, B, cols, alpha, math);
+  return trmm_lln(ex, rev(E, rows, rows), rows, rev_rows(B, rows), cols,
+                  alpha, math);
+}
+
+int potrf_lower(Exec& ex, View A, int n, int info_base, int math) {
+  if (n <= 0) return 0;
+  if (n <= kPotrfTile) return ex.potrf_tile(A, n, info_base);
+  int n1 = split(n, kPotrfTile), n2 = n - n1;
+  int rc = potrf_lower(ex, A, n1, info_base, math);
+  if (rc) return rc;
+  View A21 = sub(A, n1, 0);
+  // A21 := A21 L11^{-T}   <=>   L11 A21^T = A21^T
+  if ((rc = trsm_lln(ex, A, n1, tr(A21), n2, 1.0f, math))) return rc;
+  // A22 := A22 - A21 A21^T (lower)
+  GemmProb p = gemm_prob(A21, tr(A21), sub(A, n1, n1), n2, n2, n1, -1.0f, 1.0f,
+                         math);
+  p.c_lower = 1;
+  if ((rc = ex.gemm(&p, 1))) return rc;
+  return potrf_lower(ex, sub(A, n1, n1), n2, info_base + n1, math);
+}
+
+int trtri_lower(Exec& ex, View L, int n, int math) {
+  if (n <= 0) return 0;
+  if (n <= kTriTile) return ex.trtri_tile(L, n);
+  int n1 = split(n, kTriTile), n2 = n - n1;
+  int rc = trtri_lower(ex, L, n1, math);
+  if (rc) return rc;
+  if ((rc = trtri_lower(ex, sub(L, n1, n1), n2, math))) return rc;
+  View L21 = sub(L, n1, 0);
+  // L21 := -inv(L22) L21 inv(L11)
+  if ((rc = trmm(ex, 0, 1, 0, L, L21, n2, n1, 1.0f, math))) return rc;
+  return trmm(ex, 1, 1, 0, sub(L, n1, n1), L21, n2, n1, -1.0f, math);
+}
+
+int lauum_lower(Exec& ex, View L, int n, int math) {
+  if (n <= 0) return 0;
+  if (n <= kTriTile) return ex.lauum_tile(L, n);
+  int n1 = split(n, kTriTile), n2 = n - n1;
+  View L21 = sub(L, n1, 0);
+  int rc = lauum_lower(ex, L, n1, math);
+  if (rc) return rc;
+  GemmProb p = gemm_prob(tr(L21), L21, L, n1, n1, n2, 1.0f, 1.0f, math);
+  p.c_lower = 1;
+  if ((rc = ex.gemm(&p, 1))) return rc;
+  if ((rc = trmm(ex, 1, 1, 1, sub(L, n1, n1), L21, n2, n1, 1.0f, math)))
+    return rc;
+  return lauum_lower(ex, sub(L, n1, n1), n2, math);
+}
+
+// ---------------------------------------------------------------------------
+// RFP routines
+// ---------------------------------------------------------------------------
+
+int ssfrk(Exec& ex, int transr, int lower, int trans, int n, int k,
+          float alpha, const float* A, int lda, float beta, float* C,
+          int math) {
+  Geometry g = geometry(n, transr, lower);
+  // op(A) is n x k.  trans = N: A is n x k column-major; trans = T: A is
+  // k x n column-major and op(A) = A^T.
+  View opA = trans ? View{const_cast<float*>(A), lda, 1}
+                   : View{const_cast<float*>(A), 1, lda};
+  if (alpha == 0.0f) k = 0;  // C := beta*C; A is not read
+  View A1 = opA, A2 = sub(opA, g.n1, 0);
+  View C11 = block_view(C, g.b11), C21 = block_view(C, g.b21),
+       C22 = block_view(C, g.b22);
+  GemmProb p[3];
+  int cnt = 0;
+  if (g.n1 > 0) {
+    p[cnt] = gemm_prob(A1, tr(A1), C11, g.n1, g.n1, k, alpha, beta, math);
+    p[cnt++].c_lower = 1;
+  }
+  if (g.n1 > 0 && g.n2 > 0)
+    p[cnt++] = gemm_prob(A2, tr(A1), C21, g.n2, g.n1, k, alpha, beta, math);
+  if (g.n2 > 0) {
+    p[cnt] = gemm_prob(A2, tr(A2), C22, g.n2, g.n2, k, alpha, beta, math);
+    p[cnt++].c_lower = 1;
+  }
+  return ex.gemm(p, cnt);
+}
+
+int ssfr2k(Exec& ex, int transr, int lower, int trans, int n, int k,
+           float alpha, const float* A, int lda, const float* B, int ldb,
+           float beta, float* C) {
+  Geometry g = geometry(n, transr, lower);
+  View opA = trans ? View{const_cast<float*>(A), lda, 1}
+                   : View{const_cast<float*>(A), 1, lda};
+  View opB = trans ? View{const_cast<float*>(B), ldb, 1}
+                   : View{const_cast<float*>(B), 1, ldb};
+  if (alpha == 0.0f) k = 0;
+  View Ab[2] = {opA, sub(opA, g.n1, 0)};
+  View Bb[2] = {opB, sub(opB, g.n1, 0)};
+  View Cb[3] = {block_view(C, g.b11), block_view(C, g.b21),
+                block_view(C, g.b22)};
+  const int bi[3] = {0, 1, 1}, bj[3] = {0, 0, 1};
+  const int dm[3] = {g.n1, g.n2, g.n2}, dn[3] = {g.n1, g.n1, g.n2};
+  GemmProb p[3];
+  int cnt = 0;
+  for (int b = 0; b < 3; ++b) {
+    if (dm[b] <= 0 || dn[b] <= 0) continue;
+    GemmProb q = gemm_prob(Ab[bi[b]], tr(Bb[bj[b]]), Cb[b], dm[b], dn[b], k,
+                           alpha, beta, 0);
+    q.A2 = Bb[bi[b]];
+    q.B2 = tr(Ab[bj[b]]);
+    q.k2 = k;
+    q.c_lower = (b != 1);
+    p[cnt++] = q;
+  }
+  return ex.gemm(p, cnt);
+}
+
+int spftrf(Exec& ex, int transr, int lower, int n, float* A, int math) {
+  Geometry g = geometry(n, transr, lower);
+  View V11 = block_view(A, g.b11), V21 = block_view(A, g.b21),
+       V22 = block_view(A, g.b22);
+  int rc = potrf_lower(ex, V11, g.n1, 0, math);
+  if (rc) return rc;
+  if (g.n2 == 0) return 0;
+  if (g.n1 > 0) {
+    if ((rc = trsm_lln(ex, V11, g.n1, tr(V21), g.n2, 1.0f, math))) return rc;
+    GemmProb p = gemm_prob(V21, tr(V21), V22, g.n2, g.n2, g.n1, -1.0f, 1.0f,
+                           math);
+    p.c_lower = 1;
+    if ((rc = ex.gemm(&p, 1))) return rc;
+  }
+  return potrf_lower(ex, V22, g.n2, g.n1, math);
+}
+
+int spftrs(Exec& ex, int transr, int lower, int n, int nrhs, const float* A,
+           float* B, int ldb) {
+  Geometry g = geometry(n, transr, lower);
+  float* Af = const_cast<float*>(A);
+  View V11 = block_view(Af, g.b11), V21 = block_view(Af, g.b21),
+       V22 = block_view(Af, g.b22);
+  View B1{B, 1, ldb};
+  View B2 = sub(B1, g.n1, 0);
+  int rc;
+  // Forward: L Y = B.
+  if ((rc = trsm_lln(ex, V11, g.n1, B1, nrhs, 1.0f))) return rc;
+  if (g.n1 > 0 && g.n2 > 0) {
+    GemmProb p = gemm_prob(V21, B1, B2, g.n2, nrhs, g.n1, -1.0f, 1.0f, 0);
+    if ((rc = ex.gemm(&p, 1))) return rc;
+  }
+  if ((rc = trsm_lln(ex, V22, g.n2, B2, nrhs, 1.0f))) return rc;
+  // Backward: L^T X = Y.
+  if ((rc = trsm(ex, 1, 1, 1, V22, B2, g.n2, nrhs, 1.0f))) return rc;
+  if (g.n1 > 0 && g.n2 > 0) {
+    GemmProb p = gemm_prob(tr(V21), B2, B1, g.n1, nrhs, g.n2, -1.0f, 1.0f, 0);
+    if ((rc = ex.gemm(&p, 1))) return rc;
+  }
+  return trsm(ex, 1, 1, 1, V11, B1, g.n1, nrhs, 1.0f);
+}
+
+int spftri(Exec& ex, int transr, int lower, int n, float* A) {
+  Geometry g = geometry(n, transr, lower);
+  View V11 = block_view(A, g.b11), V21 = block_view(A, g.b21),
+       V22 = block_view(A, g.b22);
+  int rc;
+  // inv(L) = [M11 0; -M22 L21 M11  M22]
+  if ((rc = trtri_lower(ex, V11, g.n1))) return rc;
+  if ((rc = trtri_lower(ex, V22, g.n2))) return rc;
+  if (g.n1 > 0 && g.n2 > 0) {
+    if ((rc = trmm(ex, 0, 1, 0, V11, V21, g.n2, g.n1, 1.0f))) return rc;
+    if ((rc = trmm(ex, 1, 1, 0, V22, V21, g.n2, g.n1, -1.0f))) return rc;
+  }
+  // inv(A) = M^T M:  (11) = M11^T M11 + M21^T M21, (21) = M22^T M21,
+  //                  (22) = M22^T M22
+  if ((rc = lauum_lower(ex, V11, g.n1))) return rc;
+  if (g.n1 > 0 && g.n2 > 0) {
+    GemmProb p = gemm_prob(tr(V21), V21, V11, g.n1, g.n1, g.n2, 1.0f, 1.0f, 0);
+    p.c_lower = 1;
+    if ((rc = ex.gemm(&p, 1))) return rc;
+    if ((rc = trmm(ex, 1, 1, 1, V22, V21, g.n2, g.n1, 1.0f))) return rc;
+  }
+  return lauum_lower(ex, V22, g.n2);
+}
+
+}  // namespace plan
+}  // namespace rfp

@@ -1,0 +1,140 @@
+/*
+ * curfp.h — C ABI of the B200-native RFP (Rectangular Full Packed) library.
+ *
+ * Drop-in for the reference header include/curfp.h of andersx/curfp on the
+ * rank-k update + Cholesky + solve path.  Enum names, enum values, status
+ * codes, the opaque handle and every routine signature below are the ones the
+ * reference declares (cited per declaration), so code compiled against the
+ * reference header links against libcurfp_b200.so unchanged for these routines.
+ *
+ * Differences from the reference header:
+ *   - it includes <cuda_runtime.h> only (no cuBLAS / cuSOLVER headers): the
+ *     library has no cuBLAS/cuSOLVER dependency;
+ *   - routines outside the Cholesky path (slansf, spfcon, ssfmv, ssfmm, ssfr,
+ *     ssfr2 and the D-prefix twins) are not declared;
+ *   - a block of extension entry points at the end (add_to_diagonal and the
+ *     diagonal index map as device kernels, the split-BF16 precision form, and
+ *     the adjoint kernels of the differentiation form).  They have no C-level
+ *     counterpart in the reference; each comment names the reference Python
+ *     function it replaces where there is one.
+ *
+ * Conventions (same as the reference): all matrices are device pointers;
+ * alpha/beta/info are HOST pointers; dense operands are column-major with a
+ * leading dimension (cuBLAS convention) except strttf/stfttr, whose full
+ * matrix is row-major; every routine enqueues on the handle's stream.
+ */
+#ifndef CURFP_H
+#define CURFP_H
+
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes — reference include/curfp.h:14-20. */
+typedef enum {
+    CURFP_STATUS_SUCCESS          = 0,
+    CURFP_STATUS_NOT_INITIALIZED  = 1,
+    CURFP_STATUS_ALLOC_FAILED     = 2,
+    CURFP_STATUS_INVALID_VALUE    = 3,
+    CURFP_STATUS_EXECUTION_FAILED = 4
+} curfpStatus_t;
+
+/* Operation (TRANSR / TRANS) — reference include/curfp.h:25-28. */
+typedef enum {
+    CURFP_OP_N = 0,
+    CURFP_OP_T = 1
+} curfpOperation_t;
+
+/* Fill mode — reference include/curfp.h:33-36. */
+typedef enum {
+    CURFP_FILL_MODE_LOWER = 0,
+    CURFP_FILL_MODE_UPPER = 1
+} curfpFillMode_t;
+
+/* Opaque handle — reference include/curfp.h:58.  The context holds the
+ * stream, the device, a device-side info word and a grow-only workspace. */
+typedef struct curfpContext *curfpHandle_t;
+
+/* Handle management — reference include/curfp.h:63-66
+ * (src/curfp_handle.cpp:4-51). */
+curfpStatus_t curfpCreate(curfpHandle_t *handle);
+curfpStatus_t curfpDestroy(curfpHandle_t handle);
+curfpStatus_t curfpSetStream(curfpHandle_t handle, cudaStream_t stream);
+curfpStatus_t curfpGetStream(curfpHandle_t handle, cudaStream_t *stream);
+
+/* C := alpha*op(A)*op(A)^T + beta*C, C n x n symmetric in RFP.
+ * trans = N: A is n x k; trans = T: A is k x n (column-major, lda).
+ * Replaces reference include/curfp.h:79-91 (src/curfp_ssfrk.cpp:135-212). */
+curfpStatus_t curfpSsfrk(curfpHandle_t handle, curfpOperation_t transr,
+                         curfpFillMode_t uplo, curfpOperation_t trans,
+                         int n, int k, const float *alpha, const float *A,
+                         int lda, const float *beta, float *C);
+
+/* In-place RFP Cholesky: A = L*L^T (lower) or U^T*U (upper).  *info (host)
+ * = 0 on success, i > 0 when the leading minor of order i is not positive
+ * definite.  Replaces include/curfp.h:105-112 (src/curfp_spftrf.cpp:182-292). */
+curfpStatus_t curfpSpftrf(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, int n, float *A, int *info);
+
+/* Solve A*X = B with the RFP factor from curfpSpftrf; B is n x nrhs
+ * column-major (ldb), overwritten by X.
+ * Replaces include/curfp.h:123-132 (src/curfp_spftrs.cpp:215-302). */
+curfpStatus_t curfpSpftrs(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, int n, int nrhs,
+                          const float *A, float *B, int ldb);
+
+/* Full row-major n x n (lda >= n) triangle -> RFP.
+ * Replaces include/curfp.h:141-149 (src/curfp_strttf.cu:420-462). */
+curfpStatus_t curfpSstrttf(curfpHandle_t handle, curfpOperation_t transr,
+                           curfpFillMode_t uplo, int n, const float *A,
+                           int lda, float *arf);
+
+/* In-place inverse from the RFP Cholesky factor.
+ * Replaces include/curfp.h:180-186 (src/curfp_spftri.cu:159-388). */
+curfpStatus_t curfpSpftri(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, int n, float *arf);
+
+/* RFP -> triangle of a full row-major n x n (lda >= n); the other triangle is
+ * not written.  Replaces include/curfp.h:197-205 (src/curfp_stfttr.cu:134-175). */
+curfpStatus_t curfpSstfttr(curfpHandle_t handle, curfpOperation_t transr,
+                           curfpFillMode_t uplo, int n, const float *arf,
+                           float *A, int lda);
+
+/* C := alpha*(op(A)op(B)^T + op(B)op(A)^T) + beta*C in RFP.
+ * Replaces include/curfp.h:305-319 (src/curfp_ssfr2k.cpp:121-232). */
+curfpStatus_t curfpSsfr2k(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, curfpOperation_t trans,
+                          int n, int k, const float *alpha, const float *A,
+                          int lda, const float *B, int ldb, const float *beta,
+                          float *C);
+
+/* ===========================================================================
+ * Extension entry points (no C-level counterpart in the reference).
+ * ===========================================================================*/
+
+/* Diagonal of an RFP matrix: idx[i] = flat RFP offset of element (i,i), as
+ * int64 in device memory (n entries).  Replaces the Python function
+ * rfp_diag_indices, reference curfp/__init__.py:194-269 (same values). */
+curfpStatus_t curfpRfpDiagIndices(curfpHandle_t handle,
+                                  curfpOperation_t transr,
+                                  curfpFillMode_t uplo, int n, int64_t *idx);
+
+/* arf[(i,i)] += value for i < n: M := M + value*I in RFP, one kernel.
+ * Replaces the Python add_to_diagonal, reference curfp/__init__.py:272-296. */
+curfpStatus_t curfpSaddToDiagonal(curfpHandle_t handle,
+                                  curfpOperation_t transr,
+                                  curfpFillMode_t uplo, int n, float value,
+                                  float *arf);
+curfpStatus_t curfpDaddToDiagonal(curfpHandle_t handle,
+                                  curfpOperation_t transr,
+                                  curfpFillMode_t uplo, int n, double value,
+                                  double *arf);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CURFP_H */

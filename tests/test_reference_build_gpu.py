@@ -1,0 +1,92 @@
+"""Parity with the reference's own GPU build (oracle/_ref/libcurfp_ref.so,
+the unmodified reference sources on cuBLAS/cuSOLVER) on the same inputs.
+
+Bit-exact for strttf/stfttr/diag; for the floating-point routines the bounds
+are stated per quantity on O(1) data (cond ~ 45): ssfrk max-abs 1e-5, factor
+max-abs 1e-4, solution and inverse max-relative 1e-4 / 2e-4 -- the spread of
+two FP32 summation orders of the same algorithm (both results are compared
+with FP64 elsewhere)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import VARIANTS
+from helpers import REF_LIB, TR, UL, RefLib, dev, host
+
+pytestmark = pytest.mark.skipif(not REF_LIB.exists(),
+                                reason="reference build missing (make -C oracle ref)")
+
+
+@pytest.fixture(scope="module")
+def ref():
+    return RefLib()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 2, 3, 64, 65, 255, 256, 1023])
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+def test_pack_bit_exact_vs_reference(curfp, ref, n, tr, ul):
+    g = torch.Generator(device="cuda").manual_seed(n)
+    M = torch.randn(n, n, device="cuda", generator=g)
+    a_ref = torch.empty(n * (n + 1) // 2, device="cuda")
+    assert ref.strttf(tr, ul, n, M, n, a_ref) == 0
+    a_our = curfp.strttf(M, transr=TR[tr], uplo=UL[ul])
+    torch.cuda.synchronize()
+    assert torch.equal(a_our, a_ref)
+    D_ref = torch.zeros(n, n, device="cuda")
+    assert ref.stfttr(tr, ul, n, a_ref, D_ref, n) == 0
+    D_our = curfp.stfttr(a_ref, transr=TR[tr], uplo=UL[ul])
+    torch.cuda.synchronize()
+    assert torch.equal(D_our, D_ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,k", [(64, 32), (65, 32), (1000, 128), (1001, 128)])
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+def test_pipeline_vs_reference(curfp, ref, orc, n, k, tr, ul):
+    g = torch.Generator(device="cuda").manual_seed(n + 10 * tr + ul)
+    A = torch.randn(n, k, device="cuda", generator=g) / k ** 0.5
+    nt = n * (n + 1) // 2
+    C_ref = torch.empty(nt, device="cuda")
+    C_our = torch.empty(nt, device="cuda")
+    assert ref.ssfrk(tr, ul, 1, n, k, 1.0, A, k, 0.0, C_ref) == 0
+    curfp.ssfrk(A, C_our, transr=TR[tr], uplo=UL[ul])
+    torch.cuda.synchronize()
+    d = (C_our - C_ref).abs().max().item()
+    assert d <= 1e-5, d
+    curfp.add_to_diagonal(C_ref, 1.0, transr=TR[tr], uplo=UL[ul])
+    C_our.copy_(C_ref)
+    A0 = host(C_ref).astype(np.float64)
+    st, info = ref.spftrf(tr, ul, n, C_ref)
+    assert st == 0 and info == 0
+    assert curfp.spftrf(C_our, transr=TR[tr], uplo=UL[ul]) == 0
+    # factors agree to FP32 rounding (cond(A) ~ 45 here)
+    d = (C_our - C_ref).abs().max().item()
+    assert d <= 1e-4, d
+    B = torch.randn(64, n, device="cuda", generator=g)  # column-major n x 64
+    X_ref, X_our = B.clone(), B.clone()
+    assert ref.spftrs(tr, ul, n, 64, C_ref, X_ref, n) == 0
+    with curfp.Handle() as h:
+        curfp.spftrs_raw(h, tr, ul, n, 64, C_our, X_our, n)
+    torch.cuda.synchronize()
+    rel = ((X_our - X_ref).abs().max() / X_ref.abs().max()).item()
+    assert rel <= 1e-4, rel
+    I_ref, I_our = C_ref.clone(), C_our.clone()
+    assert ref.spftri(tr, ul, n, I_ref) == 0
+    curfp.spftri(I_our, transr=TR[tr], uplo=UL[ul])
+    torch.cuda.synchronize()
+    rel = ((I_our - I_ref).abs().max() / I_ref.abs().max()).item()
+    assert rel <= 2e-4, rel
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+@pytest.mark.parametrize("n,bad", [(200, 7), (200, 150)])
+def test_info_vs_reference(curfp, ref, orc, tr, ul, n, bad):
+    M = np.eye(n) * 2.0
+    M[bad - 1, bad - 1] = -3.0
+    arf = orc.strttf(tr, ul, n, M).astype(np.float32)
+    a1, a2 = dev(arf), dev(arf)
+    st, info_ref = ref.spftrf(tr, ul, n, a1)
+    assert st == 0
+    assert curfp.spftrf(a2, transr=TR[tr], uplo=UL[ul], check=False) == info_ref == bad
