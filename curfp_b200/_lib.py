@@ -35,6 +35,13 @@ SIGNATURES = {
     "curfpRfpDiagIndices": [_h, _i, _i, _i, _p],
     "curfpSaddToDiagonal": [_h, _i, _i, _i, _f, _p],
     "curfpDaddToDiagonal": [_h, _i, _i, _i, _d, _p],
+    "curfpSsfrkEx": [_h, _i, _i, _i, _i, _i, ctypes.POINTER(_f), _p, _i,
+                     ctypes.POINTER(_f), _p, _i],
+    "curfpSpftrfEx": [_h, _i, _i, _i, _p, ctypes.POINTER(_i), _i],
+    "curfpSpftrsRefine": [_h, _i, _i, _i, _i, _p, _p, _p, _i, _i, ctypes.POINTER(_i)],
+    "curfpSsfmmAcc64": [_h, _i, _i, _i, _i, ctypes.POINTER(_f), _p, _p, _i,
+                        ctypes.POINTER(_f), _p, _i],
+    "curfpGetKernelLaunchCount": [_h, ctypes.POINTER(ctypes.c_longlong)],
 }
 
 _lib = None

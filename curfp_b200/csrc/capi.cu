@@ -5,11 +5,14 @@
 // executed by the native kernels.  No cuBLAS / cuSOLVER is linked.
 #include <climits>
 #include <cstdint>
+#include <cmath>
+#include <cstring>
 #include <new>
 
 #include "../../include/curfp.h"
 #include "context.h"
 #include "k_pack.cuh"
+#include "k_refine.cuh"
 
 using rfp::CudaExec;
 using rfp::Geometry;
@@ -31,7 +34,26 @@ inline int n1_of(int n, int lower) {
   return (n & 1) ? (lower ? n - n / 2 : n / 2) : n / 2;
 }
 
-__global__ void set_int(int* p, int v) { *p = v; }
+__global__ void set_int2(int* p, int v0, int v1) { p[0] = v0; p[1] = v1; }
+
+// Reset the info word (INT_MAX = no failure) and the kernel error word.
+inline int reset_info(curfpHandle_t h) {
+  set_int2<<<1, 1, 0, h->stream>>>(h->d_info, INT_MAX, 0);
+  ++h->launches;
+  return ok_launch();
+}
+
+// Synchronise and read both words back.
+inline int read_info(curfpHandle_t h, int* info, int* err) {
+  int w[2] = {0, 0};
+  if (cudaMemcpyAsync(w, h->d_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(h->stream) != cudaSuccess)
+    return 0;
+  *info = w[0];
+  *err = w[1];
+  return 1;
+}
 
 // Flags a zero on the diagonal of the factor (the condition on which the
 // reference's SPOTRI reports failure, src/curfp_spftri.cu:318,326).
@@ -68,6 +90,7 @@ curfpStatus_t pack(curfpHandle_t h, int transr, int lower, int n,
   rfp::kpack::pack_kernel<float>
       <<<tiles, dim3(rfp::kpack::TS, rfp::kpack::TY), 0, h->stream>>>(a, src, dst,
                                                                      to_rfp);
+  ++h->launches;
   return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
 }
 
@@ -81,7 +104,7 @@ curfpStatus_t curfpCreate(curfpHandle_t* handle) {
   curfpContext* ctx = new (std::nothrow) curfpContext();
   if (!ctx) return CURFP_STATUS_ALLOC_FAILED;
   if (cudaGetDevice(&ctx->device) != cudaSuccess ||
-      cudaMalloc(&ctx->d_info, sizeof(int)) != cudaSuccess) {
+      cudaMalloc(&ctx->d_info, 2 * sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     delete ctx;
     return CURFP_STATUS_NOT_INITIALIZED;
@@ -96,6 +119,8 @@ curfpStatus_t curfpDestroy(curfpHandle_t handle) {
   cudaStreamSynchronize(handle->stream);
   if (handle->ws) cudaFree(handle->ws);
   if (handle->stage) cudaFree(handle->stage);
+  if (handle->stage2) cudaFree(handle->stage2);
+  if (handle->ws2) cudaFree(handle->ws2);
   if (handle->d_info) cudaFree(handle->d_info);
   delete handle;
   return CURFP_STATUS_SUCCESS;
@@ -119,10 +144,10 @@ curfpStatus_t curfpGetStream(curfpHandle_t handle, cudaStream_t* stream) {
 // Checks and quick returns: src/curfp_ssfrk.cpp:147-161.  The leading
 // dimension bound is the one the reference's cuBLAS calls enforce
 // (lda >= rows of the A sub-blocks for trans=N, >= k for trans=T).
-curfpStatus_t curfpSsfrk(curfpHandle_t handle, curfpOperation_t transr,
-                         curfpFillMode_t uplo, curfpOperation_t trans, int n,
-                         int k, const float* alpha, const float* A, int lda,
-                         const float* beta, float* C) {
+static curfpStatus_t ssfrk_impl(curfpHandle_t handle, curfpOperation_t transr,
+                                curfpFillMode_t uplo, curfpOperation_t trans, int n,
+                                int k, const float* alpha, const float* A, int lda,
+                                const float* beta, float* C, int math) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (n < 0 || k < 0 || lda < 1) return CURFP_STATUS_INVALID_VALUE;
   if (!alpha || !beta) return CURFP_STATUS_INVALID_VALUE;
@@ -141,7 +166,23 @@ curfpStatus_t curfpSsfrk(curfpHandle_t handle, curfpOperation_t transr,
   CudaExec ex(handle);
   return status_of(rfp::plan::ssfrk(ex, transr == CURFP_OP_T, lower,
                                     trans == CURFP_OP_T, n, k, *alpha, A, lda,
-                                    *beta, C));
+                                    *beta, C, math));
+}
+
+curfpStatus_t curfpSsfrk(curfpHandle_t handle, curfpOperation_t transr,
+                         curfpFillMode_t uplo, curfpOperation_t trans, int n,
+                         int k, const float* alpha, const float* A, int lda,
+                         const float* beta, float* C) {
+  return ssfrk_impl(handle, transr, uplo, trans, n, k, alpha, A, lda, beta, C, 0);
+}
+
+curfpStatus_t curfpSsfrkEx(curfpHandle_t handle, curfpOperation_t transr,
+                           curfpFillMode_t uplo, curfpOperation_t trans, int n, int k,
+                           const float* alpha, const float* A, int lda, const float* beta,
+                           float* C, curfpMath_t math) {
+  if (math != CURFP_MATH_FP32 && math != CURFP_MATH_SPLIT_BF16)
+    return CURFP_STATUS_INVALID_VALUE;
+  return ssfrk_impl(handle, transr, uplo, trans, n, k, alpha, A, lda, beta, C, (int)math);
 }
 
 // src/curfp_ssfr2k.cpp:121-232
@@ -174,26 +215,37 @@ curfpStatus_t curfpSsfr2k(curfpHandle_t handle, curfpOperation_t transr,
 // src/curfp_spftrf.cpp:182-292.  One stream, no host synchronisation until
 // the single info read-back at the end (the reference syncs after each of its
 // two SPOTRF calls).  A failed pivot makes every later kernel return early.
-curfpStatus_t curfpSpftrf(curfpHandle_t handle, curfpOperation_t transr,
-                          curfpFillMode_t uplo, int n, float* A, int* info) {
+static curfpStatus_t spftrf_impl(curfpHandle_t handle, curfpOperation_t transr,
+                                 curfpFillMode_t uplo, int n, float* A, int* info,
+                                 int math) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (n < 0) return CURFP_STATUS_INVALID_VALUE;
   if (!info) return CURFP_STATUS_INVALID_VALUE;
   *info = 0;
   if (n == 0) return CURFP_STATUS_SUCCESS;
-  set_int<<<1, 1, 0, handle->stream>>>(handle->d_info, INT_MAX);
-  if (!ok_launch()) return CURFP_STATUS_EXECUTION_FAILED;
+  if (!reset_info(handle)) return CURFP_STATUS_EXECUTION_FAILED;
   CudaExec ex(handle, handle->d_info);
   int rc = rfp::plan::spftrf(ex, transr == CURFP_OP_T,
-                             uplo == CURFP_FILL_MODE_LOWER, n, A);
+                             uplo == CURFP_FILL_MODE_LOWER, n, A, math);
   if (rc) return status_of(rc);
-  int h = 0;
-  if (cudaMemcpyAsync(&h, handle->d_info, sizeof(int), cudaMemcpyDeviceToHost,
-                      handle->stream) != cudaSuccess ||
-      cudaStreamSynchronize(handle->stream) != cudaSuccess)
-    return CURFP_STATUS_EXECUTION_FAILED;
+  int h = 0, err = 0;
+  if (!read_info(handle, &h, &err)) return CURFP_STATUS_EXECUTION_FAILED;
+  if (err) return CURFP_STATUS_EXECUTION_FAILED;
   *info = (h == INT_MAX) ? 0 : h;
   return CURFP_STATUS_SUCCESS;
+}
+
+curfpStatus_t curfpSpftrf(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, int n, float* A, int* info) {
+  return spftrf_impl(handle, transr, uplo, n, A, info, 0);
+}
+
+curfpStatus_t curfpSpftrfEx(curfpHandle_t handle, curfpOperation_t transr,
+                            curfpFillMode_t uplo, int n, float* A, int* info,
+                            curfpMath_t math) {
+  if (math != CURFP_MATH_FP32 && math != CURFP_MATH_SPLIT_BF16)
+    return CURFP_STATUS_INVALID_VALUE;
+  return spftrf_impl(handle, transr, uplo, n, A, info, (int)math);
 }
 
 // src/curfp_spftrs.cpp:215-302
@@ -220,15 +272,13 @@ curfpStatus_t curfpSpftri(curfpHandle_t handle, curfpOperation_t transr,
   if (n == 0) return CURFP_STATUS_SUCCESS;
   const int tr = transr == CURFP_OP_T, lower = uplo == CURFP_FILL_MODE_LOWER;
   Geometry g = rfp::geometry(n, tr, lower);
-  set_int<<<1, 1, 0, handle->stream>>>(handle->d_info, INT_MAX);
+  if (!reset_info(handle)) return CURFP_STATUS_EXECUTION_FAILED;
   diag_zero_check<<<(n + 255) / 256, 256, 0, handle->stream>>>(g, arf,
                                                               handle->d_info);
+  ++handle->launches;
   if (!ok_launch()) return CURFP_STATUS_EXECUTION_FAILED;
-  int h = 0;
-  if (cudaMemcpyAsync(&h, handle->d_info, sizeof(int), cudaMemcpyDeviceToHost,
-                      handle->stream) != cudaSuccess ||
-      cudaStreamSynchronize(handle->stream) != cudaSuccess)
-    return CURFP_STATUS_EXECUTION_FAILED;
+  int h = 0, err = 0;
+  if (!read_info(handle, &h, &err)) return CURFP_STATUS_EXECUTION_FAILED;
   if (h != INT_MAX) return CURFP_STATUS_EXECUTION_FAILED;
   CudaExec ex(handle);
   return status_of(rfp::plan::spftri(ex, tr, lower, n, arf));
@@ -264,6 +314,7 @@ curfpStatus_t curfpRfpDiagIndices(curfpHandle_t handle, curfpOperation_t transr,
   if (n == 0) return CURFP_STATUS_SUCCESS;
   Geometry g = rfp::geometry(n, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER);
   rfp::kpack::diag_indices<<<(n + 255) / 256, 256, 0, handle->stream>>>(g, idx);
+  ++handle->launches;
   return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
 }
 
@@ -276,6 +327,7 @@ curfpStatus_t curfpSaddToDiagonal(curfpHandle_t handle, curfpOperation_t transr,
   if (n == 0) return CURFP_STATUS_SUCCESS;
   Geometry g = rfp::geometry(n, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER);
   rfp::kpack::add_diag<float><<<(n + 255) / 256, 256, 0, handle->stream>>>(g, value, arf);
+  ++handle->launches;
   return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
 }
 
@@ -287,7 +339,88 @@ curfpStatus_t curfpDaddToDiagonal(curfpHandle_t handle, curfpOperation_t transr,
   if (n == 0) return CURFP_STATUS_SUCCESS;
   Geometry g = rfp::geometry(n, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER);
   rfp::kpack::add_diag<double><<<(n + 255) / 256, 256, 0, handle->stream>>>(g, value, arf);
+  ++handle->launches;
   return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
+}
+
+// Y := alpha*A*X + beta*Y, A symmetric in RFP, products summed in FP64.
+curfpStatus_t curfpSsfmmAcc64(curfpHandle_t handle, curfpOperation_t transr,
+                              curfpFillMode_t uplo, int n, int nrhs, const float* alpha,
+                              const float* A, const float* X, int ldx, const float* beta,
+                              float* Y, int ldy) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (n < 0 || nrhs < 0 || !alpha || !beta) return CURFP_STATUS_INVALID_VALUE;
+  if (n == 0 || nrhs == 0) return CURFP_STATUS_SUCCESS;
+  if (ldx < n || ldy < n) return CURFP_STATUS_INVALID_VALUE;
+  Geometry g = rfp::geometry(n, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER);
+  dim3 grid((n + rfp::kref::TB - 1) / rfp::kref::TB, (nrhs + rfp::kref::TB - 1) / rfp::kref::TB);
+  rfp::kref::symm_acc64<<<grid, 256, 0, handle->stream>>>(g, A, X, ldx, Y, ldy, nrhs,
+                                                          *alpha, *beta);
+  ++handle->launches;
+  return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
+}
+
+// Mixed-precision refinement around spftrs (see include/curfp.h).
+curfpStatus_t curfpSpftrsRefine(curfpHandle_t handle, curfpOperation_t transr,
+                                curfpFillMode_t uplo, int n, int nrhs, const float* Aorig,
+                                const float* factor, float* B, int ldb, int max_iter,
+                                int* iters) {
+  if (iters) *iters = 0;
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (n < 0 || nrhs < 0 || ldb < 1 || max_iter < 0) return CURFP_STATUS_INVALID_VALUE;
+  if (n == 0 || nrhs == 0) return CURFP_STATUS_SUCCESS;
+  if (ldb < n) return CURFP_STATUS_INVALID_VALUE;
+  const int tr = transr == CURFP_OP_T, lower = uplo == CURFP_FILL_MODE_LOWER;
+  cudaStream_t st = handle->stream;
+  const size_t blk = (size_t)n * nrhs;
+  // scratch: saved right-hand side, residual, one word for the norm
+  float* scratch = static_cast<float*>(rfp::grow_buffer(
+      handle, &handle->ws2, &handle->ws2_bytes, (2 * blk + 64) * sizeof(float)));
+  if (!scratch) return CURFP_STATUS_ALLOC_FAILED;
+  float* B0 = scratch;
+  float* R = scratch + blk;
+  unsigned* nrm = reinterpret_cast<unsigned*>(scratch + 2 * blk);
+  const int grid = 148 * 8;
+  rfp::kref::copy_block<<<grid, 256, 0, st>>>(B0, n, B, ldb, n, nrhs);
+  ++handle->launches;
+  CudaExec ex(handle);
+  int rc = rfp::plan::spftrs(ex, tr, lower, n, nrhs, factor, B, ldb);
+  if (rc) return status_of(rc);
+  Geometry g = rfp::geometry(n, tr, lower);
+  dim3 sgrid((n + rfp::kref::TB - 1) / rfp::kref::TB, (nrhs + rfp::kref::TB - 1) / rfp::kref::TB);
+  float prev = INFINITY;
+  for (int it = 0; it < max_iter; ++it) {
+    // R := B0 - A X in FP64
+    rfp::kref::copy_block<<<grid, 256, 0, st>>>(R, n, B0, n, n, nrhs);
+    rfp::kref::symm_acc64<<<sgrid, 256, 0, st>>>(g, Aorig, B, ldb, R, n, nrhs, -1.0f, 1.0f);
+    cudaMemsetAsync(nrm, 0, sizeof(unsigned), st);
+    rfp::kref::absmax<<<grid, 256, 0, st>>>(R, n, n, nrhs, nrm);
+    handle->launches += 3;
+    if (!ok_launch()) return CURFP_STATUS_EXECUTION_FAILED;
+    unsigned bits = 0;
+    if (cudaMemcpyAsync(&bits, nrm, sizeof(unsigned), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      return CURFP_STATUS_EXECUTION_FAILED;
+    float r;
+    memcpy(&r, &bits, sizeof(r));
+    if (!(r < 0.5f * prev) || r == 0.0f) break;  // converged or stalled
+    prev = r;
+    if ((rc = rfp::plan::spftrs(ex, tr, lower, n, nrhs, factor, R, n))) return status_of(rc);
+    rfp::kref::add_inplace<<<grid, 256, 0, st>>>(B, ldb, R, n, n, nrhs);
+    ++handle->launches;
+    if (!ok_launch()) return CURFP_STATUS_EXECUTION_FAILED;
+    if (iters) *iters = it + 1;
+  }
+  return CURFP_STATUS_SUCCESS;
+}
+
+// Number of kernels this handle has launched (diagnostic counter).
+curfpStatus_t curfpGetKernelLaunchCount(curfpHandle_t handle, long long* count) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (!count) return CURFP_STATUS_INVALID_VALUE;
+  *count = handle->launches;
+  return CURFP_STATUS_SUCCESS;
 }
 
 }  // extern "C"

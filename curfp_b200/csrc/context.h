@@ -16,11 +16,16 @@
 struct curfpContext {
   cudaStream_t stream = nullptr;
   int device = 0;
-  int* d_info = nullptr;   // INT_MAX = no failure
+  int* d_info = nullptr;   // [0]: INT_MAX = no pivot failure; [1]: kernel error code
   void* ws = nullptr;      // TRSM diagonal-block inverses and other scratch
   size_t ws_bytes = 0;
-  void* stage = nullptr;   // split-BF16 operand staging
+  void* stage = nullptr;   // split-BF16 operand staging (first operand)
   size_t stage_bytes = 0;
+  void* stage2 = nullptr;  // split-BF16 operand staging (second operand)
+  size_t stage2_bytes = 0;
+  void* ws2 = nullptr;     // refinement scratch (saved RHS, residual)
+  size_t ws2_bytes = 0;
+  long long launches = 0;  // kernels launched through this handle
 };
 
 namespace rfp {
@@ -36,6 +41,8 @@ class CudaExec : public Exec {
   int lauum_tile(View L, int n) override;
   float* workspace(size_t nfloats) override;
   int inplace_rows() const override { return 64; }
+  int gemm_shared(View X, int rows, int k, const SharedTask* t, int count,
+                  int math) override;
 
  private:
   curfpContext* ctx_;
@@ -44,5 +51,13 @@ class CudaExec : public Exec {
 
 // Grow a stream-ordered buffer to at least `bytes`; returns nullptr on failure.
 void* grow_buffer(curfpContext* ctx, void** buf, size_t* cur, size_t bytes);
+
+// Split-BF16 tensor-core contraction (tc_engine.cu).  C_t := alpha_t *
+// A[a_row0:+m, :] B[b_row0:+n, :]^T + beta_t C_t with A (arows x k) and B
+// (brows x k) FP32 views; B.p == nullptr means B is A.
+int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, View B,
+                int brows, int k, const SharedTask* tasks, int count);
+// Whether a contraction of this size goes to the tensor-core path.
+bool tc_worthwhile(int m, int n, int k);
 
 }  // namespace rfp

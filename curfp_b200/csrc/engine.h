@@ -31,6 +31,17 @@ struct GemmProb {
 
 constexpr int kMaxBatch = 4;
 
+// One output block of a contraction whose two operands are row ranges of the
+// same matrix X (rows x k): C := alpha * X[a_row0:+m, :] X[b_row0:+n, :]^T
+// + beta * C.  SYRK updates of the RFP blocks and the three blocks of ssfrk
+// are of this form, so the operand is staged (split) once for all of them.
+struct SharedTask {
+  int a_row0, b_row0, m, n;
+  View C;
+  float alpha, beta;
+  int c_lower;  // 1: write only i >= j; 2 (executor-internal): only i <= j
+};
+
 // Block sizes of the recursive algorithms.
 constexpr int kPotrfTile = 64;   // diagonal Cholesky tiles
 constexpr int kTrsmLeaf = 64;    // TRSM diagonal blocks (inverted, then multiplied)
@@ -57,6 +68,26 @@ class Exec {
   virtual float* workspace(size_t nfloats) = 0;
   // Largest m of an in-place GEMM.
   virtual int inplace_rows() const = 0;
+  // Contractions sharing one operand matrix.  The default lowers them to
+  // gemm(); the CUDA executor stages X once for the tensor-core path.
+  virtual int gemm_shared(View X, int rows, int k, const SharedTask* t, int count,
+                          int math) {
+    (void)rows;
+    GemmProb p[kMaxBatch];
+    if (count > kMaxBatch) return 3;
+    for (int i = 0; i < count; ++i) {
+      GemmProb& g = p[i];
+      g.A = sub(X, t[i].a_row0, 0);
+      g.B = tr(sub(X, t[i].b_row0, 0));
+      g.A2 = g.A; g.B2 = g.B;
+      g.C = t[i].C;
+      g.m = t[i].m; g.n = t[i].n; g.k = k; g.k2 = 0;
+      g.alpha = t[i].alpha; g.beta = t[i].beta;
+      g.c_lower = t[i].c_lower; g.a_lower = 0; g.inplace = 0;
+      g.math = math;
+    }
+    return gemm(p, count);
+  }
 };
 
 namespace plan {

@@ -36,7 +36,7 @@ namespace {
 
 template <int BM, int BN>
 int launch_gemm(const GemmProb* p, int count, const int* abort_flag,
-                cudaStream_t st) {
+                cudaStream_t st, long long* launches) {
   kgemm::Batch b{};
   int tiles = 0, cnt = 0;
   for (int i = 0; i < count; ++i) {
@@ -65,14 +65,54 @@ int launch_gemm(const GemmProb* p, int count, const int* abort_flag,
   b.total_tiles = tiles;
   b.abort_flag = abort_flag;
   kgemm::sgemm_batch<BM, BN><<<tiles, kgemm::kThreads, 0, st>>>(b);
+  ++*launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
 }  // namespace
 
+// Output written through a column-contiguous view keeps the tensor-core
+// epilogue's warp-wide stores coalesced: C = A B^T is computed as
+// C^T = B A^T when C's contiguous dimension is its column index.
+static void orient(View& A, int& arows, View& B, int& brows, SharedTask& t) {
+  const bool col_contig = (t.C.cs == 1 || t.C.cs == -1) && !(t.C.rs == 1 || t.C.rs == -1);
+  if (!col_contig) return;
+  View tv = A; A = B; B = tv;
+  int tr_ = arows; arows = brows; brows = tr_;
+  int x = t.a_row0; t.a_row0 = t.b_row0; t.b_row0 = x;
+  x = t.m; t.m = t.n; t.n = x;
+  t.C = tr(t.C);
+  t.c_lower = t.c_lower ? 2 : 0;  // 2 = upper mask after transposition
+}
+
+int CudaExec::gemm_shared(View X, int rows, int k, const SharedTask* t, int count,
+                          int math) {
+  bool tc = math != 0 && count <= kMaxBatch;
+  for (int i = 0; tc && i < count; ++i)
+    tc = tc_worthwhile(t[i].m, t[i].n, k);
+  if (!tc) return Exec::gemm_shared(X, rows, k, t, count, math);
+  SharedTask tt[kMaxBatch];
+  for (int i = 0; i < count; ++i) {
+    tt[i] = t[i];
+    View A = X, B{nullptr, 0, 0};
+    int ar = rows, br = rows;
+    orient(A, ar, B, br, tt[i]);  // shared operand: swapping keeps B == A
+  }
+  return tc_contract(ctx_, abort_, X, rows, View{nullptr, 0, 0}, rows, k, tt, count);
+}
+
 int CudaExec::gemm(const GemmProb* p, int count) {
   if (count <= 0) return 0;
   if (count > kMaxBatch) return 3;
+  if (count == 1 && p[0].math && !p[0].inplace && !p[0].a_lower && p[0].k2 == 0 &&
+      tc_worthwhile(p[0].m, p[0].n, p[0].k)) {
+    const GemmProb& g = p[0];
+    View A = g.A, Bt = tr(g.B);  // A: m x k, Bt: n x k
+    int ar = g.m, br = g.n;
+    SharedTask t{0, 0, g.m, g.n, g.C, g.alpha, g.beta, g.c_lower};
+    orient(A, ar, Bt, br, t);
+    return tc_contract(ctx_, abort_, A, ar, Bt, br, g.k, &t, 1);
+  }
   // Tile choice: 128 x 128 when it fills the machine, else 64 x 64.
   int64_t t128 = 0;
   int maxm = 0;
@@ -82,13 +122,14 @@ int CudaExec::gemm(const GemmProb* p, int count) {
     if (p[i].inplace && p[i].m > maxm) maxm = p[i].m;
   }
   if (t128 >= 2 * 148 && maxm == 0)
-    return launch_gemm<128, 128>(p, count, abort_, ctx_->stream);
-  return launch_gemm<64, 64>(p, count, abort_, ctx_->stream);
+    return launch_gemm<128, 128>(p, count, abort_, ctx_->stream, &ctx_->launches);
+  return launch_gemm<64, 64>(p, count, abort_, ctx_->stream, &ctx_->launches);
 }
 
 int CudaExec::potrf_tile(View L, int n, int info_base) {
   if (n <= 0) return 0;
   ktile::potrf_tile<<<1, 256, 0, ctx_->stream>>>(L, n, info_base, ctx_->d_info);
+  ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
@@ -97,6 +138,7 @@ int CudaExec::trtri_blocks(View L, int n, int nb, float* W) {
   if (nb != ktile::T) return 3;
   int nblk = (n + nb - 1) / nb;
   ktile::trtri_blocks<<<nblk, ktile::T, 0, ctx_->stream>>>(L, n, W, abort_);
+  ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
@@ -104,6 +146,7 @@ int CudaExec::trtri_tile(View L, int n) {
   if (n <= 0) return 0;
   if (n > ktile::T) return 3;
   ktile::trtri_blocks<<<1, ktile::T, 0, ctx_->stream>>>(L, n, nullptr, abort_);
+  ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
@@ -111,6 +154,7 @@ int CudaExec::lauum_tile(View L, int n) {
   if (n <= 0) return 0;
   if (n > ktile::T) return 3;
   ktile::lauum_tile<<<1, 256, 0, ctx_->stream>>>(L, n);
+  ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 

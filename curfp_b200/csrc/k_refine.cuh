@@ -1,0 +1,120 @@
+// k_refine.cuh — kernels of the iterative-refinement solve.
+//
+// symm_acc64: Y := alpha * A X + beta * Y for a symmetric A held in RFP (any
+// variant) and column-major X, Y (n x nrhs).  Products of the FP32 inputs are
+// exact in FP64 and are summed in FP64; each output is rounded to FP32 once.
+// This is the only FP64 arithmetic of the solver (the residual b - A x).
+// One CTA owns a 64-row x 64-column output block and sweeps the 64-wide column
+// blocks of A; A elements are addressed through the RFP geometry (the upper
+// half of the symmetric matrix is read from the stored lower element).
+#pragma once
+#include <cstdint>
+
+#include "rfp.h"
+
+namespace rfp {
+namespace kref {
+
+constexpr int TB = 64;
+
+__global__ void __launch_bounds__(256) symm_acc64(Geometry g, const float* __restrict__ arf,
+                                                  const float* __restrict__ X, int64_t ldx,
+                                                  float* Y, int64_t ldy, int nrhs,
+                                                  float alpha, float beta) {
+  __shared__ float As[TB][TB + 1];
+  __shared__ float Xs[TB][TB + 1];
+  const int n = g.n;
+  const int i0 = blockIdx.x * TB, c0 = blockIdx.y * TB;
+  const int tid = threadIdx.x;
+  const int tr = tid / 16, tc = tid % 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+
+  for (int j0 = 0; j0 < n; j0 += TB) {
+#pragma unroll 4
+    for (int r = 0; r < 16; ++r) {
+      const int e = tid + 256 * r;
+      const int li = e % TB, lj = e / TB;
+      const int64_t i = i0 + li, j = j0 + lj;
+      float v = 0.f;
+      if (i < n && j < n) v = arf[i >= j ? lower_offset(g, i, j) : lower_offset(g, j, i)];
+      As[li][lj] = v;
+      const int64_t c = c0 + lj;  // X tile: row j0+li, column c0+lj
+      const int64_t xr = j0 + li;
+      Xs[li][lj] = (xr < n && c < nrhs) ? X[xr + c * ldx] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = 0; k < TB; ++k) {
+      double a[4], x[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a[q] = (double)As[tr * 4 + q][k];
+        x[q] = (double)Xs[k][tc * 4 + q];
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = fma(a[p], x[q], acc[p][q]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int64_t i = i0 + tr * 4 + p;
+    if (i >= n) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t c = c0 + tc * 4 + q;
+      if (c >= nrhs) continue;
+      float* y = Y + i + c * ldy;
+      double v = (double)alpha * acc[p][q];
+      if (beta != 0.f) v += (double)beta * (double)*y;
+      *y = (float)v;
+    }
+  }
+}
+
+// max |R| over an n x nrhs column-major block into *out (as float bits; the
+// values are non-negative so integer max orders them).  *out must start at 0.
+__global__ void absmax(const float* __restrict__ R, int64_t ld, int n, int nrhs,
+                       unsigned* out) {
+  float m = 0.f;
+  const int64_t total = (int64_t)n * nrhs;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = e / n, i = e % n;
+    const float v = fabsf(R[i + c * ld]);
+    m = (v > m || v != v) ? v : m;
+  }
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+// X := X + D (column-major n x nrhs blocks).
+__global__ void add_inplace(float* X, int64_t ldx, const float* D, int64_t ldd, int n,
+                            int nrhs) {
+  const int64_t total = (int64_t)n * nrhs;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = e / n, i = e % n;
+    X[i + c * ldx] += D[i + c * ldd];
+  }
+}
+
+// Dst := Src (column-major n x nrhs blocks with their own leading dimensions).
+__global__ void copy_block(float* Dst, int64_t ldd, const float* Src, int64_t lds, int n,
+                           int nrhs) {
+  const int64_t total = (int64_t)n * nrhs;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = e / n, i = e % n;
+    Dst[i + c * ldd] = Src[i + c * lds];
+  }
+}
+
+}  // namespace kref
+}  // namespace rfp

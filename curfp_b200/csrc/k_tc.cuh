@@ -1,0 +1,346 @@
+// k_tc.cuh — split-BF16 tensor-core contraction for sm_100a (tcgen05 + TMA).
+//
+// FP32 operands are split into three BF16 terms x = hi + mid + lo (exact
+// residuals, |mid| <= 2^-8|x|, |lo| <= 2^-16|x|).  A product a*b is then the
+// sum of the six terms whose magnitude is >= 2^-16 |a b|:
+//     hi*hi + hi*mid + mid*hi + hi*lo + lo*hi + mid*mid
+// (dropped terms are <= 2^-24 |a b|, the FP32 unit roundoff), each a BF16
+// tensor-core product accumulated in FP32 in tensor memory.
+//
+// Kernel shape: one CTA per 128 x 256 output tile, 256 threads.
+//   warp 0   : TMA producer — per K-block of 32, six boxes (A hi/mid/lo
+//              128 x 32, B hi/mid/lo 256 x 32, SWIZZLE_64B) into a 3-stage
+//              shared-memory ring, completion on an mbarrier;
+//   warp 1   : MMA issuer — one elected thread issues 6 products x 2 K-steps
+//              of tcgen05.mma.cta_group::1.kind::f16 (M=128, N=256, K=16)
+//              per stage, tcgen05.commit frees the stage;
+//   warp 2   : allocates / frees 256 TMEM columns (the FP32 accumulator);
+//   warps 4-7: epilogue — tcgen05.ld of the accumulator rows of their TMEM
+//              sub-partition, C := alpha*acc + beta*C written through an
+//              arbitrary strided FP32 view (RFP block, any variant), with
+//              lower/upper masking for the triangular blocks.
+// Operands come from dense K-major BF16 staging buffers written by
+// split3_kernel, so every TMA box is 16-byte aligned whatever the RFP
+// variant's leading dimension or block offset.
+//
+// Every mbarrier wait is bounded; on timeout the kernel records an error code
+// in *err_flag, the other roles leave their loops, TMEM is freed and the CTA
+// returns (the host reports CURFP_STATUS_EXECUTION_FAILED).
+#pragma once
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <climits>
+#include <cstdint>
+
+#include "rfp.h"
+
+namespace rfp {
+namespace ktc {
+
+constexpr int BM = 128, BN = 256, BK = 32, STAGES = 3, PLANES = 3;
+constexpr int A_BYTES = BM * BK * 2;                        // 8 KB
+constexpr int B_BYTES = BN * BK * 2;                        // 16 KB
+constexpr int STAGE_BYTES = PLANES * (A_BYTES + B_BYTES);   // 72 KB
+constexpr int THREADS = 256;
+constexpr int TMEM_COLS = 256;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 128;
+constexpr int MAX_TASKS = 4;
+constexpr uint32_t WAIT_LIMIT = 1u << 24;          // polls per wait
+constexpr uint64_t WAIT_NS = 2000000000ull;        // and at most ~2 s of wall time
+
+// Instruction descriptor, kind::f16: D = F32 (bits 4-5 = 1), A = B = BF16
+// (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at bits
+// 17-22, M >> 4 at bits 24-28.
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) |
+                           ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+struct Task {
+  int a_row0, b_row0, m, n;
+  float* C;
+  int64_t c_rs, c_cs;
+  float alpha, beta;
+  int c_mask;  // 0 full, 1: write i >= j only, 2: write i <= j only
+  int tiles_m, tiles_n, tile_begin;
+};
+
+struct Batch {
+  Task t[MAX_TASKS];
+  int count;
+  int kblocks;
+  const int* abort_flag;  // non-null and != INT_MAX: no-op
+  int* err_flag;          // set non-zero on a wait timeout
+};
+
+__device__ __forceinline__ uint32_t su32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(su32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait; returns false on timeout or when another role aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity,
+                                          volatile int* abort_sh, int* err_flag,
+                                          int code) {
+  const uint64_t t0 = globaltimer();
+  for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
+    if (mbar_try(b, parity)) return true;
+    if (*abort_sh) return false;
+    if ((it & 1023u) == 1023u && globaltimer() - t0 > WAIT_NS) break;
+  }
+  *abort_sh = 1;
+  if (err_flag) atomicExch(err_flag, code);
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0,
+                                            int c1, int c2, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(su32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(su32(bar))
+      : "memory");
+}
+
+// Shared-memory matrix descriptor, K-major, SWIZZLE_64B: rows of 64 bytes,
+// 8-row swizzle atoms 512 bytes apart (SBO), version 1 (bits 46-47),
+// layout type 4 (bits 61-63).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) |
+         ((uint64_t)(512 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t ad, uint64_t bd,
+                                         uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(ad), "l"(bd), "r"(IDESC), "r"(accum));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          su32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Product table (A plane, B plane).
+__device__ __constant__ int kProdA[6] = {0, 0, 1, 0, 2, 1};
+__device__ __constant__ int kProdB[6] = {0, 1, 0, 2, 0, 1};
+
+__global__ void __launch_bounds__(THREADS, 1)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
+                   const __grid_constant__ CUtensorMap tmB, const Batch batch) {
+  if (batch.abort_flag && *batch.abort_flag != INT_MAX) return;
+  // Locate task and tile; tiles entirely outside a triangular mask exit.
+  int t = blockIdx.x, ti_ = 0;
+  while (ti_ + 1 < batch.count && t >= batch.t[ti_ + 1].tile_begin) ++ti_;
+  const Task& T = batch.t[ti_];
+  const int lt = t - T.tile_begin;
+  const int m0 = (lt % T.tiles_m) * BM, n0 = (lt / T.tiles_m) * BN;
+  if (T.c_mask == 1 && m0 + BM - 1 < n0) return;       // all i < j
+  if (T.c_mask == 2 && n0 + BN - 1 < m0) return;       // all i > j
+
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* abort_sh = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 2) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     su32(tmem_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int KB = batch.kblocks;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------- TMA producer ----------------
+      for (int kb = 0; kb < KB; ++kb) {
+        const int s = kb % STAGES;
+        const uint32_t ph = (kb / STAGES) & 1;
+        if (kb >= STAGES && !mbar_wait(&empty[s], ph ^ 1, abort_sh, batch.err_flag, 1)) break;
+        uint8_t* st = smem + s * STAGE_BYTES;
+        mbar_expect_tx(&full[s], STAGE_BYTES);
+        const int k0 = kb * BK;
+#pragma unroll
+        for (int p = 0; p < PLANES; ++p) {
+          tma_load_3d(st + p * A_BYTES, &tmA, k0, T.a_row0 + m0, p, &full[s]);
+          tma_load_3d(st + PLANES * A_BYTES + p * B_BYTES, &tmB, k0, T.b_row0 + n0, p,
+                      &full[s]);
+        }
+      }
+      // Drain: make sure no copy is still landing before the CTA exits.
+      for (int kb = KB - STAGES < 0 ? 0 : KB - STAGES; kb < KB; ++kb)
+        mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, abort_sh, nullptr, 0);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---------------- MMA issuer ----------------
+      uint32_t accum = 0;
+      for (int kb = 0; kb < KB; ++kb) {
+        const int s = kb % STAGES;
+        const uint32_t ph = (kb / STAGES) & 1;
+        if (!mbar_wait(&full[s], ph, abort_sh, batch.err_flag, 2)) break;
+        tc_fence_after();
+        const uint32_t a0 = su32(smem + s * STAGE_BYTES);
+        const uint32_t b0 = a0 + PLANES * A_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk) {
+#pragma unroll
+          for (int q = 0; q < 6; ++q) {
+            const uint64_t ad = sdesc(a0 + kProdA[q] * A_BYTES + kk * 32);
+            const uint64_t bd = sdesc(b0 + kProdB[q] * B_BYTES + kk * 32);
+            mma_bf16(tmem, ad, bd, accum);
+            accum = 1;
+          }
+        }
+        mma_commit(&empty[s]);
+      }
+      mma_commit(done);
+    }
+  } else if (warp >= 4) {
+    // ---------------- epilogue ----------------
+    const int q = warp - 4;
+    bool ok = mbar_wait(done, 0, abort_sh, batch.err_flag, 3);
+    tc_fence_after();
+    ok = __all_sync(0xffffffffu, ok && !*abort_sh);
+    if (ok) {
+      const int r = q * 32 + lane;
+      const int gi = m0 + r;
+      const bool row_ok = gi < T.m;
+      float* crow = T.C + (int64_t)gi * T.c_rs;
+      for (int c0 = 0; c0 < BN; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
+        if (!row_ok) continue;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int gj = n0 + c0 + j;
+          if (gj >= T.n) break;
+          if (T.c_mask == 1 && gj > gi) break;
+          if (T.c_mask == 2 && gj < gi) continue;
+          float* c = crow + (int64_t)gj * T.c_cs;
+          float out = T.alpha * v[j];
+          if (T.beta != 0.f) out = fmaf(T.beta, *c, out);
+          *c = out;
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TMEM_COLS));
+  }
+}
+
+// Split an FP32 view X (rows x k, element (i,j) = X.p[i*rs + j*cs]) into three
+// BF16 planes, row-major with K contiguous: out[p][i][j], plane stride
+// rows_pad * k_pad.  Padding rows/columns are written as zeros.
+// Grid (k_pad/32, rows_pad/32), block (32, 8).
+__global__ void __launch_bounds__(256) split3_kernel(View X, int rows, int k,
+                                                     __nv_bfloat16* out, int rows_pad,
+                                                     int k_pad) {
+  __shared__ float t[32][33];
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const bool kcont = (X.cs == 1 || X.cs == -1);
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    int lr, lc;
+    if (kcont) { lc = tx; lr = ty + 8 * r; }
+    else       { lr = tx; lc = ty + 8 * r; }
+    const int gr = r0 + lr, gc = c0 + lc;
+    t[lr][lc] = (gr < rows && gc < k) ? X.p[(int64_t)gr * X.rs + (int64_t)gc * X.cs] : 0.f;
+  }
+  __syncthreads();
+  const int64_t plane = (int64_t)rows_pad * k_pad;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int lr = ty + 8 * r;
+    const float x = t[lr][tx];
+    const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(hi);
+    const __nv_bfloat16 mid = __float2bfloat16_rn(r1);
+    const float r2 = r1 - __bfloat162float(mid);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(r2);
+    const int64_t o = (int64_t)(r0 + lr) * k_pad + c0 + tx;
+    out[o] = hi;
+    out[o + plane] = mid;
+    out[o + 2 * plane] = lo;
+  }
+}
+
+}  // namespace ktc
+}  // namespace rfp

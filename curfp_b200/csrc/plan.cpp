@@ -122,10 +122,8 @@ int potrf_lower(Exec& ex, View A, int n, int info_base, int math) {
   // A21 := A21 L11^{-T}   <=>   L11 A21^T = A21^T
   if ((rc = trsm_lln(ex, A, n1, tr(A21), n2, 1.0f, math))) return rc;
   // A22 := A22 - A21 A21^T (lower)
-  GemmProb p = gemm_prob(A21, tr(A21), sub(A, n1, n1), n2, n2, n1, -1.0f, 1.0f,
-                         math);
-  p.c_lower = 1;
-  if ((rc = ex.gemm(&p, 1))) return rc;
+  SharedTask t{0, 0, n2, n2, sub(A, n1, n1), -1.0f, 1.0f, 1};
+  if ((rc = ex.gemm_shared(A21, n2, n1, &t, 1, math))) return rc;
   return potrf_lower(ex, sub(A, n1, n1), n2, info_base + n1, math);
 }
 
@@ -170,22 +168,15 @@ int ssfrk(Exec& ex, int transr, int lower, int trans, int n, int k,
   View opA = trans ? View{const_cast<float*>(A), lda, 1}
                    : View{const_cast<float*>(A), 1, lda};
   if (alpha == 0.0f) k = 0;  // C := beta*C; A is not read
-  View A1 = opA, A2 = sub(opA, g.n1, 0);
   View C11 = block_view(C, g.b11), C21 = block_view(C, g.b21),
        C22 = block_view(C, g.b22);
-  GemmProb p[3];
+  SharedTask t[3];
   int cnt = 0;
-  if (g.n1 > 0) {
-    p[cnt] = gemm_prob(A1, tr(A1), C11, g.n1, g.n1, k, alpha, beta, math);
-    p[cnt++].c_lower = 1;
-  }
+  if (g.n1 > 0) t[cnt++] = SharedTask{0, 0, g.n1, g.n1, C11, alpha, beta, 1};
   if (g.n1 > 0 && g.n2 > 0)
-    p[cnt++] = gemm_prob(A2, tr(A1), C21, g.n2, g.n1, k, alpha, beta, math);
-  if (g.n2 > 0) {
-    p[cnt] = gemm_prob(A2, tr(A2), C22, g.n2, g.n2, k, alpha, beta, math);
-    p[cnt++].c_lower = 1;
-  }
-  return ex.gemm(p, cnt);
+    t[cnt++] = SharedTask{g.n1, 0, g.n2, g.n1, C21, alpha, beta, 0};
+  if (g.n2 > 0) t[cnt++] = SharedTask{g.n1, g.n1, g.n2, g.n2, C22, alpha, beta, 1};
+  return ex.gemm_shared(opA, n, k, t, cnt, math);
 }
 
 int ssfr2k(Exec& ex, int transr, int lower, int trans, int n, int k,
@@ -227,10 +218,8 @@ int spftrf(Exec& ex, int transr, int lower, int n, float* A, int math) {
   if (g.n2 == 0) return 0;
   if (g.n1 > 0) {
     if ((rc = trsm_lln(ex, V11, g.n1, tr(V21), g.n2, 1.0f, math))) return rc;
-    GemmProb p = gemm_prob(V21, tr(V21), V22, g.n2, g.n2, g.n1, -1.0f, 1.0f,
-                           math);
-    p.c_lower = 1;
-    if ((rc = ex.gemm(&p, 1))) return rc;
+    SharedTask t{0, 0, g.n2, g.n2, V22, -1.0f, 1.0f, 1};
+    if ((rc = ex.gemm_shared(V21, g.n2, g.n1, &t, 1, math))) return rc;
   }
   return potrf_lower(ex, V22, g.n2, g.n1, math);
 }

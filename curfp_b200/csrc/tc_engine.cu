@@ -1,0 +1,126 @@
+// tc_engine.cu — host side of the split-BF16 tensor-core contraction:
+// operand staging (FP32 -> 3 BF16 planes), TMA descriptors, task tiling and
+// the launch of ktc::tc_gemm_kernel on the handle's stream.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "context.h"
+#include "k_tc.cuh"
+
+namespace rfp {
+
+namespace {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+inline int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+struct Staged {
+  __nv_bfloat16* p;
+  int rows_pad;
+  int k_pad;
+};
+
+// Split X (rows x k) into 3 BF16 planes in a context staging buffer.
+int stage(curfpContext* ctx, void** buf, size_t* cur, View X, int rows, int k,
+          Staged* out) {
+  out->rows_pad = (int)(round_up(rows, ktc::BN) + ktc::BN);
+  out->k_pad = (int)round_up(k, ktc::BK);
+  size_t bytes = (size_t)3 * out->rows_pad * out->k_pad * sizeof(__nv_bfloat16);
+  void* p = grow_buffer(ctx, buf, cur, bytes);
+  if (!p) return 2;
+  out->p = static_cast<__nv_bfloat16*>(p);
+  dim3 grid(out->k_pad / 32, out->rows_pad / 32);
+  ktc::split3_kernel<<<grid, dim3(32, 8), 0, ctx->stream>>>(X, rows, k, out->p,
+                                                            out->rows_pad, out->k_pad);
+  ++ctx->launches;
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+int make_map(const Staged& s, int box_rows, CUtensorMap* map) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return 4;
+  cuuint64_t dims[3] = {(cuuint64_t)s.k_pad, (cuuint64_t)s.rows_pad, 3};
+  cuuint64_t strides[2] = {(cuuint64_t)s.k_pad * 2, (cuuint64_t)s.k_pad * 2 * s.rows_pad};
+  cuuint32_t box[3] = {(cuuint32_t)ktc::BK, (cuuint32_t)box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, s.p, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : 4;
+}
+
+}  // namespace
+
+bool tc_worthwhile(int m, int n, int k) {
+  return m >= 128 && n >= 128 && k >= 128 && (double)m * n * k >= 6.7e7;
+}
+
+int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, View B,
+                int brows, int k, const SharedTask* tasks, int count) {
+  if (count <= 0 || k <= 0) return 0;
+  if (count > ktc::MAX_TASKS) return 3;
+  Staged sa, sb;
+  int rc = stage(ctx, &ctx->stage, &ctx->stage_bytes, A, arows, k, &sa);
+  if (rc) return rc;
+  if (B.p) {
+    if ((rc = stage(ctx, &ctx->stage2, &ctx->stage2_bytes, B, brows, k, &sb))) return rc;
+  } else {
+    sb = sa;
+  }
+  CUtensorMap mA, mB;
+  if ((rc = make_map(sa, ktc::BM, &mA)) || (rc = make_map(sb, ktc::BN, &mB))) return rc;
+
+  ktc::Batch b{};
+  int tiles = 0, cnt = 0;
+  for (int i = 0; i < count; ++i) {
+    const SharedTask& s = tasks[i];
+    if (s.m <= 0 || s.n <= 0) continue;
+    ktc::Task& t = b.t[cnt++];
+    t.a_row0 = s.a_row0; t.b_row0 = s.b_row0; t.m = s.m; t.n = s.n;
+    t.C = s.C.p; t.c_rs = s.C.rs; t.c_cs = s.C.cs;
+    t.alpha = s.alpha; t.beta = s.beta;
+    t.c_mask = s.c_lower;  // 0 full, 1 lower, 2 upper
+    t.tiles_m = (s.m + ktc::BM - 1) / ktc::BM;
+    t.tiles_n = (s.n + ktc::BN - 1) / ktc::BN;
+    t.tile_begin = tiles;
+    tiles += t.tiles_m * t.tiles_n;
+  }
+  if (cnt == 0) return 0;
+  b.count = cnt;
+  b.kblocks = sa.k_pad / ktc::BK;
+  b.abort_flag = abort_flag;
+  b.err_flag = ctx->d_info + 1;
+  static bool attr_set = false;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(ktc::tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             ktc::SMEM_BYTES) != cudaSuccess)
+      return 4;
+    attr_set = true;
+  }
+  ktc::tc_gemm_kernel<<<tiles, ktc::THREADS, ktc::SMEM_BYTES, ctx->stream>>>(mA, mB, b);
+  ++ctx->launches;
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+}  // namespace rfp

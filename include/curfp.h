@@ -133,6 +133,54 @@ curfpStatus_t curfpDaddToDiagonal(curfpHandle_t handle,
                                   curfpFillMode_t uplo, int n, double value,
                                   double *arf);
 
+/* Arithmetic of the contractions inside ssfrk / spftrf (the precision form).
+ *   CURFP_MATH_FP32:       SIMT FP32 FMA, the drop-in (same as curfpSsfrk /
+ *                          curfpSpftrf).
+ *   CURFP_MATH_SPLIT_BF16: large contractions (SYRK / GEMM updates) run on the
+ *                          tcgen05 tensor cores with every FP32 operand split
+ *                          into three BF16 terms (hi + mid + lo) and six BF16
+ *                          products accumulated in FP32; diagonal blocks and
+ *                          small updates stay FP32. */
+typedef enum {
+    CURFP_MATH_FP32       = 0,
+    CURFP_MATH_SPLIT_BF16 = 1
+} curfpMath_t;
+
+/* curfpSsfrk with a selectable contraction arithmetic. */
+curfpStatus_t curfpSsfrkEx(curfpHandle_t handle, curfpOperation_t transr,
+                           curfpFillMode_t uplo, curfpOperation_t trans,
+                           int n, int k, const float *alpha, const float *A,
+                           int lda, const float *beta, float *C,
+                           curfpMath_t math);
+
+/* curfpSpftrf with a selectable contraction arithmetic. */
+curfpStatus_t curfpSpftrfEx(curfpHandle_t handle, curfpOperation_t transr,
+                            curfpFillMode_t uplo, int n, float *A, int *info,
+                            curfpMath_t math);
+
+/* Solve A*X = B with iterative refinement: X0 = spftrs(factor, B), then
+ * repeatedly R = B - A*X with the products of the ORIGINAL matrix Aorig (RFP,
+ * same transr/uplo) summed in FP64, D = spftrs(factor, R), X += D, for at most
+ * max_iter corrections, stopping when max|R| no longer halves.  B (n x nrhs,
+ * column-major, ldb >= n) is overwritten with X; *iters (host, may be NULL)
+ * receives the number of corrections applied.  Synchronises the stream once
+ * per iteration (the stopping test). */
+curfpStatus_t curfpSpftrsRefine(curfpHandle_t handle, curfpOperation_t transr,
+                                curfpFillMode_t uplo, int n, int nrhs,
+                                const float *Aorig, const float *factor,
+                                float *B, int ldb, int max_iter, int *iters);
+
+/* Y := alpha*A*X + beta*Y, A symmetric in RFP (n x n), X and Y n x nrhs
+ * column-major; products summed in FP64, each result rounded once. */
+curfpStatus_t curfpSsfmmAcc64(curfpHandle_t handle, curfpOperation_t transr,
+                              curfpFillMode_t uplo, int n, int nrhs,
+                              const float *alpha, const float *A,
+                              const float *X, int ldx, const float *beta,
+                              float *Y, int ldy);
+
+/* Number of kernels launched through this handle since its creation. */
+curfpStatus_t curfpGetKernelLaunchCount(curfpHandle_t handle, long long *count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -218,22 +218,23 @@ def test_spftri_zero_pivot_fails(curfp, orc):
 
 @pytest.mark.gpu
 def test_streams(curfp, orc):
-    """All routines on a non-default stream (reference test_spftrs.py:169-188)."""
+    """All routines on a non-default stream, with the tensors produced and
+    consumed on that stream too (reference test_spftrs.py:169-188)."""
     n, k = 300, 40
     s = torch.cuda.Stream()
     rng = np.random.default_rng(1)
     A = (rng.standard_normal((n, k)) / np.sqrt(k)).astype(np.float32)
     B = rng.standard_normal((n, 3)).astype(np.float32)
-    with torch.cuda.stream(s):
-        Ad, Bd = dev(A), dev(B)
-        C = torch.empty(n * (n + 1) // 2, device="cuda")
-    s.synchronize()
     curfp.set_stream(s)
     try:
-        curfp.ssfrk(Ad, C)
-        curfp.add_to_diagonal(C, 1.0)
-        curfp.spftrf(C)
-        curfp.spftrs(C, Bd)
+        with torch.cuda.stream(s):
+            Ad, Bd = dev(A), dev(B)
+            C = torch.empty(n * (n + 1) // 2, device="cuda")
+            curfp.ssfrk(Ad, C)
+            curfp.add_to_diagonal(C, 1.0)
+            curfp.spftrf(C)
+            curfp.spftrs(C, Bd)
+            out = Bd.cpu()
     finally:
         s.synchronize()
         curfp.set_stream(None)
@@ -241,4 +242,4 @@ def test_streams(curfp, orc):
     Co[orc.diag_indices(1, 1, n)] += 1.0
     Fo, _ = orc.spftrf(1, 1, n, Co)
     Xo = orc.spftrs(1, 1, n, 3, Fo, B.T.ravel(), n).reshape(3, n).T
-    np.testing.assert_allclose(host(Bd), Xo, atol=1e-3)
+    np.testing.assert_allclose(out.numpy(), Xo, atol=1e-3)
