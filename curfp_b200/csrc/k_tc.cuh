@@ -1,31 +1,45 @@
 // k_tc.cuh — split-BF16 tensor-core contraction for sm_100a (tcgen05 + TMA).
 //
-// FP32 operands are split into three BF16 terms x = hi + mid + lo (exact
-// residuals, |mid| <= 2^-8|x|, |lo| <= 2^-16|x|).  A product a*b is then the
-// sum of the six terms whose magnitude is >= 2^-16 |a b|:
-//     hi*hi + hi*mid + mid*hi + hi*lo + lo*hi + mid*mid
-// (dropped terms are <= 2^-24 |a b|, the FP32 unit roundoff), each a BF16
-// tensor-core product accumulated in FP32 in tensor memory.
+// Operand representation.  Every row i of an FP32 operand is scaled by a
+// power of two s_i >= max_k |x_ik| and written as three integer digits,
+//     x_ik = s_i * 2^-7 * (d0 + d1 * 2^-8 + d2 * 2^-16),  |d_t| <= 128,
+// each digit exact in BF16 (8 significant bits); the truncation is at most
+// 2^-24 s_i.  The six products whose weight is >= 2^-16,
+//     level 0: d0*d0     level 1: d0*d1 + d1*d0     level 2: d0*d2 + d2*d0 + d1*d1,
+// are BF16 tensor-core products summed in three FP32 accumulators in tensor
+// memory.  Digit products are integers <= 2^14, so over a chunk of 256 of the
+// K dimension every partial sum is an integer below 2^24 and the tensor-core
+// accumulation is EXACT (its internal truncation never drops a bit).  After
+// each chunk the epilogue warps fold the three level sums into an FP32
+// register accumulator with round-to-nearest:
+//     acc += L0 + (L1 + L2 * 2^-8) * 2^-8,
+// and at the end C := alpha * s_i s_j 2^-14 * acc + beta * C.  Rounding errors
+// are then those of K/256 round-to-nearest additions plus the 2^-24 s digit
+// truncation: FP32-level accuracy from BF16 tensor cores.  (Summing floating
+// BF16 splits directly in one accumulator loses several bits: tcgen05
+// accumulation rounds toward zero at every step.)
 //
-// Kernel shape: one CTA per 128 x 256 output tile, 256 threads.
-//   warp 0   : TMA producer — per K-block of 32, six boxes (A hi/mid/lo
-//              128 x 32, B hi/mid/lo 256 x 32, SWIZZLE_64B) into a 3-stage
+// Kernel shape: one CTA per 128 x 128 output tile, 256 threads.
+//   warp 0   : TMA producer — per K-block of 32, six boxes (A d0/d1/d2 and
+//              B d0/d1/d2, 128 x 32 BF16 each, SWIZZLE_64B) into a 4-stage
 //              shared-memory ring, completion on an mbarrier;
 //   warp 1   : MMA issuer — one elected thread issues 6 products x 2 K-steps
-//              of tcgen05.mma.cta_group::1.kind::f16 (M=128, N=256, K=16)
-//              per stage, tcgen05.commit frees the stage;
-//   warp 2   : allocates / frees 256 TMEM columns (the FP32 accumulator);
-//   warps 4-7: epilogue — tcgen05.ld of the accumulator rows of their TMEM
-//              sub-partition, C := alpha*acc + beta*C written through an
-//              arbitrary strided FP32 view (RFP block, any variant), with
-//              lower/upper masking for the triangular blocks.
-// Operands come from dense K-major BF16 staging buffers written by
-// split3_kernel, so every TMA box is 16-byte aligned whatever the RFP
-// variant's leading dimension or block offset.
+//              of tcgen05.mma.cta_group::1.kind::f16 (M=128, N=128, K=16) per
+//              stage into the level accumulators; tcgen05.commit frees the
+//              stage and signals the end of each 256-deep chunk;
+//   warp 2   : allocates / frees the tensor memory (3 x 128 columns used);
+//   warps 4-7: epilogue — per chunk, tcgen05.ld of the three level sums of
+//              their TMEM lane quarter into registers; at the end C is
+//              written through an arbitrary strided FP32 view (RFP block,
+//              any variant) with lower/upper masking.
+// Operands come from dense K-major staging buffers written by digits_kernel,
+// so every TMA box is 16-byte aligned whatever the RFP variant's leading
+// dimension or block offset.
 //
-// Every mbarrier wait is bounded; on timeout the kernel records an error code
-// in *err_flag, the other roles leave their loops, TMEM is freed and the CTA
-// returns (the host reports CURFP_STATUS_EXECUTION_FAILED).
+// Every mbarrier wait is bounded (polls and ~2 s of wall time); on timeout the
+// kernel records an error code in *err_flag, the roles leave their loops,
+// tensor memory is freed and the CTA returns (the host then reports
+// CURFP_STATUS_EXECUTION_FAILED).
 #pragma once
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -38,13 +52,14 @@
 namespace rfp {
 namespace ktc {
 
-constexpr int BM = 128, BN = 256, BK = 32, STAGES = 3, PLANES = 3;
+constexpr int BM = 128, BN = 128, BK = 32, STAGES = 4, PLANES = 3;
+constexpr int CHUNK_KB = 8;                                 // 8 x 32 = 256 deep
 constexpr int A_BYTES = BM * BK * 2;                        // 8 KB
-constexpr int B_BYTES = BN * BK * 2;                        // 16 KB
-constexpr int STAGE_BYTES = PLANES * (A_BYTES + B_BYTES);   // 72 KB
+constexpr int B_BYTES = BN * BK * 2;                        // 8 KB
+constexpr int STAGE_BYTES = PLANES * (A_BYTES + B_BYTES);   // 48 KB
 constexpr int THREADS = 256;
-constexpr int TMEM_COLS = 256;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 128;
+constexpr int TMEM_COLS = 512;                              // 3 x 128 used
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 constexpr int MAX_TASKS = 4;
 constexpr uint32_t WAIT_LIMIT = 1u << 24;          // polls per wait
 constexpr uint64_t WAIT_NS = 2000000000ull;        // and at most ~2 s of wall time
@@ -68,6 +83,8 @@ struct Batch {
   Task t[MAX_TASKS];
   int count;
   int kblocks;
+  const float* a_scale;   // per staged row of A: s_i (power of two)
+  const float* b_scale;   // per staged row of B
   const int* abort_flag;  // non-null and != INT_MAX: no-op
   int* err_flag;          // set non-zero on a wait timeout
 };
@@ -84,6 +101,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)),
                "r"(bytes)
                : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
@@ -173,9 +194,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Product table (A plane, B plane).
+// Product table: (A digit plane, B digit plane, level).
 __device__ __constant__ int kProdA[6] = {0, 0, 1, 0, 2, 1};
 __device__ __constant__ int kProdB[6] = {0, 1, 0, 2, 0, 1};
+__device__ __constant__ int kProdL[6] = {0, 1, 1, 2, 2, 2};
 
 __global__ void __launch_bounds__(THREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
@@ -195,8 +217,9 @@ __global__ void __launch_bounds__(THREADS, 1)
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
   uint64_t* empty = full + STAGES;
-  uint64_t* done = empty + STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  uint64_t* chunk_full = empty + STAGES;
+  uint64_t* drained = chunk_full + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
   volatile int* abort_sh = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -205,7 +228,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(done, 1);
+    mbar_init(chunk_full, 1);
+    mbar_init(drained, 128);
     *abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -220,6 +244,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   const int KB = batch.kblocks;
+  const int NCHUNK = (KB + CHUNK_KB - 1) / CHUNK_KB;
 
   if (warp == 0) {
     if (lane == 0) {
@@ -238,58 +263,86 @@ __global__ void __launch_bounds__(THREADS, 1)
                       &full[s]);
         }
       }
-      // Drain: make sure no copy is still landing before the CTA exits.
+      // Drain: no copy may still be landing when the CTA exits.
       for (int kb = KB - STAGES < 0 ? 0 : KB - STAGES; kb < KB; ++kb)
         mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, abort_sh, nullptr, 0);
     }
   } else if (warp == 1) {
     if (lane == 0) {
       // ---------------- MMA issuer ----------------
-      uint32_t accum = 0;
-      for (int kb = 0; kb < KB; ++kb) {
-        const int s = kb % STAGES;
-        const uint32_t ph = (kb / STAGES) & 1;
-        if (!mbar_wait(&full[s], ph, abort_sh, batch.err_flag, 2)) break;
-        tc_fence_after();
-        const uint32_t a0 = su32(smem + s * STAGE_BYTES);
-        const uint32_t b0 = a0 + PLANES * A_BYTES;
-#pragma unroll
-        for (int kk = 0; kk < BK / 16; ++kk) {
-#pragma unroll
-          for (int q = 0; q < 6; ++q) {
-            const uint64_t ad = sdesc(a0 + kProdA[q] * A_BYTES + kk * 32);
-            const uint64_t bd = sdesc(b0 + kProdB[q] * B_BYTES + kk * 32);
-            mma_bf16(tmem, ad, bd, accum);
-            accum = 1;
-          }
+      int kb = 0;
+      for (int c = 0; c < NCHUNK; ++c) {
+        if (c > 0) {
+          if (!mbar_wait(drained, (c - 1) & 1, abort_sh, batch.err_flag, 4)) break;
+          tc_fence_after();
         }
-        mma_commit(&empty[s]);
+        uint32_t started = 0;  // bit l: level l accumulates
+        const int kb_end = (kb + CHUNK_KB < KB) ? kb + CHUNK_KB : KB;
+        bool ok = true;
+        for (; kb < kb_end; ++kb) {
+          const int s = kb % STAGES;
+          const uint32_t ph = (kb / STAGES) & 1;
+          if (!mbar_wait(&full[s], ph, abort_sh, batch.err_flag, 2)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t a0 = su32(smem + s * STAGE_BYTES);
+          const uint32_t b0 = a0 + PLANES * A_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+              const int l = kProdL[q];
+              const uint64_t ad = sdesc(a0 + kProdA[q] * A_BYTES + kk * 32);
+              const uint64_t bd = sdesc(b0 + kProdB[q] * B_BYTES + kk * 32);
+              mma_bf16(tmem + (uint32_t)(l * BN), ad, bd, (started >> l) & 1u);
+              started |= 1u << l;
+            }
+          }
+          mma_commit(&empty[s]);
+        }
+        mma_commit(chunk_full);
+        if (!ok) break;
       }
-      mma_commit(done);
     }
   } else if (warp >= 4) {
     // ---------------- epilogue ----------------
     const int q = warp - 4;
-    bool ok = mbar_wait(done, 0, abort_sh, batch.err_flag, 3);
-    tc_fence_after();
-    ok = __all_sync(0xffffffffu, ok && !*abort_sh);
+    const uint32_t tq = tmem + ((uint32_t)(q * 32) << 16);
+    float acc[BN];
+#pragma unroll
+    for (int j = 0; j < BN; ++j) acc[j] = 0.f;
+    bool ok = true;
+    for (int c = 0; c < NCHUNK; ++c) {
+      bool w = mbar_wait(chunk_full, c & 1, abort_sh, batch.err_flag, 3);
+      ok = __all_sync(0xffffffffu, w && !*abort_sh);
+      if (!ok) break;
+      tc_fence_after();
+#pragma unroll
+      for (int c0 = 0; c0 < BN; c0 += 16) {
+        float l0[16], l1[16], l2[16];
+        tmem_ld16(tq + (uint32_t)c0, l0);
+        tmem_ld16(tq + (uint32_t)(BN + c0), l1);
+        tmem_ld16(tq + (uint32_t)(2 * BN + c0), l2);
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          acc[c0 + j] += l0[j] + (l1[j] + l2[j] * 0x1p-8f) * 0x1p-8f;
+      }
+      tc_fence_before();
+      mbar_arrive(drained);
+    }
     if (ok) {
       const int r = q * 32 + lane;
       const int gi = m0 + r;
-      const bool row_ok = gi < T.m;
-      float* crow = T.C + (int64_t)gi * T.c_rs;
-      for (int c0 = 0; c0 < BN; c0 += 16) {
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
-        if (!row_ok) continue;
+      if (gi < T.m) {
+        const float sa = batch.a_scale[T.a_row0 + gi] * 0x1p-14f;
+        float* crow = T.C + (int64_t)gi * T.c_rs;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int gj = n0 + c0 + j;
+        for (int j = 0; j < BN; ++j) {
+          const int gj = n0 + j;
           if (gj >= T.n) break;
           if (T.c_mask == 1 && gj > gi) break;
           if (T.c_mask == 2 && gj < gi) continue;
           float* c = crow + (int64_t)gj * T.c_cs;
-          float out = T.alpha * v[j];
+          float out = T.alpha * (acc[j] * (sa * batch.b_scale[T.b_row0 + gj]));
           if (T.beta != 0.f) out = fmaf(T.beta, *c, out);
           *c = out;
         }
@@ -305,11 +358,65 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
 }
 
-// Split an FP32 view X (rows x k, element (i,j) = X.p[i*rs + j*cs]) into three
-// BF16 planes, row-major with K contiguous: out[p][i][j], plane stride
-// rows_pad * k_pad.  Padding rows/columns are written as zeros.
+// Row scales of an FP32 view X (rows x k): s_i = smallest power of two with
+// s_i >= max_k |X_ik| (1 for an all-zero row), for rows < rows_pad (padding
+// rows get 1).  One block of 256 threads per 32 rows; the warp runs along
+// the contiguous dimension of X.
+__global__ void __launch_bounds__(256) rowscale_kernel(View X, int rows, int k,
+                                                       float* scale, int rows_pad) {
+  __shared__ float red[8][33];
+  const int r0 = blockIdx.x * 32;
+  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
+  const bool kcont = (X.cs == 1 || X.cs == -1);
+  float m[4] = {0.f, 0.f, 0.f, 0.f};
+  if (kcont) {
+    // warp ty handles rows r0 + ty + 8 j; lanes stride over k
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = r0 + ty + 8 * j;
+      if (r < rows)
+        for (int c = tx; c < k; c += 32)
+          m[j] = fmaxf(m[j], fabsf(X.p[(int64_t)r * X.rs + (int64_t)c * X.cs]));
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      for (int o = 16; o; o >>= 1) m[j] = fmaxf(m[j], __shfl_xor_sync(0xffffffffu, m[j], o));
+      if (tx == 0) red[0][ty + 8 * j] = m[j];
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) m[0] = red[0][threadIdx.x];
+  } else {
+    // thread (tx, ty): row r0 + tx, k in ty, ty + 8, ...
+    const int r = r0 + tx;
+    if (r < rows)
+      for (int c = ty; c < k; c += 8)
+        m[0] = fmaxf(m[0], fabsf(X.p[(int64_t)r * X.rs + (int64_t)c * X.cs]));
+    red[ty][tx] = m[0];
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      m[0] = red[0][threadIdx.x];
+      for (int y = 1; y < 8; ++y) m[0] = fmaxf(m[0], red[y][threadIdx.x]);
+    }
+  }
+  if (threadIdx.x < 32) {
+    const int r = r0 + threadIdx.x;
+    if (r < rows_pad) {
+      float s = 1.0f;
+      if (r < rows && m[0] > 0.f) {
+        int e;
+        frexpf(m[0], &e);   // m = f * 2^e, f in [0.5, 1)  ->  2^e >= m
+        s = ldexpf(1.0f, e);
+      }
+      scale[r] = s;
+    }
+  }
+}
+
+// Digits of X (see the header): three BF16 planes, row-major with K
+// contiguous, out[p][i][j], plane stride rows_pad * k_pad; zero padding.
 // Grid (k_pad/32, rows_pad/32), block (32, 8).
-__global__ void __launch_bounds__(256) split3_kernel(View X, int rows, int k,
+__global__ void __launch_bounds__(256) digits_kernel(View X, int rows, int k,
+                                                     const float* __restrict__ scale,
                                                      __nv_bfloat16* out, int rows_pad,
                                                      int k_pad) {
   __shared__ float t[32][33];
@@ -329,16 +436,17 @@ __global__ void __launch_bounds__(256) split3_kernel(View X, int rows, int k,
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const int lr = ty + 8 * r;
-    const float x = t[lr][tx];
-    const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-    const float r1 = x - __bfloat162float(hi);
-    const __nv_bfloat16 mid = __float2bfloat16_rn(r1);
-    const float r2 = r1 - __bfloat162float(mid);
-    const __nv_bfloat16 lo = __float2bfloat16_rn(r2);
+    const float inv = 1.0f / scale[r0 + lr];            // power of two: exact
+    const float y0 = t[lr][tx] * inv * 128.0f;          // |y0| <= 128, exact
+    const float d0 = rintf(y0);
+    const float y1 = (y0 - d0) * 256.0f;                // exact, |y1| <= 128
+    const float d1 = rintf(y1);
+    const float y2 = (y1 - d1) * 256.0f;                // exact
+    const float d2 = rintf(y2);
     const int64_t o = (int64_t)(r0 + lr) * k_pad + c0 + tx;
-    out[o] = hi;
-    out[o + plane] = mid;
-    out[o + 2 * plane] = lo;
+    out[o] = __float2bfloat16_rn(d0);                   // integers <= 128: exact
+    out[o + plane] = __float2bfloat16_rn(d1);
+    out[o + 2 * plane] = __float2bfloat16_rn(d2);
   }
 }
 

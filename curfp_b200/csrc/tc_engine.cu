@@ -36,24 +36,31 @@ EncodeTiledFn encode_fn() {
 inline int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
 struct Staged {
-  __nv_bfloat16* p;
+  __nv_bfloat16* p;   // 3 digit planes
+  float* scale;       // per-row power-of-two scales
   int rows_pad;
   int k_pad;
 };
 
-// Split X (rows x k) into 3 BF16 planes in a context staging buffer.
+// Stage X (rows x k) as row scales + 3 BF16 digit planes in a context
+// staging buffer (two kernels: row maxima, then digits).
 int stage(curfpContext* ctx, void** buf, size_t* cur, View X, int rows, int k,
           Staged* out) {
   out->rows_pad = (int)(round_up(rows, ktc::BN) + ktc::BN);
   out->k_pad = (int)round_up(k, ktc::BK);
-  size_t bytes = (size_t)3 * out->rows_pad * out->k_pad * sizeof(__nv_bfloat16);
-  void* p = grow_buffer(ctx, buf, cur, bytes);
+  const size_t plane_bytes =
+      (size_t)3 * out->rows_pad * out->k_pad * sizeof(__nv_bfloat16);
+  const size_t off = (size_t)round_up((int64_t)plane_bytes, 256);
+  void* p = grow_buffer(ctx, buf, cur, off + (size_t)out->rows_pad * sizeof(float));
   if (!p) return 2;
   out->p = static_cast<__nv_bfloat16*>(p);
+  out->scale = reinterpret_cast<float*>(static_cast<char*>(p) + off);
+  ktc::rowscale_kernel<<<out->rows_pad / 32, 256, 0, ctx->stream>>>(X, rows, k, out->scale,
+                                                                   out->rows_pad);
   dim3 grid(out->k_pad / 32, out->rows_pad / 32);
-  ktc::split3_kernel<<<grid, dim3(32, 8), 0, ctx->stream>>>(X, rows, k, out->p,
+  ktc::digits_kernel<<<grid, dim3(32, 8), 0, ctx->stream>>>(X, rows, k, out->scale, out->p,
                                                             out->rows_pad, out->k_pad);
-  ++ctx->launches;
+  ctx->launches += 2;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
@@ -109,6 +116,8 @@ int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, Vie
   if (cnt == 0) return 0;
   b.count = cnt;
   b.kblocks = sa.k_pad / ktc::BK;
+  b.a_scale = sa.scale;
+  b.b_scale = sb.scale;
   b.abort_flag = abort_flag;
   b.err_flag = ctx->d_info + 1;
   static bool attr_set = false;
