@@ -1,37 +1,42 @@
 """RFP Cholesky+solve benchmark (one JSON line on rank 0).
 
-Workload: n = 32768, transr='T', uplo='U', C = A A^T + 1.0 I with
-A ~ N(0,1)/sqrt(k), k = 1024 (synthetic, seeded, built on the device by the
-library's own ssfrk), 64 right-hand sides B ~ N(0,1).
-One step = spftrf (in-place Cholesky) + spftrs (64 RHS) on a fresh copy of C.
-Metric: Cholesky+solve TFLOP/s = (n^3/3 + 2 n^2 nrhs) / time.
-The RFP matrix (2.1 GB) is larger than L2 (126 MB), so no extra L2 flush.
+Workload (per GPU): n = 32768, transr='T', uplo='U', C = A A^T + 1.0 I with
+A ~ N(0,1)/sqrt(k), k = 1024, 64 right-hand sides B ~ N(0,1) -- synthetic and
+seeded, built on the device by the library's own ssfrk.
+One step = Cholesky of a fresh copy of C + solve of the 64 right-hand sides:
+  headline (--math bf16x3, default): curfpSpftrfEx(split-BF16 tensor-core
+      updates) + curfpSpftrsRefine(FP64-residual refinement, <= 2 corrections);
+  also measured and reported beside it: the plain FP32 drop-in
+      (curfpSpftrf + curfpSpftrs).
+Metric: Cholesky+solve TFLOP/s = (n^3/3 + n^2/2 + n/6 + 2 n^2 nrhs) / time.
+The RFP matrix (2.1 GB) is larger than L2 (126 MB): no extra L2 flush.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--math fp32|bf16x3] [--n 32768] [--nrhs 64]
+                  [--math bf16x3|fp32] [--n 32768] [--k 1024] [--nrhs 64]
 
 --impl reference times the reference's algorithm on the host cores: LAPACK's
-RFP routines (ssfrk/spftrf/spftrs via scipy/OpenBLAS, all threads), which the
+RFP routines (spftrf/spftrs via scipy/OpenBLAS, all threads), which the
 reference's GPU code translates call for call; each step is a bounded sample
-(n = 8192) of the same workload.  N > 1 GPUs run independent replicas
-(the path has no cross-GPU exchange); value = total flops / max-rank time.
+(n = 8192) of the same workload.  N > 1 GPUs run independent replicas (the
+path has no cross-GPU exchange); value = total flops / max-over-ranks time.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
 import subprocess
 import sys
 import threading
-import time
 from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "RFP Cholesky+solve TFLOP/s at n=32768 (spftrf + spftrs 64 RHS)"
+METRIC = "RFP Cholesky+solve TFLOP/s at n=32768 (spftrf + spftrs 64 RHS), split-BF16 vs plain FP32"
+CPU_SAMPLE_N = 8192
 
 
 def chol_solve_flops(n: int, nrhs: int) -> float:
@@ -39,7 +44,7 @@ def chol_solve_flops(n: int, nrhs: int) -> float:
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -48,7 +53,6 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.rows: list[list[str]] = []
-        self._stop = threading.Event()
         self._proc = None
 
     def __enter__(self):
@@ -57,8 +61,7 @@ class ClockSampler:
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
-            self._t.start()
+            threading.Thread(target=self._read, daemon=True).start()
         except Exception:
             self._proc = None
         return self
@@ -76,8 +79,13 @@ class ClockSampler:
                 self._proc.kill()
 
     def summary(self) -> dict:
-        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in self.rows if len(r) > 8 and num(r[1]) is not None]
+        mx = [num(r[2]) for r in self.rows if len(r) > 8 and num(r[2]) is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in self.rows if len(r) > 8
                           for i in range(4) if r[5 + i].lower() == "active"})
@@ -91,15 +99,13 @@ def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
     if world > 1:
         import datetime
 
         import torch.distributed as dist
-        torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
-    else:
-        torch.cuda.set_device(local)
     return rank, world, local
 
 
@@ -119,13 +125,21 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
-def cpu_baseline(n_sample: int = 8192, nrhs: int = 64, reps: int = 2) -> dict:
-    """LAPACK (scipy/OpenBLAS) on the host: spftrf + spftrs at n_sample."""
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"bf16_tflops": d["bf16_tflops"], "hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"bf16_tflops": 1590.0, "hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def cpu_baseline(n_sample: int = CPU_SAMPLE_N, nrhs: int = 64, reps: int = 2) -> dict:
+    """LAPACK (scipy/OpenBLAS) spftrf + spftrs on the host at n_sample."""
     import numpy as np
 
     from oracle import port
     rng = np.random.default_rng(0)
-    k = n_sample // 32
+    k = max(1, n_sample // 32)
     A = (rng.standard_normal((n_sample, k)) / np.sqrt(k)).astype(np.float32)
     B = rng.standard_normal((n_sample, nrhs)).astype(np.float32)
     best = None
@@ -134,10 +148,10 @@ def cpu_baseline(n_sample: int = 8192, nrhs: int = 64, reps: int = 2) -> dict:
         t = r["spftrf"] + r["spftrs"]
         best = t if best is None else min(best, t)
     val = chol_solve_flops(n_sample, nrhs) / best / 1e12
-    return {"value": round(val, 4), "unit": "TFLOP/s", "cores": port.threads(),
-            "kind": "port",
-            "sample": f"LAPACK spftrf+spftrs (scipy/OpenBLAS) at n={n_sample}, k={k}, "
-                      f"nrhs={nrhs}, transr=T uplo=U, best of {reps}"}
+    return {"value": round(val, 5), "unit": "TFLOP/s", "cores": port.threads(), "kind": "port",
+            "sample": f"LAPACK spftrf+spftrs (scipy {__import__('scipy').__version__}, OpenBLAS) "
+                      f"at n={n_sample}, nrhs={nrhs}, transr=T uplo=U, C=AA^T+I (k={k}), "
+                      f"best of {reps}"}
 
 
 def run_reference(args, rank, world):
@@ -148,29 +162,77 @@ def run_reference(args, rank, world):
     vals = [cpu_baseline(reps=1)["value"] for _ in range(args.steps)]
     cb = cpu_baseline(reps=1)
     v = statistics.median(vals)
-    n_s = 8192
-    ms = chol_solve_flops(n_s, args.nrhs) / (v * 1e12) * 1e3
+    ms = chol_solve_flops(CPU_SAMPLE_N, args.nrhs) / (v * 1e12) * 1e3
     cb["value"] = v
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "TFLOP/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"RFP Cholesky+solve, host LAPACK sample n={n_s}, "
+            "config": {"workload": f"RFP Cholesky+solve on host LAPACK, sample n={CPU_SAMPLE_N}, "
                                    f"nrhs={args.nrhs}, transr=T, uplo=U",
-                       "n": n_s, "nrhs": args.nrhs, "parallelism": "replicas"},
+                       "n": CPU_SAMPLE_N, "nrhs": args.nrhs, "parallelism": "host"},
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
+class Lib:
+    """Direct C-ABI calls (the boundary a C/ctypes caller uses)."""
+
+    def __init__(self):
+        import curfp_b200 as curfp
+        self.h = curfp._get_handle()
+        self.lib = self.h._lib
+        self.info = ctypes.c_int(0)
+        self.iters = ctypes.c_int(0)
+
+    def spftrf(self, n, C, math):
+        st = self.lib.curfpSpftrfEx(self.h.ptr, 1, 1, n, ctypes.c_void_p(C.data_ptr()),
+                                    ctypes.byref(self.info), math)
+        assert st == 0 and self.info.value == 0, (st, self.info.value)
+
+    def spftrs(self, n, nrhs, F, X):
+        assert self.lib.curfpSpftrs(self.h.ptr, 1, 1, n, nrhs, ctypes.c_void_p(F.data_ptr()),
+                                    ctypes.c_void_p(X.data_ptr()), n) == 0
+
+    def refine(self, n, nrhs, A, F, X, max_iter):
+        st = self.lib.curfpSpftrsRefine(self.h.ptr, 1, 1, n, nrhs, ctypes.c_void_p(A.data_ptr()),
+                                        ctypes.c_void_p(F.data_ptr()), ctypes.c_void_p(X.data_ptr()),
+                                        n, max_iter, ctypes.byref(self.iters))
+        assert st == 0, st
+        return self.iters.value
+
+    def launches(self):
+        c = ctypes.c_longlong(0)
+        self.lib.curfpGetKernelLaunchCount(self.h.ptr, ctypes.byref(c))
+        return c.value
+
+
+def timed_steps(step, prep, steps, world):
+    import torch
+    times = []
+    for _ in range(steps):
+        prep()
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times
+
+
 def run_ours(args, rank, world, local):
     import torch
 
     import curfp_b200 as curfp
-    from curfp_b200 import _lib
+    from curfp_b200 import precision as P
 
     n, k, nrhs = args.n, args.k, args.nrhs
+    math_head = 1 if args.math == "bf16x3" else 0
     flops = chol_solve_flops(n, nrhs)
     nt = n * (n + 1) // 2
     dev = torch.device("cuda", local)
@@ -182,85 +244,140 @@ def run_ours(args, rank, world, local):
     curfp.add_to_diagonal(C0, 1.0)
     del A
     C = torch.empty_like(C0)
-    Bc = B0.t().contiguous()         # column-major n x nrhs for the C ABI
+    Bc = B0.t().contiguous()          # column-major n x nrhs (the C ABI layout)
     X = torch.empty_like(Bc)
-    h = curfp._get_handle()
-    lib = _lib.load()
-    import ctypes
-    info = ctypes.c_int(0)
+    L = Lib()
 
-    def step():
-        st = lib.curfpSpftrf(h.ptr, 1, 1, n, ctypes.c_void_p(C.data_ptr()), ctypes.byref(info))
-        assert st == 0 and info.value == 0, (st, info.value)
-        st = lib.curfpSpftrs(h.ptr, 1, 1, n, nrhs, ctypes.c_void_p(C.data_ptr()),
-                             ctypes.c_void_p(X.data_ptr()), n)
-        assert st == 0
-
-    for _ in range(args.warmup):
+    def prep():
         C.copy_(C0)
         X.copy_(Bc)
-        step()
+
+    def step_prec():
+        L.spftrf(n, C, 1)
+        L.refine(n, nrhs, C0, C, X, args.max_iter)
+
+    def step_plain():
+        L.spftrf(n, C, 0)
+        L.spftrs(n, nrhs, C, X)
+
+    step_head = step_prec if math_head else step_plain
+    for _ in range(args.warmup):
+        prep()
+        step_head()
     torch.cuda.synchronize()
 
-    times = []
+    l0 = L.launches()
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            C.copy_(C0)
-            X.copy_(Bc)
-            barrier(world)
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            step()
-            e1.record()
-            torch.cuda.synchronize()
-            times.append(e0.elapsed_time(e1))
+        times = timed_steps(step_head, prep, args.steps, world)
+    launches = L.launches() - l0
     total_ms = max_over_ranks(sum(times), world)
     ms_step = total_ms / args.steps
     value = world * args.steps * flops / (total_ms * 1e-3) / 1e12
 
-    # End to end through the C ABI with host buffers: H2D of the RFP matrix
-    # and B (pinned), factor + solve, D2H of X.
+    # Accuracy of the measured step (FP64 backward errors, one solve).
+    prep()
+    step_head()
+    torch.cuda.synchronize()
+    res = B0.double() - P.ssfmm_acc64(C0, X.t().contiguous()).double()
+    berr_solve = (torch.linalg.norm(res, dim=0) /
+                  torch.linalg.norm(B0.double(), dim=0)).max().item()
+
+    # The other form, same workload, for the ratio the metric names.
+    other = {}
+    if not args.no_other:
+        step_other = step_plain if math_head else step_prec
+        for _ in range(1):
+            prep()
+            step_other()
+        t_other = timed_steps(step_other, prep, max(1, args.steps // 2), world)
+        ms_other = max_over_ranks(sum(t_other), world) / len(t_other)
+        other = {"value": round(flops / (ms_other * 1e-3) / 1e12, 4), "unit": "TFLOP/s",
+                 "ms_per_step": round(ms_other, 3),
+                 "form": "plain FP32 (curfpSpftrf + curfpSpftrs)" if math_head
+                 else "split-BF16 (curfpSpftrfEx + curfpSpftrsRefine)"}
+
+    # Live per-kernel-class timing over the same steps (a second pass with the
+    # library's event bracketing on; the headline number above has it off).
+    P.profile_enable(True)
+    timed_steps(step_head, prep, args.steps, world)
+    prof = P.profile_read()
+    P.profile_enable(False)
+    kernels = {k_: {"ms_per_step": round(v["ms"] / args.steps, 3),
+                    "launches_per_step": v["launches"] // args.steps} for k_, v in prof.items()}
+    peaks = measured_peaks()
+    roof = None
+    dom = "tc_gemm" if math_head else "sgemm"
+    if dom in prof and prof[dom]["ms"] > 0:
+        ach = prof[dom]["flops"] / (prof[dom]["ms"] * 1e-3) / 1e12
+        if math_head:
+            # six BF16 tensor products per FP32 product: the tensor roofline in
+            # FP32-equivalent flops is the BF16 peak / 6
+            peak = peaks["bf16_tflops"] / 6.0
+            roof = {"kernel": "tc_gemm_kernel (split-BF16 tcgen05)", "bound": "tensor",
+                    "achieved": round(ach, 2), "peak": round(peak, 2), "unit": "TFLOP/s",
+                    "frac": round(ach / peak, 4), "traffic": None,
+                    "note": f"FP32-equivalent flops; peak = {peaks['source']} bf16 "
+                            f"{peaks['bf16_tflops']} TFLOP/s / 6 products",
+                    "share_of_step": round(prof[dom]["ms"] / sum(t for t in times), 3)}
+        else:
+            roof = {"kernel": "sgemm_batch (SIMT FP32)", "bound": "fp32-simt",
+                    "achieved": round(ach, 2), "peak": None, "unit": "TFLOP/s", "frac": None,
+                    "traffic": None}
+
+    # End to end through the C ABI with host buffers (pinned): H2D of the RFP
+    # matrix and B, on-device copy of the matrix kept for the refinement
+    # residual, factor + solve, D2H of X.
     e2e = None
     if not args.no_e2e:
         C_h = C0.cpu().pin_memory()
         B_h = Bc.cpu().pin_memory()
         X_h = torch.empty_like(B_h).pin_memory()
-        e2e_times = []
-        for i in range(args.warmup + args.steps):
-            barrier(world)
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            C.copy_(C_h, non_blocking=True)
-            X.copy_(B_h, non_blocking=True)
-            step()
+        Corig = torch.empty_like(C0)
+
+        def step_e2e():
+            if math_head:
+                Corig.copy_(C_h, non_blocking=True)
+                C.copy_(Corig)
+                X.copy_(B_h, non_blocking=True)
+                L.spftrf(n, C, 1)
+                L.refine(n, nrhs, Corig, C, X, args.max_iter)
+            else:
+                C.copy_(C_h, non_blocking=True)
+                X.copy_(B_h, non_blocking=True)
+                step_plain()
             X_h.copy_(X, non_blocking=True)
-            e1.record()
-            torch.cuda.synchronize()
-            if i >= args.warmup:
-                e2e_times.append(e0.elapsed_time(e1))
-        e2e_ms = max_over_ranks(sum(e2e_times), world)
+
+        for _ in range(1):
+            step_e2e()
+        t_e2e = timed_steps(step_e2e, lambda: None, args.steps, world)
+        e2e_ms = max_over_ranks(sum(t_e2e), world)
         e2e = {"value": round(world * args.steps * flops / (e2e_ms * 1e-3) / 1e12, 4),
                "unit": "TFLOP/s", "h2d_bytes_per_step": nt * 4 + n * nrhs * 4,
-               "d2h_bytes_per_step": n * nrhs * 4 + 4}
+               "d2h_bytes_per_step": n * nrhs * 4}
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline()
 
     if rank == 0:
+        form = "split-BF16 tcgen05 + FP64-residual refinement" if math_head else "plain FP32"
         line = {"metric": METRIC, "value": round(value, 4), "unit": "TFLOP/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": round(ms_step, 3), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic",
-                "config": {"workload": f"RFP Cholesky+solve n={n} k={k} nrhs={nrhs} "
-                                       f"transr=T uplo=U shift=1.0 math={args.math}",
+                "config": {"workload": f"RFP Cholesky+solve n={n} nrhs={nrhs} transr=T uplo=U, "
+                                       f"C=AA^T+1.0I (A {n}x{k} N(0,1)/sqrt(k)), form: {form}",
                            "n": n, "k": k, "nrhs": nrhs, "math": args.math,
-                           "parallelism": f"replicas{world}",
+                           "refine_max_iter": args.max_iter if math_head else 0,
+                           "parallelism": f"replicas x{world}",
                            "l2": "inputs (2.1 GB RFP) larger than L2, no flush"},
-                "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cb}
+                "other_form": other, "solve_rel_residual_fp64": berr_solve,
+                "gpu_launches": launches, "kernels": kernels,
+                "roofline": roof, "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cb}
+        if other and other.get("value"):
+            line["precision_over_plain"] = round(
+                (value / other["value"]) if math_head else (other["value"] / value), 3)
         print(json.dumps(line), flush=True)
 
 
@@ -270,12 +387,14 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--math", default="fp32", choices=["fp32", "bf16x3"])
+    ap.add_argument("--math", default="bf16x3", choices=["fp32", "bf16x3"])
     ap.add_argument("--n", type=int, default=32768)
     ap.add_argument("--k", type=int, default=1024)
     ap.add_argument("--nrhs", type=int, default=64)
+    ap.add_argument("--max-iter", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-other", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -42,6 +42,9 @@ SIGNATURES = {
     "curfpSsfmmAcc64": [_h, _i, _i, _i, _i, ctypes.POINTER(_f), _p, _p, _i,
                         ctypes.POINTER(_f), _p, _i],
     "curfpGetKernelLaunchCount": [_h, ctypes.POINTER(ctypes.c_longlong)],
+    "curfpProfileEnable": [_h, _i],
+    "curfpProfileRead": [_h, _i, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_d),
+                         ctypes.POINTER(ctypes.c_longlong)],
 }
 
 _lib = None

@@ -55,6 +55,17 @@ inline int read_info(curfpHandle_t h, int* info, int* err) {
   return 1;
 }
 
+inline bool symm_attr() {
+  static bool done = false;
+  if (!done) {
+    if (cudaFuncSetAttribute(rfp::kref::symm_acc64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             rfp::kref::SYMM_SMEM) != cudaSuccess)
+      return false;
+    done = true;
+  }
+  return true;
+}
+
 // Flags a zero on the diagonal of the factor (the condition on which the
 // reference's SPOTRI reports failure, src/curfp_spftri.cu:318,326).
 __global__ void diag_zero_check(Geometry g, const float* arf, int* flag) {
@@ -87,6 +98,7 @@ curfpStatus_t pack(curfpHandle_t h, int transr, int lower, int n,
   a.upper = !lower;
   a.lda = lda;
   if (tiles == 0) return CURFP_STATUS_SUCCESS;
+  rfp::ProfScope ps(h->prof, h->stream, rfp::K_PACK, 0, 4.0 * n * ((double)n + 1));
   rfp::kpack::pack_kernel<float>
       <<<tiles, dim3(rfp::kpack::TS, rfp::kpack::TY), 0, h->stream>>>(a, src, dst,
                                                                      to_rfp);
@@ -109,6 +121,14 @@ curfpStatus_t curfpCreate(curfpHandle_t* handle) {
     delete ctx;
     return CURFP_STATUS_NOT_INITIALIZED;
   }
+  // Keep memory released by the stream-ordered workspace in the device pool
+  // (workspaces grow with the problem; re-mapping on every growth is slow).
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
   *handle = ctx;
   return CURFP_STATUS_SUCCESS;
 }
@@ -354,8 +374,13 @@ curfpStatus_t curfpSsfmmAcc64(curfpHandle_t handle, curfpOperation_t transr,
   if (ldx < n || ldy < n) return CURFP_STATUS_INVALID_VALUE;
   Geometry g = rfp::geometry(n, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER);
   dim3 grid((n + rfp::kref::TB - 1) / rfp::kref::TB, (nrhs + rfp::kref::TB - 1) / rfp::kref::TB);
-  rfp::kref::symm_acc64<<<grid, 256, 0, handle->stream>>>(g, A, X, ldx, Y, ldy, nrhs,
-                                                          *alpha, *beta);
+  {
+    rfp::ProfScope ps(handle->prof, handle->stream, rfp::K_SYMM64, 2.0 * n * (double)n * nrhs,
+                      4.0 * n * (double)n);
+    if (!symm_attr()) return CURFP_STATUS_EXECUTION_FAILED;
+    rfp::kref::symm_acc64<<<grid, 256, rfp::kref::SYMM_SMEM, handle->stream>>>(
+        g, A, X, ldx, Y, ldy, nrhs, *alpha, *beta);
+  }
   ++handle->launches;
   return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
 }
@@ -392,7 +417,13 @@ curfpStatus_t curfpSpftrsRefine(curfpHandle_t handle, curfpOperation_t transr,
   for (int it = 0; it < max_iter; ++it) {
     // R := B0 - A X in FP64
     rfp::kref::copy_block<<<grid, 256, 0, st>>>(R, n, B0, n, n, nrhs);
-    rfp::kref::symm_acc64<<<sgrid, 256, 0, st>>>(g, Aorig, B, ldb, R, n, nrhs, -1.0f, 1.0f);
+    {
+      rfp::ProfScope ps(handle->prof, st, rfp::K_SYMM64, 2.0 * n * (double)n * nrhs,
+                        4.0 * n * (double)n);
+      if (!symm_attr()) return CURFP_STATUS_EXECUTION_FAILED;
+      rfp::kref::symm_acc64<<<sgrid, 256, rfp::kref::SYMM_SMEM, st>>>(g, Aorig, B, ldb, R, n,
+                                                                    nrhs, -1.0f, 1.0f);
+    }
     cudaMemsetAsync(nrm, 0, sizeof(unsigned), st);
     rfp::kref::absmax<<<grid, 256, 0, st>>>(R, n, n, nrhs, nrm);
     handle->launches += 3;
@@ -412,6 +443,33 @@ curfpStatus_t curfpSpftrsRefine(curfpHandle_t handle, curfpOperation_t transr,
     if (!ok_launch()) return CURFP_STATUS_EXECUTION_FAILED;
     if (iters) *iters = it + 1;
   }
+  return CURFP_STATUS_SUCCESS;
+}
+
+// Per-kernel-class event timing (profile.h).
+curfpStatus_t curfpProfileEnable(curfpHandle_t handle, int enable) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  cudaStreamSynchronize(handle->stream);
+  handle->prof.reset();
+  handle->prof.on = enable != 0;
+  return CURFP_STATUS_SUCCESS;
+}
+
+curfpStatus_t curfpProfileRead(curfpHandle_t handle, int kclass, double* ms, double* flops,
+                               double* bytes, long long* launches) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (kclass < 0 || kclass >= rfp::K_NCLASS || !ms || !flops || !bytes || !launches)
+    return CURFP_STATUS_INVALID_VALUE;
+  if (cudaStreamSynchronize(handle->stream) != cudaSuccess) return CURFP_STATUS_EXECUTION_FAILED;
+  double t = 0, f = 0, b = 0;
+  long long c = 0;
+  for (const auto& r : handle->prof.recs) {
+    if (r.cls != kclass) continue;
+    float e = 0.f;
+    if (cudaEventElapsedTime(&e, r.e0, r.e1) != cudaSuccess) return CURFP_STATUS_EXECUTION_FAILED;
+    t += e; f += r.flops; b += r.bytes; ++c;
+  }
+  *ms = t; *flops = f; *bytes = b; *launches = c;
   return CURFP_STATUS_SUCCESS;
 }
 

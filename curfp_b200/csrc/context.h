@@ -12,6 +12,7 @@
 #include <cstddef>
 
 #include "engine.h"
+#include "profile.h"
 
 struct curfpContext {
   cudaStream_t stream = nullptr;
@@ -26,6 +27,9 @@ struct curfpContext {
   void* ws2 = nullptr;     // refinement scratch (saved RHS, residual)
   size_t ws2_bytes = 0;
   long long launches = 0;  // kernels launched through this handle
+  rfp::Profiler prof;      // optional per-class event timing
+  void* tsv = nullptr;     // wavefront solve flags / tickets
+  size_t tsv_bytes = 0;
 };
 
 namespace rfp {
@@ -43,6 +47,7 @@ class CudaExec : public Exec {
   int inplace_rows() const override { return 64; }
   int gemm_shared(View X, int rows, int k, const SharedTask* t, int count,
                   int math) override;
+  int trsm_wave(View L, int n, View B, int m, float alpha, const float* W) override;
 
  private:
   curfpContext* ctx_;

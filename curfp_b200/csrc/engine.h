@@ -43,10 +43,13 @@ struct SharedTask {
 };
 
 // Block sizes of the recursive algorithms.
-constexpr int kPotrfTile = 64;   // diagonal Cholesky tiles
+constexpr int kPotrfTile = 128;  // diagonal Cholesky tiles
 constexpr int kTrsmLeaf = 64;    // TRSM diagonal blocks (inverted, then multiplied)
 constexpr int kTriTile = 64;     // trtri / lauum tiles
 constexpr int kTrmmLeaf = 64;    // TRMM leaves (masked in-place multiply)
+constexpr int kTrsvMaxRhs = 512; // wavefront solve for at most this many RHS
+constexpr int kWaveLeaf = 512;   // recursive TRSM hands blocks <= this to the wavefront solve
+constexpr int kNotSupported = -1;
 
 class Exec {
  public:
@@ -68,6 +71,14 @@ class Exec {
   virtual float* workspace(size_t nfloats) = 0;
   // Largest m of an in-place GEMM.
   virtual int inplace_rows() const = 0;
+  // One-launch triangular solve L X = alpha B for few right-hand sides, with
+  // W holding the inverted 64 x 64 diagonal blocks (trtri_blocks).  Returns
+  // kNotSupported when the executor has no such path (the planner then uses
+  // the recursive blocked solve).
+  virtual int trsm_wave(View L, int n, View B, int m, float alpha, const float* W) {
+    (void)L; (void)n; (void)B; (void)m; (void)alpha; (void)W;
+    return kNotSupported;
+  }
   // Contractions sharing one operand matrix.  The default lowers them to
   // gemm(); the CUDA executor stages X once for the tensor-core path.
   virtual int gemm_shared(View X, int rows, int k, const SharedTask* t, int count,

@@ -6,6 +6,7 @@
 #include "context.h"
 #include "k_gemm.cuh"
 #include "k_tile.cuh"
+#include "k_trsv.cuh"
 
 namespace rfp {
 
@@ -14,13 +15,20 @@ void* grow_buffer(curfpContext* ctx, void** buf, size_t* cur, size_t bytes) {
   if (*buf) {
     cudaFreeAsync(*buf, ctx->stream);
     *buf = nullptr;
-    *cur = 0;
   }
+  // grow geometrically so that a recursion of increasing sizes reallocates
+  // O(log) times
   size_t want = bytes < 256 ? 256 : bytes;
+  if (*cur && want < *cur + *cur / 2) want = *cur + *cur / 2;
   void* p = nullptr;
   if (cudaMallocAsync(&p, want, ctx->stream) != cudaSuccess) {
     cudaGetLastError();
-    return nullptr;
+    want = bytes;  // retry without the growth margin
+    if (cudaMallocAsync(&p, want, ctx->stream) != cudaSuccess) {
+      cudaGetLastError();
+      *cur = 0;
+      return nullptr;
+    }
   }
   *buf = p;
   *cur = want;
@@ -36,7 +44,9 @@ namespace {
 
 template <int BM, int BN>
 int launch_gemm(const GemmProb* p, int count, const int* abort_flag,
-                cudaStream_t st, long long* launches) {
+                curfpContext* ctx) {
+  cudaStream_t st = ctx->stream;
+  double flops = 0;
   kgemm::Batch b{};
   int tiles = 0, cnt = 0;
   for (int i = 0; i < count; ++i) {
@@ -58,14 +68,16 @@ int launch_gemm(const GemmProb* p, int count, const int* abort_flag,
       return 3;
     q.tile_begin = tiles;
     tiles += g.c_lower ? q.tiles_m * (q.tiles_m + 1) / 2 : q.tiles_m * q.tiles_n;
+    flops += 2.0 * g.m * g.n * (double)(g.k + g.k2) * (g.c_lower ? 0.5 : 1.0);
     ++cnt;
   }
   if (cnt == 0) return 0;
   b.count = cnt;
   b.total_tiles = tiles;
   b.abort_flag = abort_flag;
+  ProfScope ps(ctx->prof, st, K_SGEMM, flops, 0);
   kgemm::sgemm_batch<BM, BN><<<tiles, kgemm::kThreads, 0, st>>>(b);
-  ++*launches;
+  ++ctx->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
@@ -122,13 +134,21 @@ int CudaExec::gemm(const GemmProb* p, int count) {
     if (p[i].inplace && p[i].m > maxm) maxm = p[i].m;
   }
   if (t128 >= 2 * 148 && maxm == 0)
-    return launch_gemm<128, 128>(p, count, abort_, ctx_->stream, &ctx_->launches);
-  return launch_gemm<64, 64>(p, count, abort_, ctx_->stream, &ctx_->launches);
+    return launch_gemm<128, 128>(p, count, abort_, ctx_);
+  return launch_gemm<64, 64>(p, count, abort_, ctx_);
 }
 
 int CudaExec::potrf_tile(View L, int n, int info_base) {
   if (n <= 0) return 0;
-  ktile::potrf_tile<<<1, 256, 0, ctx_->stream>>>(L, n, info_base, ctx_->d_info);
+  ProfScope ps(ctx_->prof, ctx_->stream, K_POTRF, (double)n * n * n / 3.0, 0);
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(ktile::potrf_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             ktile::POTRF_SMEM) != cudaSuccess)
+      return 4;
+    attr = true;
+  }
+  ktile::potrf_tile<<<1, 256, ktile::POTRF_SMEM, ctx_->stream>>>(L, n, info_base, ctx_->d_info);
   ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
@@ -137,6 +157,7 @@ int CudaExec::trtri_blocks(View L, int n, int nb, float* W) {
   if (n <= 0) return 0;
   if (nb != ktile::T) return 3;
   int nblk = (n + nb - 1) / nb;
+  ProfScope ps(ctx_->prof, ctx_->stream, K_TRTRI, (double)n * nb * nb / 3.0, 0);
   ktile::trtri_blocks<<<nblk, ktile::T, 0, ctx_->stream>>>(L, n, W, abort_);
   ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
@@ -145,6 +166,7 @@ int CudaExec::trtri_blocks(View L, int n, int nb, float* W) {
 int CudaExec::trtri_tile(View L, int n) {
   if (n <= 0) return 0;
   if (n > ktile::T) return 3;
+  ProfScope ps(ctx_->prof, ctx_->stream, K_TRTRI, (double)n * n * n / 3.0, 0);
   ktile::trtri_blocks<<<1, ktile::T, 0, ctx_->stream>>>(L, n, nullptr, abort_);
   ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
@@ -153,7 +175,29 @@ int CudaExec::trtri_tile(View L, int n) {
 int CudaExec::lauum_tile(View L, int n) {
   if (n <= 0) return 0;
   if (n > ktile::T) return 3;
+  ProfScope ps(ctx_->prof, ctx_->stream, K_LAUUM, (double)n * n * n / 3.0, 0);
   ktile::lauum_tile<<<1, 256, 0, ctx_->stream>>>(L, n);
+  ++ctx_->launches;
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+int CudaExec::trsm_wave(View L, int n, View B, int m, float alpha, const float* W) {
+  if (n <= 0 || m <= 0) return 0;
+  const int nblk = (n + ktrsv::NB - 1) / ktrsv::NB, nchunk = (m + ktrsv::NB - 1) / ktrsv::NB;
+  const size_t words = 1 + (size_t)nblk * nchunk;
+  int* sync = static_cast<int*>(grow_buffer(ctx_, &ctx_->tsv, &ctx_->tsv_bytes, words * 4));
+  if (!sync) return 2;
+  if (cudaMemsetAsync(sync, 0, words * 4, ctx_->stream) != cudaSuccess) return 4;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(ktrsv::trsm_wave, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             ktrsv::SMEM) != cudaSuccess)
+      return 4;
+    attr = true;
+  }
+  ProfScope ps(ctx_->prof, ctx_->stream, K_TRSV, (double)n * n * m, (double)n * n * 2.0);
+  ktrsv::trsm_wave<<<nblk * nchunk, 256, ktrsv::SMEM, ctx_->stream>>>(L, n, B, m, alpha, W, sync,
+                                                                     ctx_->d_info + 1, abort_);
   ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }

@@ -17,12 +17,18 @@ namespace kref {
 
 constexpr int TB = 64;
 
+// Operands are converted to FP64 once, when staged in shared memory, so the
+// inner loop is pure DFMA (16 per 8 shared loads).  Dynamic shared memory:
+// 2 x 64 x 65 doubles.
+constexpr int SYMM_SMEM = 2 * TB * (TB + 1) * 8;
+
 __global__ void __launch_bounds__(256) symm_acc64(Geometry g, const float* __restrict__ arf,
                                                   const float* __restrict__ X, int64_t ldx,
                                                   float* Y, int64_t ldy, int nrhs,
                                                   float alpha, float beta) {
-  __shared__ float As[TB][TB + 1];
-  __shared__ float Xs[TB][TB + 1];
+  extern __shared__ double dsm[];
+  double (*As)[TB + 1] = reinterpret_cast<double (*)[TB + 1]>(dsm);
+  double (*Xs)[TB + 1] = reinterpret_cast<double (*)[TB + 1]>(dsm + TB * (TB + 1));
   const int n = g.n;
   const int i0 = blockIdx.x * TB, c0 = blockIdx.y * TB;
   const int tid = threadIdx.x;
@@ -34,17 +40,31 @@ __global__ void __launch_bounds__(256) symm_acc64(Geometry g, const float* __res
     for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
 
   for (int j0 = 0; j0 < n; j0 += TB) {
-#pragma unroll 4
+    // The warp runs along the RFP block's contiguous direction: element
+    // (i,j) of the symmetric matrix is the stored lower element
+    // (max, min) = (p, q) at off + p*rs + q*cs.
+    const bool lower_tile = i0 >= j0;
+    const int64_t p0 = lower_tile ? i0 : j0, q0 = lower_tile ? j0 : i0;
+    const BlockGeom& bg = q0 < g.n1 ? (p0 < g.n1 ? g.b11 : g.b21) : g.b22;
+    const bool p_cont = (bg.rs == 1 || bg.rs == -1);
+    const bool i_fast = lower_tile ? p_cont : !p_cont;
+    float av[16], xv[16];
+#pragma unroll
     for (int r = 0; r < 16; ++r) {
       const int e = tid + 256 * r;
-      const int li = e % TB, lj = e / TB;
+      const int li = i_fast ? e % TB : e / TB, lj = i_fast ? e / TB : e % TB;
       const int64_t i = i0 + li, j = j0 + lj;
-      float v = 0.f;
-      if (i < n && j < n) v = arf[i >= j ? lower_offset(g, i, j) : lower_offset(g, j, i)];
-      As[li][lj] = v;
-      const int64_t c = c0 + lj;  // X tile: row j0+li, column c0+lj
-      const int64_t xr = j0 + li;
-      Xs[li][lj] = (xr < n && c < nrhs) ? X[xr + c * ldx] : 0.f;
+      av[r] = (i < n && j < n) ? arf[i >= j ? lower_offset(g, i, j) : lower_offset(g, j, i)]
+                               : 0.f;
+      const int64_t xr = j0 + (e % TB), c = c0 + (e / TB);  // X column-major: rows fastest
+      xv[r] = (xr < n && c < nrhs) ? X[xr + c * ldx] : 0.f;
+    }
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int e = tid + 256 * r;
+      const int li = i_fast ? e % TB : e / TB, lj = i_fast ? e / TB : e % TB;
+      As[li][lj] = (double)av[r];
+      Xs[e % TB][e / TB] = (double)xv[r];
     }
     __syncthreads();
 #pragma unroll 8
@@ -52,8 +72,8 @@ __global__ void __launch_bounds__(256) symm_acc64(Geometry g, const float* __res
       double a[4], x[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        a[q] = (double)As[tr * 4 + q][k];
-        x[q] = (double)Xs[k][tc * 4 + q];
+        a[q] = As[tr * 4 + q][k];
+        x[q] = Xs[k][tc * 4 + q];
       }
 #pragma unroll
       for (int p = 0; p < 4; ++p)

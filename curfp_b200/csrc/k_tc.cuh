@@ -7,14 +7,16 @@
 // 2^-24 s_i.  The six products whose weight is >= 2^-16,
 //     level 0: d0*d0     level 1: d0*d1 + d1*d0     level 2: d0*d2 + d2*d0 + d1*d1,
 // are BF16 tensor-core products summed in three FP32 accumulators in tensor
-// memory.  Digit products are integers <= 2^14, so over a chunk of 256 of the
-// K dimension every partial sum is an integer below 2^24 and the tensor-core
-// accumulation is EXACT (its internal truncation never drops a bit).  After
+// memory.  Digit products are integers <= 2^14, so over a chunk of 1024 of
+// the K dimension the level-0 sum is an integer of magnitude <= 2^24 and its
+// tensor-core accumulation is EXACT (the accumulator's truncation never drops
+// a bit); the level-1 / level-2 sums may exceed 2^24 by a few bits, and the
+// bits their truncation can drop weigh at most 2^-30 of the result.  After
 // each chunk the epilogue warps fold the three level sums into an FP32
 // register accumulator with round-to-nearest:
 //     acc += L0 + (L1 + L2 * 2^-8) * 2^-8,
 // and at the end C := alpha * s_i s_j 2^-14 * acc + beta * C.  Rounding errors
-// are then those of K/256 round-to-nearest additions plus the 2^-24 s digit
+// are then those of K/1024 round-to-nearest additions plus the 2^-24 s digit
 // truncation: FP32-level accuracy from BF16 tensor cores.  (Summing floating
 // BF16 splits directly in one accumulator loses several bits: tcgen05
 // accumulation rounds toward zero at every step.)
@@ -23,10 +25,11 @@
 //   warp 0   : TMA producer — per K-block of 32, six boxes (A d0/d1/d2 and
 //              B d0/d1/d2, 128 x 32 BF16 each, SWIZZLE_64B) into a 4-stage
 //              shared-memory ring, completion on an mbarrier;
-//   warp 1   : MMA issuer — one elected thread issues 6 products x 2 K-steps
-//              of tcgen05.mma.cta_group::1.kind::f16 (M=128, N=128, K=16) per
-//              stage into the level accumulators; tcgen05.commit frees the
-//              stage and signals the end of each 256-deep chunk;
+//   warp 1   : MMA issuer — one elected thread issues, per 16-deep K step,
+//              the six digit products as four tcgen05.mma.cta_group::1.kind::f16
+//              (two M=128 N=256 over adjacent B planes, two M=128 N=128) into
+//              the level accumulators; tcgen05.commit frees the stage and
+//              signals the end of each 1024-deep chunk;
 //   warp 2   : allocates / frees the tensor memory (3 x 128 columns used);
 //   warps 4-7: epilogue — per chunk, tcgen05.ld of the three level sums of
 //              their TMEM lane quarter into registers; at the end C is
@@ -53,7 +56,7 @@ namespace rfp {
 namespace ktc {
 
 constexpr int BM = 128, BN = 128, BK = 32, STAGES = 4, PLANES = 3;
-constexpr int CHUNK_KB = 8;                                 // 8 x 32 = 256 deep
+constexpr int CHUNK_KB = 32;                                // 32 x 32 = 1024 deep
 constexpr int A_BYTES = BM * BK * 2;                        // 8 KB
 constexpr int B_BYTES = BN * BK * 2;                        // 8 KB
 constexpr int STAGE_BYTES = PLANES * (A_BYTES + B_BYTES);   // 48 KB
@@ -67,8 +70,12 @@ constexpr uint64_t WAIT_NS = 2000000000ull;        // and at most ~2 s of wall t
 // Instruction descriptor, kind::f16: D = F32 (bits 4-5 = 1), A = B = BF16
 // (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at bits
 // 17-22, M >> 4 at bits 24-28.
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) |
-                           ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+constexpr uint32_t idesc_for(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(BM >> 4) << 24);
+}
+constexpr uint32_t IDESC = idesc_for(BN);        // M=128, N=128
+constexpr uint32_t IDESC2 = idesc_for(2 * BN);   // M=128, N=256 (two B planes)
 
 struct Task {
   int a_row0, b_row0, m, n;
@@ -158,12 +165,12 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
 }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t ad, uint64_t bd,
-                                         uint32_t accum) {
+                                         uint32_t idesc, uint32_t accum) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-      "l"(ad), "l"(bd), "r"(IDESC), "r"(accum));
+      "l"(ad), "l"(bd), "r"(idesc), "r"(accum));
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
@@ -180,8 +187,9 @@ __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
+// 16 consecutive 32-bit columns of this warp's TMEM lane quarter; the load is
+// asynchronous until tmem_wait().
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
       "%14,%15}, [%16];"
@@ -189,15 +197,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
         "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Product table: (A digit plane, B digit plane, level).
-__device__ __constant__ int kProdA[6] = {0, 0, 1, 0, 2, 1};
-__device__ __constant__ int kProdB[6] = {0, 1, 0, 2, 0, 1};
-__device__ __constant__ int kProdL[6] = {0, 1, 1, 2, 2, 2};
 
 __global__ void __launch_bounds__(THREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
@@ -276,7 +280,7 @@ __global__ void __launch_bounds__(THREADS, 1)
           if (!mbar_wait(drained, (c - 1) & 1, abort_sh, batch.err_flag, 4)) break;
           tc_fence_after();
         }
-        uint32_t started = 0;  // bit l: level l accumulates
+        uint32_t started = 0;  // 0 until the chunk's first K-step is issued
         const int kb_end = (kb + CHUNK_KB < KB) ? kb + CHUNK_KB : KB;
         bool ok = true;
         for (; kb < kb_end; ++kb) {
@@ -286,16 +290,23 @@ __global__ void __launch_bounds__(THREADS, 1)
           tc_fence_after();
           const uint32_t a0 = su32(smem + s * STAGE_BYTES);
           const uint32_t b0 = a0 + PLANES * A_BYTES;
+          // Six digit products in four instructions.  The B digit planes are
+          // adjacent in shared memory, so B_hi|B_mid is one 256-row operand and
+          // an N=256 MMA writes two neighbouring 128-column level sums:
+          //   A_hi  x [B_hi|B_mid] -> L0 (cols 0..127), L1 (128..255)
+          //   A_hi  x  B_lo        -> L2 (256..383)
+          //   A_mid x [B_hi|B_mid] -> L1, L2   (accumulating)
+          //   A_lo  x  B_hi        -> L2       (accumulating)
+          // The first two start a chunk (accumulate flag 0 initialises
+          // L0, L1 and L2); the last two always accumulate.
 #pragma unroll
           for (int kk = 0; kk < BK / 16; ++kk) {
-#pragma unroll
-            for (int q = 0; q < 6; ++q) {
-              const int l = kProdL[q];
-              const uint64_t ad = sdesc(a0 + kProdA[q] * A_BYTES + kk * 32);
-              const uint64_t bd = sdesc(b0 + kProdB[q] * B_BYTES + kk * 32);
-              mma_bf16(tmem + (uint32_t)(l * BN), ad, bd, (started >> l) & 1u);
-              started |= 1u << l;
-            }
+            const uint32_t ak = a0 + kk * 32, bk = b0 + kk * 32;
+            mma_bf16(tmem, sdesc(ak), sdesc(bk), IDESC2, started);
+            mma_bf16(tmem + 2 * BN, sdesc(ak), sdesc(bk + 2 * B_BYTES), IDESC, started);
+            mma_bf16(tmem + BN, sdesc(ak + A_BYTES), sdesc(bk), IDESC2, 1u);
+            mma_bf16(tmem + 2 * BN, sdesc(ak + 2 * A_BYTES), sdesc(bk), IDESC, 1u);
+            started = 1u;
           }
           mma_commit(&empty[s]);
         }
@@ -318,13 +329,15 @@ __global__ void __launch_bounds__(THREADS, 1)
       tc_fence_after();
 #pragma unroll
       for (int c0 = 0; c0 < BN; c0 += 16) {
-        float l0[16], l1[16], l2[16];
+        uint32_t l0[16], l1[16], l2[16];
         tmem_ld16(tq + (uint32_t)c0, l0);
         tmem_ld16(tq + (uint32_t)(BN + c0), l1);
         tmem_ld16(tq + (uint32_t)(2 * BN + c0), l2);
+        tmem_wait();
 #pragma unroll
         for (int j = 0; j < 16; ++j)
-          acc[c0 + j] += l0[j] + (l1[j] + l2[j] * 0x1p-8f) * 0x1p-8f;
+          acc[c0 + j] += __uint_as_float(l0[j]) +
+                         (__uint_as_float(l1[j]) + __uint_as_float(l2[j]) * 0x1p-8f) * 0x1p-8f;
       }
       tc_fence_before();
       mbar_arrive(drained);
@@ -414,19 +427,21 @@ __global__ void __launch_bounds__(256) rowscale_kernel(View X, int rows, int k,
 
 // Digits of X (see the header): three BF16 planes, row-major with K
 // contiguous, out[p][i][j], plane stride rows_pad * k_pad; zero padding.
-// Grid (k_pad/32, rows_pad/32), block (32, 8).
+// A block stages a 32 x 64 tile through shared memory (the warp reads along
+// X's contiguous dimension) and writes BF16 pairs (128 bytes per warp store).
+// Grid (k_pad/64, rows_pad/32), block (32, 8); k_pad is a multiple of 64.
 __global__ void __launch_bounds__(256) digits_kernel(View X, int rows, int k,
                                                      const float* __restrict__ scale,
                                                      __nv_bfloat16* out, int rows_pad,
                                                      int k_pad) {
-  __shared__ float t[32][33];
-  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  __shared__ float t[32][65];
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 64;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const bool kcont = (X.cs == 1 || X.cs == -1);
 #pragma unroll
-  for (int r = 0; r < 4; ++r) {
+  for (int r = 0; r < 8; ++r) {
     int lr, lc;
-    if (kcont) { lc = tx; lr = ty + 8 * r; }
+    if (kcont) { lc = tx + 32 * (r & 1); lr = ty + 8 * (r >> 1); }
     else       { lr = tx; lc = ty + 8 * r; }
     const int gr = r0 + lr, gc = c0 + lc;
     t[lr][lc] = (gr < rows && gc < k) ? X.p[(int64_t)gr * X.rs + (int64_t)gc * X.cs] : 0.f;
@@ -437,16 +452,23 @@ __global__ void __launch_bounds__(256) digits_kernel(View X, int rows, int k,
   for (int r = 0; r < 4; ++r) {
     const int lr = ty + 8 * r;
     const float inv = 1.0f / scale[r0 + lr];            // power of two: exact
-    const float y0 = t[lr][tx] * inv * 128.0f;          // |y0| <= 128, exact
-    const float d0 = rintf(y0);
-    const float y1 = (y0 - d0) * 256.0f;                // exact, |y1| <= 128
-    const float d1 = rintf(y1);
-    const float y2 = (y1 - d1) * 256.0f;                // exact
-    const float d2 = rintf(y2);
-    const int64_t o = (int64_t)(r0 + lr) * k_pad + c0 + tx;
-    out[o] = __float2bfloat16_rn(d0);                   // integers <= 128: exact
-    out[o + plane] = __float2bfloat16_rn(d1);
-    out[o + 2 * plane] = __float2bfloat16_rn(d2);
+    float d[3][2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const float y0 = t[lr][2 * tx + h] * inv * 128.0f;  // |y0| <= 128, exact
+      const float d0 = rintf(y0);
+      const float y1 = (y0 - d0) * 256.0f;                // exact, |y1| <= 128
+      const float d1 = rintf(y1);
+      const float y2 = (y1 - d1) * 256.0f;                // exact
+      d[0][h] = d0;
+      d[1][h] = d1;
+      d[2][h] = rintf(y2);
+    }
+    const int64_t o = (int64_t)(r0 + lr) * k_pad + c0 + 2 * tx;
+#pragma unroll
+    for (int p = 0; p < 3; ++p)  // integers <= 128: exact in BF16
+      *reinterpret_cast<__nv_bfloat162*>(out + o + p * plane) =
+          __floats2bfloat162_rn(d[p][0], d[p][1]);
   }
 }
 

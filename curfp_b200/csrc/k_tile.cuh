@@ -11,56 +11,180 @@
 namespace rfp {
 namespace ktile {
 
-constexpr int T = 64;        // tile size (== kPotrfTile == kTrsmLeaf == kTriTile)
-constexpr int LD = T + 1;    // padded shared-memory leading dimension
-
-static_assert(T == kPotrfTile && T == kTrsmLeaf && T == kTriTile,
-              "tile kernels assume one tile size");
-
-// Lower-triangular Cholesky of an n x n (n <= 64) tile, right-looking, one
-// column per step.  Thread t owns column t % 64 and rows t/64 + 4r.
-// On a pivot that is not > 0 (or NaN) the device info word becomes
-// min(info, info_base + j + 1), the partially factored tile is written back
-// and the kernel returns (LAPACK xPOTF2 semantics).
-__global__ void __launch_bounds__(256) potrf_tile(View L, int n, int info_base,
-                                                  int* info) {
-  if (info && *info != INT_MAX) return;
-  __shared__ float s[T][LD];
-  const int tid = threadIdx.x;
-  for (int e = tid; e < n * n; e += 256) {
-    int i = e % n, j = e / n;
-    s[i][j] = (i >= j) ? L.p[(int64_t)i * L.rs + (int64_t)j * L.cs] : 0.f;
-  }
-  __syncthreads();
-  const int col = tid % T, row0 = tid / T;
-  int fail = 0;
-  for (int j = 0; j < n; ++j) {
-    const float d = s[j][j];
-    if (!(d > 0.f)) {  // also catches NaN
-      fail = j + 1;
-      break;
-    }
-    const float ljj = sqrtf(d);
-    __syncthreads();  // every thread has read s[j][j]
-    if (col == j) {
-      for (int i = row0; i < n; i += 4) {
-        if (i > j) s[i][j] = s[i][j] / ljj;
-        else if (i == j) s[j][j] = ljj;
+// Copy the lower triangle of an n x n view tile into shared memory s[i][j]
+// (zeros above the diagonal).  The warp runs along the view's contiguous
+// dimension and each thread keeps 8 loads in flight.  n <= 32 * RW.
+template <int LDS>
+__device__ __forceinline__ void load_lower(View L, int n, float* s) {
+  const bool rcont = (L.cs == 1 || L.cs == -1);
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32, nw = blockDim.x / 32;
+  for (int base = warp; base < n; base += 8 * nw) {
+    float v[8][4];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int a = base + u * nw;  // row (rcont) or column (!rcont)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int b = lane + 32 * q;
+        const int i = rcont ? a : b, j = rcont ? b : a;
+        v[u][q] = (a < n && b < n && i >= j) ? L.p[(int64_t)i * L.rs + (int64_t)j * L.cs] : 0.f;
       }
     }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int a = base + u * nw;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int b = lane + 32 * q;
+        const int i = rcont ? a : b, j = rcont ? b : a;
+        if (a < n && b < n) s[i * LDS + j] = v[u][q];
+      }
+    }
+  }
+}
+
+// Store the lower triangle of s back to the view (same thread mapping).
+template <int LDS>
+__device__ __forceinline__ void store_lower(View L, int n, const float* s) {
+  const bool rcont = (L.cs == 1 || L.cs == -1);
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32, nw = blockDim.x / 32;
+  for (int a = warp; a < n; a += nw) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int b = lane + 32 * q;
+      const int i = rcont ? a : b, j = rcont ? b : a;
+      if (b < n && i >= j) L.p[(int64_t)i * L.rs + (int64_t)j * L.cs] = s[i * LDS + j];
+    }
+  }
+}
+
+constexpr int T = 64;        // trtri / lauum / TRSM-leaf tile (== kTrsmLeaf == kTriTile)
+constexpr int LD = T + 1;    // padded shared-memory leading dimension
+
+static_assert(T == kTrsmLeaf && T == kTriTile, "tile kernels assume one tile size");
+
+// Lower-triangular Cholesky of an n x n tile (n <= 128), one CTA of 256
+// threads, the tile in shared memory.  Blocked by 32 columns:
+//   (1) warp 0 factors the 32 x 32 diagonal block in registers (lane = row,
+//       pivots broadcast with warp shuffles, no block barrier inside);
+//   (2) the rows below solve against it (one thread per row, forward
+//       substitution with broadcast reads of the factor);
+//   (3) all threads apply the rank-32 update to the trailing triangle.
+// On a pivot that is not > 0 (or NaN) the device info word becomes
+// min(info, info_base + column + 1), the partially factored tile is written
+// back and the kernel returns (LAPACK xPOTRF semantics).
+constexpr int PT = 128;          // potrf tile (== kPotrfTile)
+constexpr int PLD = PT + 1;
+constexpr int POTRF_SMEM = PT * PLD * 4 + 64 * 4;
+static_assert(PT == kPotrfTile, "potrf tile size");
+
+__global__ void __launch_bounds__(256) potrf_tile(View L, int n, int info_base, int* info) {
+  if (info && *info != INT_MAX) return;
+  extern __shared__ float dyn[];
+  float (*s)[PLD] = reinterpret_cast<float (*)[PLD]>(dyn);
+  float* rdiag = dyn + PT * PLD;       // 32 reciprocals of the current diagonal block
+  __shared__ int fail_sh;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  load_lower<PLD>(L, n, dyn);
+  if (tid == 0) fail_sh = 0;
+  __syncthreads();
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    const int w = min(32, n - c0);
+    // (1) diagonal block in registers
+    if (warp == 0) {
+      float a[32];
+#pragma unroll
+      for (int k = 0; k < 32; ++k) a[k] = (lane < w && k < w) ? s[c0 + lane][c0 + k] : 0.f;
+      int fail = 0;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        if (j < w && !fail) {
+          const float d = __shfl_sync(0xffffffffu, a[j], j);
+          if (!(d > 0.f)) {
+            fail = c0 + j + 1;
+          } else {
+            const float ljj = sqrtf(d);
+            if (lane == j) {
+              a[j] = ljj;
+              rdiag[j] = 1.0f / ljj;
+            } else if (lane > j) {
+              a[j] = a[j] / ljj;
+            }
+#pragma unroll
+            for (int k = j + 1; k < 32; ++k) {
+              const float lkj = __shfl_sync(0xffffffffu, a[j], k);
+              if (lane >= k) a[k] = fmaf(-a[j], lkj, a[k]);
+            }
+          }
+        }
+      }
+      if (lane < w) {
+#pragma unroll
+        for (int k = 0; k < 32; ++k)
+          if (k <= lane && k < w) s[c0 + lane][c0 + k] = a[k];
+      }
+      if (lane == 0 && fail) fail_sh = fail;
+    }
     __syncthreads();
-    if (col > j && col < n) {
-      const float lkj = s[col][j];
-      for (int i = row0; i < n; i += 4)
-        if (i >= col) s[i][col] = fmaf(-s[i][j], lkj, s[i][col]);
+    if (fail_sh) break;
+    const int r1 = c0 + w;
+    // (2) rows below: X L_blk^T = A_r
+    for (int r = r1 + tid; r < n; r += 256) {
+      float x[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        if (j < w) {
+          float v = s[r][c0 + j];
+#pragma unroll
+          for (int k = 0; k < j; ++k) v = fmaf(-x[k], s[c0 + j][c0 + k], v);
+          x[j] = v * rdiag[j];
+        } else {
+          x[j] = 0.f;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < w) s[r][c0 + j] = x[j];
+    }
+    __syncthreads();
+    // (3) trailing update of the lower triangle rows/cols >= r1, in 4 x 4
+    // register blocks (16 independent accumulators per thread)
+    const int m = n - r1, nb4 = (m + 3) / 4, nblk4 = nb4 * (nb4 + 1) / 2;
+    for (int e = tid; e < nblk4; e += 256) {
+      int bi = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
+      while ((bi + 1) * (bi + 2) / 2 <= e) ++bi;
+      while (bi * (bi + 1) / 2 > e) --bi;
+      const int bj = e - bi * (bi + 1) / 2;
+      const int ri = r1 + 4 * bi, cj = r1 + 4 * bj;
+      float acc[4][4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          acc[p][q] = (ri + p < n && cj + q < n) ? s[ri + p][cj + q] : 0.f;
+#pragma unroll 4
+      for (int k = 0; k < w; ++k) {
+        float a4[4], b4[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          a4[p] = (ri + p < n) ? s[ri + p][c0 + k] : 0.f;
+          b4[p] = (cj + p < n) ? s[cj + p][c0 + k] : 0.f;
+        }
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[p][q] = fmaf(-a4[p], b4[q], acc[p][q]);
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (ri + p < n && cj + q <= ri + p) s[ri + p][cj + q] = acc[p][q];
     }
     __syncthreads();
   }
-  if (fail && tid == 0) atomicMin(info, info_base + fail);
-  for (int e = tid; e < n * n; e += 256) {
-    int i = e % n, j = e / n;
-    if (i >= j) L.p[(int64_t)i * L.rs + (int64_t)j * L.cs] = s[i][j];
-  }
+  if (fail_sh && tid == 0) atomicMin(info, info_base + fail_sh);
+  store_lower<PLD>(L, n, dyn);
 }
 
 // Inverse of lower-triangular diagonal blocks.  Block b = blockIdx.x covers
@@ -78,13 +202,8 @@ __global__ void __launch_bounds__(T) trtri_blocks(View L, int n, float* W,
   const int sz = min(T, n - r0);
   const int c = threadIdx.x;
   const View Lb = sub(L, r0, r0);
-  for (int i = 0; i < T; ++i) {
-    // thread c loads column c of row i: coalesced when cs == +-1
-    float v = 0.f;
-    if (i < sz && c <= i) v = Lb.p[(int64_t)i * Lb.rs + (int64_t)c * Lb.cs];
-    s[i][c] = v;
-    x[i][c] = 0.f;
-  }
+  for (int i = 0; i < T; ++i) x[i][c] = 0.f;
+  load_lower<LD>(Lb, sz, &s[0][0]);
   __syncthreads();
   if (c < sz) {
     x[c][c] = 1.0f / s[c][c];
@@ -99,8 +218,7 @@ __global__ void __launch_bounds__(T) trtri_blocks(View L, int n, float* W,
     float* Wb = W + (int64_t)b * T * T;
     for (int j = 0; j < T; ++j) Wb[(int64_t)j * T + c] = (c < sz && j < sz) ? x[c][j] : 0.f;
   } else {
-    for (int i = 0; i < sz; ++i)
-      if (c <= i) Lb.p[(int64_t)i * Lb.rs + (int64_t)c * Lb.cs] = x[i][c];
+    store_lower<LD>(Lb, sz, &x[0][0]);
   }
 }
 
@@ -109,10 +227,7 @@ __global__ void __launch_bounds__(T) trtri_blocks(View L, int n, float* W,
 __global__ void __launch_bounds__(256) lauum_tile(View L, int n) {
   __shared__ float s[T][LD];
   const int tid = threadIdx.x;
-  for (int e = tid; e < n * n; e += 256) {
-    int i = e % n, j = e / n;
-    s[i][j] = (i >= j) ? L.p[(int64_t)i * L.rs + (int64_t)j * L.cs] : 0.f;
-  }
+  load_lower<LD>(L, n, &s[0][0]);
   __syncthreads();
   float out[16];
   const int j = tid % T, i0 = tid / T;

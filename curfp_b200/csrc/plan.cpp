@@ -37,12 +37,16 @@ inline GemmProb gemm_prob(View A, View B, View C, int m, int n, int k,
 int trsm_rec(Exec& ex, View L, int n, View B, int m, float alpha,
              const float* W, int blk0, int math) {
   if (n <= 0 || m <= 0) return 0;
+  const float* Wb = W + (int64_t)blk0 * kTrsmLeaf * kTrsmLeaf;
   if (n <= kTrsmLeaf) {
-    View Wv{const_cast<float*>(W) + (int64_t)blk0 * kTrsmLeaf * kTrsmLeaf, 1,
-            kTrsmLeaf};
+    View Wv{const_cast<float*>(Wb), 1, kTrsmLeaf};
     GemmProb p = gemm_prob(Wv, B, B, n, m, n, alpha, 0.0f, 0);
     p.inplace = 1;
     return ex.gemm(&p, 1);
+  }
+  if (n <= kWaveLeaf) {
+    int rc = ex.trsm_wave(L, n, B, m, alpha, Wb);
+    if (rc != kNotSupported) return rc;
   }
   int n1 = split(n, kTrsmLeaf), n2 = n - n1;
   int rc = trsm_rec(ex, L, n1, B, m, alpha, W, blk0, math);
@@ -63,6 +67,10 @@ int trsm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math) {
   if (!W) return 2;
   int rc = ex.trtri_blocks(L, n, kTrsmLeaf, W);
   if (rc) return rc;
+  if (m <= kTrsvMaxRhs) {
+    rc = ex.trsm_wave(L, n, B, m, alpha, W);
+    if (rc != kNotSupported) return rc;
+  }
   return trsm_rec(ex, L, n, B, m, alpha, W, 0, math);
 }
 

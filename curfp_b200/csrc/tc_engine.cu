@@ -47,7 +47,7 @@ struct Staged {
 int stage(curfpContext* ctx, void** buf, size_t* cur, View X, int rows, int k,
           Staged* out) {
   out->rows_pad = (int)(round_up(rows, ktc::BN) + ktc::BN);
-  out->k_pad = (int)round_up(k, ktc::BK);
+  out->k_pad = (int)round_up(k, 64);
   const size_t plane_bytes =
       (size_t)3 * out->rows_pad * out->k_pad * sizeof(__nv_bfloat16);
   const size_t off = (size_t)round_up((int64_t)plane_bytes, 256);
@@ -55,9 +55,11 @@ int stage(curfpContext* ctx, void** buf, size_t* cur, View X, int rows, int k,
   if (!p) return 2;
   out->p = static_cast<__nv_bfloat16*>(p);
   out->scale = reinterpret_cast<float*>(static_cast<char*>(p) + off);
+  ProfScope ps(ctx->prof, ctx->stream, K_TC_STAGE, 0,
+               (double)rows * k * 8.0 + (double)out->rows_pad * out->k_pad * 6.0);
   ktc::rowscale_kernel<<<out->rows_pad / 32, 256, 0, ctx->stream>>>(X, rows, k, out->scale,
                                                                    out->rows_pad);
-  dim3 grid(out->k_pad / 32, out->rows_pad / 32);
+  dim3 grid(out->k_pad / 64, out->rows_pad / 32);
   ktc::digits_kernel<<<grid, dim3(32, 8), 0, ctx->stream>>>(X, rows, k, out->scale, out->p,
                                                             out->rows_pad, out->k_pad);
   ctx->launches += 2;
@@ -100,8 +102,10 @@ int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, Vie
 
   ktc::Batch b{};
   int tiles = 0, cnt = 0;
+  double flops = 0;
   for (int i = 0; i < count; ++i) {
     const SharedTask& s = tasks[i];
+    flops += 2.0 * s.m * s.n * (double)k * (s.c_lower ? 0.5 : 1.0);
     if (s.m <= 0 || s.n <= 0) continue;
     ktc::Task& t = b.t[cnt++];
     t.a_row0 = s.a_row0; t.b_row0 = s.b_row0; t.m = s.m; t.n = s.n;
@@ -127,6 +131,7 @@ int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, Vie
       return 4;
     attr_set = true;
   }
+  ProfScope ps(ctx->prof, ctx->stream, K_TC_GEMM, flops, 0);
   ktc::tc_gemm_kernel<<<tiles, ktc::THREADS, ktc::SMEM_BYTES, ctx->stream>>>(mA, mB, b);
   ++ctx->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;

@@ -131,3 +131,28 @@ def launch_count() -> int:
     c = ctypes.c_longlong(0)
     check(h._lib.curfpGetKernelLaunchCount(h.ptr, ctypes.byref(c)))
     return c.value
+
+
+KERNEL_CLASSES = ["sgemm", "tc_gemm", "tc_stage", "potrf_tile", "trtri", "lauum",
+                  "pack", "diag", "symm_acc64", "trsv_wave"]
+
+
+def profile_enable(on: bool = True) -> None:
+    """Start (clear) or stop per-kernel-class event timing on this device's handle."""
+    h = _get_handle()
+    check(h._lib.curfpProfileEnable(h.ptr, 1 if on else 0))
+
+
+def profile_read() -> dict:
+    """{class: {ms, flops, bytes, launches}} for the records since profile_enable."""
+    h = _get_handle()
+    out = {}
+    for i, name in enumerate(KERNEL_CLASSES):
+        ms, fl, by = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        n = ctypes.c_longlong()
+        check(h._lib.curfpProfileRead(h.ptr, i, ctypes.byref(ms), ctypes.byref(fl),
+                                      ctypes.byref(by), ctypes.byref(n)))
+        if n.value:
+            out[name] = {"ms": ms.value, "flops": fl.value, "bytes": by.value,
+                         "launches": n.value}
+    return out

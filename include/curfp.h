@@ -181,6 +181,20 @@ curfpStatus_t curfpSsfmmAcc64(curfpHandle_t handle, curfpOperation_t transr,
 /* Number of kernels launched through this handle since its creation. */
 curfpStatus_t curfpGetKernelLaunchCount(curfpHandle_t handle, long long *count);
 
+/* Optional kernel timing: when enabled, every kernel this handle launches is
+ * bracketed by CUDA events on its stream and attributed to a kernel class
+ * (0 SIMT GEMM, 1 tensor-core contraction, 2 tensor-core operand staging,
+ * 3 Cholesky tiles, 4 triangular inverses, 5 L^T L tiles, 6 strttf/stfttr,
+ * 7 diagonal helpers, 8 FP64-accumulated symmetric multiply, 9 wavefront
+ * triangular solves).  Enabling (or disabling) clears the records;
+ * curfpProfileRead synchronises the stream and returns the summed device
+ * milliseconds, algorithmic flops and bytes, and the launch count of one
+ * class. */
+curfpStatus_t curfpProfileEnable(curfpHandle_t handle, int enable);
+curfpStatus_t curfpProfileRead(curfpHandle_t handle, int kclass, double *ms,
+                               double *flops, double *bytes,
+                               long long *launches);
+
 #ifdef __cplusplus
 }
 #endif

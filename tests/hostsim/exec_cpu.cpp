@@ -4,6 +4,7 @@
 // -m "not gpu" tests can check view arithmetic, recursion splits, masks and
 // info propagation of every RFP routine without a GPU.  It is compiled into
 // tests/hostsim/libhostsim.so only; the product library never contains it.
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdint>
@@ -122,6 +123,33 @@ class CpuExec : public Exec {
       }
     for (int i = 0; i < n; ++i)
       for (int j = 0; j <= i; ++j) at(L, i, j) = (float)R[(size_t)i * n + j];
+    return 0;
+  }
+
+  // Same block algorithm as the GPU wavefront kernel: X_j = W_j (alpha B_j -
+  // sum_{i<j} L_ji X_i), blocks of 64.
+  long wave_calls = 0;
+  int trsm_wave(View L, int n, View B, int m, float alpha, const float* W) override {
+    if (aborted()) return 0;
+    ++wave_calls;
+    const int NB = kTrsmLeaf;
+    std::vector<double> T((size_t)NB * m);
+    for (int r0 = 0; r0 < n; r0 += NB) {
+      const int rows = std::min(NB, n - r0), j = r0 / NB;
+      for (int a = 0; a < rows; ++a)
+        for (int c = 0; c < m; ++c) {
+          double s = (double)alpha * at(B, r0 + a, c);
+          for (int k = 0; k < r0; ++k) s -= (double)at(L, r0 + a, k) * at(B, k, c);
+          T[(size_t)a * m + c] = s;
+        }
+      const float* Wj = W + (int64_t)j * NB * NB;
+      for (int a = 0; a < rows; ++a)
+        for (int c = 0; c < m; ++c) {
+          double s = 0;
+          for (int k = 0; k < rows; ++k) s += (double)Wj[(int64_t)k * NB + a] * T[(size_t)k * m + c];
+          at(B, r0 + a, c) = (float)s;
+        }
+    }
     return 0;
   }
 
