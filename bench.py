@@ -5,7 +5,7 @@ A ~ N(0,1)/sqrt(k), k = 1024, 64 right-hand sides B ~ N(0,1) -- synthetic and
 seeded, built on the device by the library's own ssfrk.
 One step = Cholesky of a fresh copy of C + solve of the 64 right-hand sides:
   headline (--math bf16x3, default): curfpSpftrfEx(split-BF16 tensor-core
-      updates) + curfpSpftrsRefine(FP64-residual refinement, <= 2 corrections);
+      updates) + curfpSpftrsRefine(FP64-residual refinement, one correction);
   also measured and reported beside it: the plain FP32 drop-in
       (curfpSpftrf + curfpSpftrs).
 Metric: Cholesky+solve TFLOP/s = (n^3/3 + n^2/2 + n/6 + 2 n^2 nrhs) / time.
@@ -391,7 +391,7 @@ def main():
     ap.add_argument("--n", type=int, default=32768)
     ap.add_argument("--k", type=int, default=1024)
     ap.add_argument("--nrhs", type=int, default=64)
-    ap.add_argument("--max-iter", type=int, default=2)
+    ap.add_argument("--max-iter", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-other", action="store_true")

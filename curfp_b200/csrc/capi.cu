@@ -55,6 +55,12 @@ inline int read_info(curfpHandle_t h, int* info, int* err) {
   return 1;
 }
 
+// Launch the FP64-accumulated symmetric multiply; when the row blocks alone
+// do not fill the GPU the column-block sum is split over gridDim.z with an
+// FP64 accumulator in workspace (atomic adds, rounded once by symm_finish).
+int symm_launch(curfpHandle_t h, const Geometry& g, const float* A, const float* X,
+                int64_t ldx, float* Y, int64_t ldy, int nrhs, float alpha, float beta);
+
 inline bool symm_attr() {
   static bool done = false;
   if (!done) {
@@ -106,6 +112,35 @@ curfpStatus_t pack(curfpHandle_t h, int transr, int lower, int n,
   return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
 }
 
+int symm_launch(curfpHandle_t h, const Geometry& g, const float* A, const float* X,
+                int64_t ldx, float* Y, int64_t ldy, int nrhs, float alpha, float beta) {
+  if (!symm_attr()) return 4;
+  const int n = g.n;
+  const int bx = (n + rfp::kref::TB - 1) / rfp::kref::TB, by = (nrhs + rfp::kref::TB - 1) / rfp::kref::TB;
+  int split = 1;
+  while ((int64_t)bx * by * split < 4 * 148 && split < 16 && bx / (split * 2) >= 4) split *= 2;
+  double* R = nullptr;
+  if (split > 1) {
+    R = static_cast<double*>(rfp::grow_buffer(h, &h->ws3, &h->ws3_bytes,
+                                              (size_t)n * nrhs * sizeof(double)));
+    if (!R) return 2;
+    if (cudaMemsetAsync(R, 0, (size_t)n * nrhs * sizeof(double), h->stream) != cudaSuccess)
+      return 4;
+  }
+  {
+    rfp::ProfScope ps(h->prof, h->stream, rfp::K_SYMM64, 2.0 * n * (double)n * nrhs,
+                      4.0 * n * (double)n);
+    rfp::kref::symm_acc64<<<dim3(bx, by, split), 256, rfp::kref::SYMM_SMEM, h->stream>>>(
+        g, A, X, ldx, Y, ldy, nrhs, alpha, beta, R);
+    ++h->launches;
+    if (R) {
+      rfp::kref::symm_finish<<<148 * 4, 256, 0, h->stream>>>(R, n, nrhs, Y, ldy, alpha, beta);
+      ++h->launches;
+    }
+  }
+  return ok_launch() ? 0 : 4;
+}
+
 }  // namespace
 
 extern "C" {
@@ -141,6 +176,8 @@ curfpStatus_t curfpDestroy(curfpHandle_t handle) {
   if (handle->stage) cudaFree(handle->stage);
   if (handle->stage2) cudaFree(handle->stage2);
   if (handle->ws2) cudaFree(handle->ws2);
+  if (handle->ws3) cudaFree(handle->ws3);
+  if (handle->tsv) cudaFree(handle->tsv);
   if (handle->d_info) cudaFree(handle->d_info);
   delete handle;
   return CURFP_STATUS_SUCCESS;
@@ -374,15 +411,8 @@ curfpStatus_t curfpSsfmmAcc64(curfpHandle_t handle, curfpOperation_t transr,
   if (ldx < n || ldy < n) return CURFP_STATUS_INVALID_VALUE;
   Geometry g = rfp::geometry(n, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER);
   dim3 grid((n + rfp::kref::TB - 1) / rfp::kref::TB, (nrhs + rfp::kref::TB - 1) / rfp::kref::TB);
-  {
-    rfp::ProfScope ps(handle->prof, handle->stream, rfp::K_SYMM64, 2.0 * n * (double)n * nrhs,
-                      4.0 * n * (double)n);
-    if (!symm_attr()) return CURFP_STATUS_EXECUTION_FAILED;
-    rfp::kref::symm_acc64<<<grid, 256, rfp::kref::SYMM_SMEM, handle->stream>>>(
-        g, A, X, ldx, Y, ldy, nrhs, *alpha, *beta);
-  }
-  ++handle->launches;
-  return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
+  (void)grid;
+  return status_of(symm_launch(handle, g, A, X, ldx, Y, ldy, nrhs, *alpha, *beta));
 }
 
 // Mixed-precision refinement around spftrs (see include/curfp.h).
@@ -412,21 +442,15 @@ curfpStatus_t curfpSpftrsRefine(curfpHandle_t handle, curfpOperation_t transr,
   int rc = rfp::plan::spftrs(ex, tr, lower, n, nrhs, factor, B, ldb);
   if (rc) return status_of(rc);
   Geometry g = rfp::geometry(n, tr, lower);
-  dim3 sgrid((n + rfp::kref::TB - 1) / rfp::kref::TB, (nrhs + rfp::kref::TB - 1) / rfp::kref::TB);
   float prev = INFINITY;
   for (int it = 0; it < max_iter; ++it) {
     // R := B0 - A X in FP64
     rfp::kref::copy_block<<<grid, 256, 0, st>>>(R, n, B0, n, n, nrhs);
-    {
-      rfp::ProfScope ps(handle->prof, st, rfp::K_SYMM64, 2.0 * n * (double)n * nrhs,
-                        4.0 * n * (double)n);
-      if (!symm_attr()) return CURFP_STATUS_EXECUTION_FAILED;
-      rfp::kref::symm_acc64<<<sgrid, 256, rfp::kref::SYMM_SMEM, st>>>(g, Aorig, B, ldb, R, n,
-                                                                    nrhs, -1.0f, 1.0f);
-    }
+    if ((rc = symm_launch(handle, g, Aorig, B, ldb, R, n, nrhs, -1.0f, 1.0f)))
+      return status_of(rc);
     cudaMemsetAsync(nrm, 0, sizeof(unsigned), st);
     rfp::kref::absmax<<<grid, 256, 0, st>>>(R, n, n, nrhs, nrm);
-    handle->launches += 3;
+    handle->launches += 2;
     if (!ok_launch()) return CURFP_STATUS_EXECUTION_FAILED;
     unsigned bits = 0;
     if (cudaMemcpyAsync(&bits, nrm, sizeof(unsigned), cudaMemcpyDeviceToHost, st) !=

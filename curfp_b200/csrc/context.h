@@ -26,6 +26,8 @@ struct curfpContext {
   size_t stage2_bytes = 0;
   void* ws2 = nullptr;     // refinement scratch (saved RHS, residual)
   size_t ws2_bytes = 0;
+  void* ws3 = nullptr;     // FP64 accumulator of split symmetric multiplies
+  size_t ws3_bytes = 0;
   long long launches = 0;  // kernels launched through this handle
   rfp::Profiler prof;      // optional per-class event timing
   void* tsv = nullptr;     // wavefront solve flags / tickets

@@ -49,6 +49,7 @@ constexpr int kTriTile = 64;     // trtri / lauum tiles
 constexpr int kTrmmLeaf = 64;    // TRMM leaves (masked in-place multiply)
 constexpr int kTrsvMaxRhs = 512; // wavefront solve for at most this many RHS
 constexpr int kWaveLeaf = 512;   // recursive TRSM hands blocks <= this to the wavefront solve
+constexpr int kWaveLeafWide = 512;  // ... when there are more than 4 * kTrsvMaxRhs RHS
 constexpr int kNotSupported = -1;
 
 class Exec {

@@ -383,13 +383,24 @@ __global__ void __launch_bounds__(256) rowscale_kernel(View X, int rows, int k,
   const bool kcont = (X.cs == 1 || X.cs == -1);
   float m[4] = {0.f, 0.f, 0.f, 0.f};
   if (kcont) {
-    // warp ty handles rows r0 + ty + 8 j; lanes stride over k
+    // warp ty handles rows r0 + ty + 8 j; lanes stride over k, 8 loads in
+    // flight per lane
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int r = r0 + ty + 8 * j;
-      if (r < rows)
-        for (int c = tx; c < k; c += 32)
-          m[j] = fmaxf(m[j], fabsf(X.p[(int64_t)r * X.rs + (int64_t)c * X.cs]));
+      if (r < rows) {
+        const float* row = X.p + (int64_t)r * X.rs;
+        for (int c = tx; c < k; c += 256) {
+          float v[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int cc = c + 32 * u;
+            v[u] = cc < k ? fabsf(row[(int64_t)cc * X.cs]) : 0.f;
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) m[j] = fmaxf(m[j], v[u]);
+        }
+      }
     }
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -399,11 +410,21 @@ __global__ void __launch_bounds__(256) rowscale_kernel(View X, int rows, int k,
     __syncthreads();
     if (threadIdx.x < 32) m[0] = red[0][threadIdx.x];
   } else {
-    // thread (tx, ty): row r0 + tx, k in ty, ty + 8, ...
+    // thread (tx, ty): row r0 + tx, k in ty, ty + 8, ...; 8 loads in flight
     const int r = r0 + tx;
-    if (r < rows)
-      for (int c = ty; c < k; c += 8)
-        m[0] = fmaxf(m[0], fabsf(X.p[(int64_t)r * X.rs + (int64_t)c * X.cs]));
+    if (r < rows) {
+      const float* row = X.p + (int64_t)r * X.rs;
+      for (int c = ty; c < k; c += 64) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int cc = c + 8 * u;
+          v[u] = cc < k ? fabsf(row[(int64_t)cc * X.cs]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) m[0] = fmaxf(m[0], v[u]);
+      }
+    }
     red[ty][tx] = m[0];
     __syncthreads();
     if (threadIdx.x < 32) {

@@ -103,13 +103,13 @@ __global__ void __launch_bounds__(256) potrf_tile(View L, int n, int info_base, 
           if (!(d > 0.f)) {
             fail = c0 + j + 1;
           } else {
-            const float ljj = sqrtf(d);
-            if (lane == j) {
-              a[j] = ljj;
-              rdiag[j] = 1.0f / ljj;
-            } else if (lane > j) {
-              a[j] = a[j] / ljj;
-            }
+            // 1/sqrt(d) from rsqrtf refined by one Newton-Raphson step for
+            // y = x^-1/2 (y <- y (3 - d y^2) / 2); the column is scaled by
+            // multiplication, branch-free across the warp.
+            float r = rsqrtf(d);
+            r = r * fmaf(-0.5f * d * r, r, 1.5f);
+            a[j] = (lane == j) ? d * r : (lane > j ? a[j] * r : a[j]);
+            if (lane == j) rdiag[j] = r;
 #pragma unroll
             for (int k = j + 1; k < 32; ++k) {
               const float lkj = __shfl_sync(0xffffffffu, a[j], k);

@@ -44,7 +44,10 @@ int trsm_rec(Exec& ex, View L, int n, View B, int m, float alpha,
     p.inplace = 1;
     return ex.gemm(&p, 1);
   }
-  if (n <= kWaveLeaf) {
+  // Few right-hand sides: the whole block goes to the wavefront solve (its
+  // chain is short relative to the work).  Many right-hand sides: small
+  // leaves, so that most of the work is in the (tensor-core) GEMM updates.
+  if (n <= (m <= kTrsvMaxRhs * 4 ? kWaveLeaf : kWaveLeafWide)) {
     int rc = ex.trsm_wave(L, n, B, m, alpha, Wb);
     if (rc != kNotSupported) return rc;
   }
