@@ -51,7 +51,7 @@ class CudaExec : public Exec {
                   int math) override;
   int trsm_wave(View L, int n, View B, int m, float alpha, const float* W) override;
 
- private:
+ protected:
   curfpContext* ctx_;
   const int* abort_;
 };
@@ -64,6 +64,10 @@ void* grow_buffer(curfpContext* ctx, void** buf, size_t* cur, size_t bytes);
 // (brows x k) FP32 views; B.p == nullptr means B is A.
 int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, View B,
                 int brows, int k, const SharedTask* tasks, int count);
+// The wavefront solve with a caller-provided flag buffer of sync_words words
+// (cleared here on the stream); no allocation.
+int launch_trsm_wave_fixed(curfpContext* ctx, const int* abort_flag, View L, int n, View B,
+                           int m, float alpha, const float* W, int* sync, size_t sync_words);
 // Whether a contraction of this size goes to the tensor-core path.
 bool tc_worthwhile(int m, int n, int k);
 

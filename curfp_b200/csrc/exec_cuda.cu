@@ -202,4 +202,21 @@ int CudaExec::trsm_wave(View L, int n, View B, int m, float alpha, const float* 
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
+int launch_trsm_wave_fixed(curfpContext* ctx, const int* abort_flag, View L, int n, View B,
+                           int m, float alpha, const float* W, int* sync, size_t sync_words) {
+  if (n <= 0 || m <= 0) return 0;
+  const int nblk = (n + ktrsv::NB - 1) / ktrsv::NB, nchunk = (m + ktrsv::NB - 1) / ktrsv::NB;
+  const size_t words = 1 + (size_t)nblk * nchunk;
+  if (words > sync_words) return 3;
+  if (cudaMemsetAsync(sync, 0, words * 4, ctx->stream) != cudaSuccess) return 4;
+  if (cudaFuncSetAttribute(ktrsv::trsm_wave, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           ktrsv::SMEM) != cudaSuccess)
+    return 4;
+  ProfScope ps(ctx->prof, ctx->stream, K_TRSV, (double)n * n * m, (double)n * n * 2.0);
+  ktrsv::trsm_wave<<<nblk * nchunk, 256, ktrsv::SMEM, ctx->stream>>>(L, n, B, m, alpha, W, sync,
+                                                                    ctx->d_info + 1, abort_flag);
+  ++ctx->launches;
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
 }  // namespace rfp

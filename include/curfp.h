@@ -178,6 +178,21 @@ curfpStatus_t curfpSsfmmAcc64(curfpHandle_t handle, curfpOperation_t transr,
                               const float *X, int ldx, const float *beta,
                               float *Y, int ldy);
 
+/* curfpSpftrs without any device allocation on the call path; no
+ * counterpart in the reference.  For callers that cannot let the library
+ * allocate device memory while they run (their GPU memory is owned by
+ * another allocator, or a cudaMalloc's possible synchronisation or failure
+ * is not acceptable in their loop).  The solve's scratch (inverted diagonal
+ * blocks and wavefront flags) lives in one static device array of
+ * 2 MiB + 4 KiB that each GPU loading the library keeps until exit.
+ * Limits: n <= 16384, nrhs <= 512 (larger sizes return
+ * CURFP_STATUS_INVALID_VALUE).  The array's device address is fetched on the
+ * first call per device (make that call before any stream capture).  All
+ * calls share the array: calls that overlap on the GPU race. */
+curfpStatus_t curfpSpftrsNoAlloc(curfpHandle_t handle, curfpOperation_t transr,
+                                 curfpFillMode_t uplo, int n, int nrhs,
+                                 const float *A, float *B, int ldb);
+
 /* Number of kernels launched through this handle since its creation. */
 curfpStatus_t curfpGetKernelLaunchCount(curfpHandle_t handle, long long *count);
 
