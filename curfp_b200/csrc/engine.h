@@ -22,7 +22,12 @@ struct GemmProb {
   int m, n, k, k2;
   float alpha, beta;
   int c_lower;  // write only C(i,j) with i >= j (tiles above the diagonal skipped)
-  int a_lower;  // treat A(i,kk) as 0 for kk > i (product 1 only)
+  // Triangular operands: 0 = full, 1 = lower (incl. diagonal), 2 = upper
+  // (incl. diagonal); elements outside are treated as 0 and never read.
+  // For A (m x k): lower keeps kk <= i, upper kk >= i.  For B (k x n): lower
+  // keeps kk >= j, upper kk <= j.  a_tri/b_tri apply to product 1,
+  // a2_tri/b2_tri to product 2.
+  int a_tri, b_tri, a2_tri, b2_tri;
   int inplace;  // C aliases B: the executor must read all of B's column block
                 // before writing it (the planner guarantees m <= inplace_rows())
   int math;     // 0 = FP32 FMA, 1 = split-BF16 tensor cores (engine may ignore
@@ -95,7 +100,8 @@ class Exec {
       g.C = t[i].C;
       g.m = t[i].m; g.n = t[i].n; g.k = k; g.k2 = 0;
       g.alpha = t[i].alpha; g.beta = t[i].beta;
-      g.c_lower = t[i].c_lower; g.a_lower = 0; g.inplace = 0;
+      g.c_lower = t[i].c_lower; g.inplace = 0;
+      g.a_tri = g.b_tri = g.a2_tri = g.b2_tri = 0;
       g.math = math;
     }
     return gemm(p, count);
@@ -133,6 +139,27 @@ int spftrf(Exec& ex, int transr, int lower, int n, float* A, int math = 0);
 int spftrs(Exec& ex, int transr, int lower, int n, int nrhs, const float* A,
            float* B, int ldb);
 int spftri(Exec& ex, int transr, int lower, int n, float* A);
+
+// Building blocks of the adjoints, on the logical lower factor L held in an
+// RFP array (all 8 variants):
+// L X = alpha B (trans = 0) or L^T X = alpha B (trans = 1), B dense n x m.
+int rfp_trsm(Exec& ex, int transr, int lower, int n, const float* L, int trans, View B,
+             int m, float alpha, int math = 0);
+// B := L^T B (B dense n x m).
+int rfp_trmm_t(Exec& ex, int transr, int lower, int n, const float* L, View B, int m);
+// D(i,j) := (L^T Lbar)(i,j) for i >= j (D dense n x n view; upper part
+// untouched); L and Lbar in RFP with the same variant.
+int rfp_ltl(Exec& ex, int transr, int lower, int n, const float* L, const float* Lbar,
+            View D);
+// Lower triangle of the logical matrix C (RFP): C := alpha (A1 B1 + A2 B2)
+// + beta C with A1, A2 n x k and B1, B2 k x n dense views.
+int rfp_gemm_lower2(Exec& ex, int transr, int lower, int n, float* C, View A1, View B1,
+                    View A2, View B2, int k, float alpha, float beta);
+// Y := alpha (G_L + G_L^T) X + beta Y where G_L is the stored lower triangle
+// (diagonal included, so the diagonal counts twice) of the RFP array G; X, Y
+// dense n x m views.
+int rfp_symm_dbl(Exec& ex, int transr, int lower, int n, const float* G, View X, View Y,
+                 int m, float alpha, float beta);
 
 }  // namespace plan
 }  // namespace rfp

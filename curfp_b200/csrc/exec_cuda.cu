@@ -60,7 +60,8 @@ int launch_gemm(const GemmProb* p, int count, const int* abort_flag,
     q.C = g.C.p; q.c_rs = g.C.rs; q.c_cs = g.C.cs;
     q.m = g.m; q.n = g.n; q.k = g.k; q.k2 = g.k2;
     q.alpha = g.alpha; q.beta = g.beta;
-    q.c_lower = g.c_lower; q.a_lower = g.a_lower;
+    q.c_lower = g.c_lower;
+    q.a_tri = g.a_tri; q.b_tri = g.b_tri; q.a2_tri = g.a2_tri; q.b2_tri = g.b2_tri;
     q.tiles_m = (g.m + BM - 1) / BM;
     q.tiles_n = (g.n + BN - 1) / BN;
     if (g.inplace && q.tiles_m != 1) return 3;  // planner contract
@@ -116,7 +117,7 @@ int CudaExec::gemm_shared(View X, int rows, int k, const SharedTask* t, int coun
 int CudaExec::gemm(const GemmProb* p, int count) {
   if (count <= 0) return 0;
   if (count > kMaxBatch) return 3;
-  if (count == 1 && p[0].math && !p[0].inplace && !p[0].a_lower && p[0].k2 == 0 &&
+  if (count == 1 && p[0].math && !p[0].inplace && !p[0].a_tri && !p[0].b_tri && p[0].k2 == 0 &&
       tc_worthwhile(p[0].m, p[0].n, p[0].k)) {
     const GemmProb& g = p[0];
     View A = g.A, Bt = tr(g.B);  // A: m x k, Bt: n x k

@@ -36,7 +36,8 @@ struct Prob {
   float* C; int64_t c_rs, c_cs;
   int m, n, k, k2;
   float alpha, beta;
-  int c_lower, a_lower;
+  int c_lower;
+  int a_tri, b_tri, a2_tri, b2_tri;  // 0 full, 1 lower, 2 upper (incl. diagonal)
   int tiles_m, tiles_n;
   int tile_begin;
 };
@@ -95,7 +96,7 @@ __device__ __forceinline__ void load_stage(Smem<BM, BN>& sm, int buf,
                                            int64_t a_cs, const float* B,
                                            int64_t b_rs, int64_t b_cs, int m,
                                            int n, int k, int m0, int n0,
-                                           int k0, int a_lower) {
+                                           int k0, int a_tri, int b_tri) {
   const int tid = threadIdx.x;
   constexpr int LA = BM * kBK / kThreads;
   constexpr int LB = BN * kBK / kThreads;
@@ -107,7 +108,7 @@ __device__ __forceinline__ void load_stage(Smem<BM, BN>& sm, int buf,
     if (a_mcont) { i = e % BM; kk = e / BM; }
     else         { i = e / kBK; kk = e % kBK; }
     int gi = m0 + i, gk = k0 + kk;
-    bool ok = gi < m && gk < k && (!a_lower || gk <= gi);
+    bool ok = gi < m && gk < k && (a_tri != 1 || gk <= gi) && (a_tri != 2 || gk >= gi);
     const float* src = ok ? A + (int64_t)gi * a_rs + (int64_t)gk * a_cs : A;
     cp_async4(&sm.a[buf][kk][i], src, ok);
   }
@@ -119,7 +120,7 @@ __device__ __forceinline__ void load_stage(Smem<BM, BN>& sm, int buf,
     if (b_ncont) { j = e % BN; kk = e / BN; }
     else         { j = e / kBK; kk = e % kBK; }
     int gj = n0 + j, gk = k0 + kk;
-    bool ok = gj < n && gk < k;
+    bool ok = gj < n && gk < k && (b_tri != 1 || gk >= gj) && (b_tri != 2 || gk <= gj);
     const float* src = ok ? B + (int64_t)gk * b_rs + (int64_t)gj * b_cs : B;
     cp_async4(&sm.b[buf][kk][j], src, ok);
   }
@@ -157,10 +158,10 @@ __global__ void __launch_bounds__(kThreads, 2) sgemm_batch(const Batch batch) {
   auto issue = [&](int kt, int buf) {
     if (kt < kt1)
       load_stage<BM, BN>(sm, buf, P.A, P.a_rs, P.a_cs, P.B, P.b_rs, P.b_cs,
-                         P.m, P.n, P.k, m0, n0, kt * kBK, P.a_lower);
+                         P.m, P.n, P.k, m0, n0, kt * kBK, P.a_tri, P.b_tri);
     else
       load_stage<BM, BN>(sm, buf, P.A2, P.a2_rs, P.a2_cs, P.B2, P.b2_rs,
-                         P.b2_cs, P.m, P.n, P.k2, m0, n0, (kt - kt1) * kBK, 0);
+                         P.b2_cs, P.m, P.n, P.k2, m0, n0, (kt - kt1) * kBK, P.a2_tri, P.b2_tri);
   };
 
   if (ktiles > 0) {

@@ -29,7 +29,8 @@ inline GemmProb gemm_prob(View A, View B, View C, int m, int n, int k,
   p.A2 = A; p.B2 = B;
   p.m = m; p.n = n; p.k = k; p.k2 = 0;
   p.alpha = alpha; p.beta = beta;
-  p.c_lower = 0; p.a_lower = 0; p.inplace = 0;
+  p.c_lower = 0; p.inplace = 0;
+  p.a_tri = p.b_tri = p.a2_tri = p.b2_tri = 0;
   p.math = math;
   return p;
 }
@@ -96,7 +97,7 @@ int trmm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math) {
   int leaf = kTrmmLeaf < ex.inplace_rows() ? kTrmmLeaf : ex.inplace_rows();
   if (n <= leaf) {
     GemmProb p = gemm_prob(L, B, B, n, m, n, alpha, 0.0f, 0);
-    p.a_lower = 1;
+    p.a_tri = 1;
     p.inplace = 1;
     return ex.gemm(&p, 1);
   }
@@ -282,6 +283,162 @@ int spftri(Exec& ex, int transr, int lower, int n, float* A) {
     if ((rc = trmm(ex, 1, 1, 1, V22, V21, g.n2, g.n1, 1.0f))) return rc;
   }
   return lauum_lower(ex, V22, g.n2);
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint building blocks
+// ---------------------------------------------------------------------------
+
+namespace {
+struct Blocks {
+  Geometry g;
+  View V11, V21, V22;
+};
+inline Blocks blocks(int transr, int lower, int n, const float* A) {
+  Blocks b;
+  b.g = geometry(n, transr, lower);
+  float* p = const_cast<float*>(A);
+  b.V11 = block_view(p, b.g.b11);
+  b.V21 = block_view(p, b.g.b21);
+  b.V22 = block_view(p, b.g.b22);
+  return b;
+}
+}  // namespace
+
+int rfp_trsm(Exec& ex, int transr, int lower, int n, const float* L, int trans, View B,
+             int m, float alpha, int math) {
+  Blocks b = blocks(transr, lower, n, L);
+  const int n1 = b.g.n1, n2 = b.g.n2;
+  View B1 = B, B2 = sub(B, n1, 0);
+  int rc;
+  if (!trans) {
+    if ((rc = trsm_lln(ex, b.V11, n1, B1, m, alpha, math))) return rc;
+    if (n1 > 0 && n2 > 0) {
+      GemmProb p = gemm_prob(b.V21, B1, B2, n2, m, n1, -1.0f, alpha, math);
+      if ((rc = ex.gemm(&p, 1))) return rc;
+    }
+    return trsm_lln(ex, b.V22, n2, B2, m, n1 > 0 ? 1.0f : alpha, math);
+  }
+  if ((rc = trsm(ex, 1, 1, 1, b.V22, B2, n2, m, alpha, math))) return rc;
+  if (n1 > 0 && n2 > 0) {
+    GemmProb p = gemm_prob(tr(b.V21), B2, B1, n1, m, n2, -1.0f, alpha, math);
+    if ((rc = ex.gemm(&p, 1))) return rc;
+  }
+  return trsm(ex, 1, 1, 1, b.V11, B1, n1, m, n2 > 0 ? 1.0f : alpha, math);
+}
+
+int rfp_trmm_t(Exec& ex, int transr, int lower, int n, const float* L, View B, int m) {
+  Blocks b = blocks(transr, lower, n, L);
+  const int n1 = b.g.n1, n2 = b.g.n2;
+  View B1 = B, B2 = sub(B, n1, 0);
+  int rc;
+  // (L^T B)_1 = L11^T B1 + L21^T B2 ; (L^T B)_2 = L22^T B2
+  if ((rc = trmm(ex, 1, 1, 1, b.V11, B1, n1, m, 1.0f))) return rc;
+  if (n1 > 0 && n2 > 0) {
+    GemmProb p = gemm_prob(tr(b.V21), B2, B1, n1, m, n2, 1.0f, 1.0f, 0);
+    if ((rc = ex.gemm(&p, 1))) return rc;
+  }
+  return trmm(ex, 1, 1, 1, b.V22, B2, n2, m, 1.0f);
+}
+
+int rfp_ltl(Exec& ex, int transr, int lower, int n, const float* L, const float* Lbar,
+            View D) {
+  Blocks a = blocks(transr, lower, n, L), c = blocks(transr, lower, n, Lbar);
+  const int n1 = a.g.n1, n2 = a.g.n2;
+  GemmProb p[3];
+  int cnt = 0;
+  // (L^T Lbar) lower blocks:
+  //   11: tril(L11^T Lbar11) + L21^T Lbar21     21: L22^T Lbar21
+  //   22: tril(L22^T Lbar22)
+  if (n1 > 0) {
+    GemmProb q = gemm_prob(tr(a.V11), c.V11, D, n1, n1, n1, 1.0f, 0.0f, 0);
+    q.a_tri = 2;  // L11^T is upper
+    q.b_tri = 1;  // Lbar11 is lower
+    if (n2 > 0) {
+      q.A2 = tr(a.V21);
+      q.B2 = c.V21;
+      q.k2 = n2;
+    }
+    q.c_lower = 1;
+    p[cnt++] = q;
+  }
+  if (n1 > 0 && n2 > 0) {
+    GemmProb q = gemm_prob(tr(a.V22), c.V21, sub(D, n1, 0), n2, n1, n2, 1.0f, 0.0f, 0);
+    q.a_tri = 2;
+    p[cnt++] = q;
+  }
+  if (n2 > 0) {
+    GemmProb q = gemm_prob(tr(a.V22), c.V22, sub(D, n1, n1), n2, n2, n2, 1.0f, 0.0f, 0);
+    q.a_tri = 2;
+    q.b_tri = 1;
+    q.c_lower = 1;
+    p[cnt++] = q;
+  }
+  return ex.gemm(p, cnt);
+}
+
+int rfp_gemm_lower2(Exec& ex, int transr, int lower, int n, float* C, View A1, View B1,
+                    View A2, View B2, int k, float alpha, float beta) {
+  Blocks c = blocks(transr, lower, n, C);
+  const int n1 = c.g.n1, n2 = c.g.n2;
+  View Cb[3] = {c.V11, c.V21, c.V22};
+  const int r0[3] = {0, n1, n1}, c0[3] = {0, 0, n1};
+  const int dm[3] = {n1, n2, n2}, dn[3] = {n1, n1, n2};
+  GemmProb p[3];
+  int cnt = 0;
+  for (int b = 0; b < 3; ++b) {
+    if (dm[b] <= 0 || dn[b] <= 0) continue;
+    GemmProb q = gemm_prob(sub(A1, r0[b], 0), sub(B1, 0, c0[b]), Cb[b], dm[b], dn[b], k,
+                           alpha, beta, 0);
+    q.A2 = sub(A2, r0[b], 0);
+    q.B2 = sub(B2, 0, c0[b]);
+    q.k2 = k;
+    q.c_lower = (b != 1);
+    p[cnt++] = q;
+  }
+  return ex.gemm(p, cnt);
+}
+
+int rfp_symm_dbl(Exec& ex, int transr, int lower, int n, const float* G, View X, View Y,
+                 int m, float alpha, float beta) {
+  Blocks g = blocks(transr, lower, n, G);
+  const int n1 = g.g.n1, n2 = g.g.n2;
+  View X1 = X, X2 = sub(X, n1, 0), Y1 = Y, Y2 = sub(Y, n1, 0);
+  int rc;
+  // Y1 = a (G11_L + G11_L^T) X1 + a G21^T X2 + b Y1
+  // Y2 = a G21 X1 + a (G22_L + G22_L^T) X2 + b Y2
+  GemmProb p[2];
+  int cnt = 0;
+  if (n1 > 0) {
+    GemmProb q = gemm_prob(g.V11, X1, Y1, n1, m, n1, alpha, beta, 0);
+    q.a_tri = 1;
+    q.A2 = tr(g.V11);
+    q.B2 = X1;
+    q.k2 = n1;
+    q.a2_tri = 2;
+    p[cnt++] = q;
+  }
+  if (n2 > 0) {
+    GemmProb q = gemm_prob(g.V21, X1, Y2, n2, m, n1, alpha, beta, 0);
+    if (n1 == 0) q.k = 0;
+    q.A2 = g.V22;
+    q.B2 = X2;
+    q.k2 = n2;
+    q.a2_tri = 1;
+    p[cnt++] = q;
+  }
+  if ((rc = ex.gemm(p, cnt))) return rc;
+  cnt = 0;
+  if (n1 > 0 && n2 > 0) {
+    GemmProb q = gemm_prob(tr(g.V21), X2, Y1, n1, m, n2, alpha, 1.0f, 0);
+    p[cnt++] = q;
+  }
+  if (n2 > 0) {
+    GemmProb q = gemm_prob(tr(g.V22), X2, Y2, n2, m, n2, alpha, 1.0f, 0);
+    q.a_tri = 2;
+    p[cnt++] = q;
+  }
+  return ex.gemm(p, cnt);
 }
 
 }  // namespace plan

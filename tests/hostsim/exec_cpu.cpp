@@ -42,11 +42,14 @@ class CpuExec : public Exec {
       for (int j = 0; j < g.n; ++j)
         for (int i = 0; i < g.m; ++i) {
           double s = 0.0;
-          for (int k = 0; k < g.k; ++k) {
-            if (g.a_lower && k > i) continue;
-            s += (double)at(g.A, i, k) * (double)at(g.B, k, j);
-          }
-          for (int k = 0; k < g.k2; ++k) s += (double)at(g.A2, i, k) * (double)at(g.B2, k, j);
+          auto keep = [&](int at_, int bt_, int k) {
+            return (at_ != 1 || k <= i) && (at_ != 2 || k >= i) && (bt_ != 1 || k >= j) &&
+                   (bt_ != 2 || k <= j);
+          };
+          for (int k = 0; k < g.k; ++k)
+            if (keep(g.a_tri, g.b_tri, k)) s += (double)at(g.A, i, k) * (double)at(g.B, k, j);
+          for (int k = 0; k < g.k2; ++k)
+            if (keep(g.a2_tri, g.b2_tri, k)) s += (double)at(g.A2, i, k) * (double)at(g.B2, k, j);
           tmp[(size_t)j * g.m + i] = s;
         }
       for (int j = 0; j < g.n; ++j)
