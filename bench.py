@@ -225,6 +225,65 @@ def timed_steps(step, prep, steps, world):
     return times
 
 
+def nll_fwd_bwd(local, reps: int = 5, n: int = 8192, d: int = 256) -> dict:
+    """The differentiation form's workload: loss = 1/2 y^T C^-1 y + sum log
+    diag(L), C = s X X^T + sigma2 I (X (n, d) N(0,1), s = 1/d, sigma2 = 0.1),
+    forward + backward to X, s, sigma2 through curfp_b200.autograd; ms per
+    fwd+bwd (CUDA events, median of reps after one warm-up), and the
+    gradient's relative error against dense FP64 torch autograd."""
+    import torch
+
+    import curfp_b200.autograd as ag
+
+    dev = torch.device("cuda", local)
+    g = torch.Generator(device=dev).manual_seed(8192)
+    X = torch.randn(n, d, device=dev, generator=g)
+    y = torch.randn(n, device=dev, generator=g)
+    s, sig2 = 1.0 / d, 0.1
+    out = {"workload": f"GP NLL n={n} d={d} s=1/{d} sigma2={sig2}, grads to X, s, sigma2",
+           "forms": {"fused": "curfp_b200.autograd.nll (refined alpha, curfpSgpnllBackward)",
+                     "composed": "per-op adjoints chained by torch autograd"},
+           "ms": {}, "grad_rel_err_vs_fp64": {}}
+
+    def run(math, fused):
+        Xt = X.clone().requires_grad_(True)
+        st = torch.tensor(s, device=dev, requires_grad=True)
+        vt = torch.tensor(sig2, device=dev, requires_grad=True)
+        loss = ag.nll(Xt, st, vt, y, math=math, fused=fused)
+        loss.backward()
+        return Xt.grad, st.grad, vt.grad
+
+    Xd = X.double().requires_grad_(True)
+    sd = torch.tensor(s, dtype=torch.float64, device=dev, requires_grad=True)
+    vd = torch.tensor(sig2, dtype=torch.float64, device=dev, requires_grad=True)
+    Cd = sd * Xd @ Xd.T + vd * torch.eye(n, dtype=torch.float64, device=dev)
+    Ld = torch.linalg.cholesky(Cd)
+    al = torch.cholesky_solve(y.double()[:, None], Ld)[:, 0]
+    (0.5 * torch.dot(y.double(), al) + torch.log(torch.diagonal(Ld)).sum()).backward()
+    ref = (Xd.grad, sd.grad, vd.grad)
+    del Cd, Ld
+    for form, fused in (("fused", True), ("composed", False)):
+        out["ms"][form], out["grad_rel_err_vs_fp64"][form] = {}, {}
+        for math in ("fp32", "bf16x3"):
+            run(math, fused)
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(reps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                gx, gs, gv = run(math, fused)
+                e1.record()
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            out["ms"][form][math] = round(sorted(ts)[len(ts) // 2], 3)
+            out["grad_rel_err_vs_fp64"][form][math] = {
+                "X": float(torch.linalg.norm(gx.double() - ref[0]) / torch.linalg.norm(ref[0])),
+                "s": float(abs(gs.double() - ref[1]) / abs(ref[1])),
+                "sigma2": float(abs(gv.double() - ref[2]) / abs(ref[2]))}
+    return out
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -358,6 +417,9 @@ def run_ours(args, rank, world, local):
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline()
+    fb = None
+    if not args.no_nll:
+        fb = nll_fwd_bwd(local)
 
     if rank == 0:
         form = "split-BF16 tcgen05 + FP64-residual refinement" if math_head else "plain FP32"
@@ -374,7 +436,8 @@ def run_ours(args, rank, world, local):
                            "l2": "inputs (2.1 GB RFP) larger than L2, no flush"},
                 "other_form": other, "solve_rel_residual_fp64": berr_solve,
                 "gpu_launches": launches, "kernels": kernels,
-                "roofline": roof, "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cb}
+                "roofline": roof, "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cb,
+                "fwd_bwd": fb}
         if other and other.get("value"):
             line["precision_over_plain"] = round(
                 (value / other["value"]) if math_head else (other["value"] / value), 3)
@@ -395,6 +458,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-other", action="store_true")
+    ap.add_argument("--no-nll", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -43,6 +43,10 @@ SIGNATURES = {
                         ctypes.POINTER(_f), _p, _i],
     "curfpGetKernelLaunchCount": [_h, ctypes.POINTER(ctypes.c_longlong)],
     "curfpSpftrsNoAlloc": [_h, _i, _i, _i, _i, _p, _p, _i],
+    "curfpSsfrkBackward": [_h, _i, _i, _i, _i, _i, ctypes.POINTER(_f), _p, _i, _p, _p, _i],
+    "curfpSpftrfBackward": [_h, _i, _i, _i, _p, _p, _p, _i],
+    "curfpSpftrsBackward": [_h, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _i, _p],
+    "curfpSgpnllBackward": [_h, _i, _i, _i, _i, _f, _p, _p, _i, _p, _p, _p, _i, _p, _i],
     "curfpProfileEnable": [_h, _i],
     "curfpProfileRead": [_h, _i, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_d),
                          ctypes.POINTER(ctypes.c_longlong)],

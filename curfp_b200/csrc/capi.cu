@@ -79,8 +79,12 @@ __global__ void diag_zero_check(Geometry g, const float* arf, int* flag) {
   if (i < g.n && arf[rfp::diag_offset(g, i)] == 0.0f) atomicMin(flag, (int)i + 1);
 }
 
-curfpStatus_t pack(curfpHandle_t h, int transr, int lower, int n,
-                   const float* src, float* dst, int64_t lda, int to_rfp) {
+// Copy between the logical lower triangle of a dense n x n view (element
+// (P,Q) at src/dst[P*drs + Q*dcs]) and an RFP array; dense -> RFP multiplies
+// the diagonal by diag_scale.
+curfpStatus_t pack_strided(curfpHandle_t h, int transr, int lower, int n, const float* src,
+                           float* dst, int64_t drs, int64_t dcs, int to_rfp,
+                           float diag_scale) {
   Geometry g = rfp::geometry(n, transr, lower);
   rfp::kpack::PackArgs a{};
   const rfp::BlockGeom* bg[3] = {&g.b11, &g.b21, &g.b22};
@@ -101,8 +105,9 @@ curfpStatus_t pack(curfpHandle_t h, int transr, int lower, int n,
   }
   a.nblocks = cnt;
   a.total_tiles = tiles;
-  a.upper = !lower;
-  a.lda = lda;
+  a.drs = drs;
+  a.dcs = dcs;
+  a.diag_scale = diag_scale;
   if (tiles == 0) return CURFP_STATUS_SUCCESS;
   rfp::ProfScope ps(h->prof, h->stream, rfp::K_PACK, 0, 4.0 * n * ((double)n + 1));
   rfp::kpack::pack_kernel<float>
@@ -110,6 +115,13 @@ curfpStatus_t pack(curfpHandle_t h, int transr, int lower, int n,
                                                                      to_rfp);
   ++h->launches;
   return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
+}
+
+// strttf / stfttr on a row-major n x n matrix with leading dimension lda.
+curfpStatus_t pack(curfpHandle_t h, int transr, int lower, int n, const float* src,
+                   float* dst, int64_t lda, int to_rfp) {
+  return pack_strided(h, transr, lower, n, src, dst, lower ? lda : 1, lower ? 1 : lda,
+                      to_rfp, 1.0f);
 }
 
 int symm_launch(curfpHandle_t h, const Geometry& g, const float* A, const float* X,
@@ -178,6 +190,7 @@ curfpStatus_t curfpDestroy(curfpHandle_t handle) {
   if (handle->ws2) cudaFree(handle->ws2);
   if (handle->ws3) cudaFree(handle->ws3);
   if (handle->tsv) cudaFree(handle->tsv);
+  if (handle->wsg) cudaFree(handle->wsg);
   if (handle->d_info) cudaFree(handle->d_info);
   delete handle;
   return CURFP_STATUS_SUCCESS;
@@ -410,9 +423,100 @@ curfpStatus_t curfpSsfmmAcc64(curfpHandle_t handle, curfpOperation_t transr,
   if (n == 0 || nrhs == 0) return CURFP_STATUS_SUCCESS;
   if (ldx < n || ldy < n) return CURFP_STATUS_INVALID_VALUE;
   Geometry g = rfp::geometry(n, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER);
-  dim3 grid((n + rfp::kref::TB - 1) / rfp::kref::TB, (nrhs + rfp::kref::TB - 1) / rfp::kref::TB);
-  (void)grid;
   return status_of(symm_launch(handle, g, A, X, ldx, Y, ldy, nrhs, *alpha, *beta));
+}
+
+// ---------------------------------------------------------------------------
+// Adjoints (differentiation form)
+// ---------------------------------------------------------------------------
+
+// Abar := alpha (tril(Cbar) + tril(Cbar)^T) op(A): the cotangent of A for
+// C = alpha op(A) op(A)^T + beta C when Cbar is the cotangent of C's stored
+// elements (an off-diagonal stored element is two entries of the symmetric
+// matrix, hence the doubled diagonal of the symmetric factor).
+curfpStatus_t curfpSsfrkBackward(curfpHandle_t handle, curfpOperation_t transr,
+                                 curfpFillMode_t uplo, curfpOperation_t trans, int n, int k,
+                                 const float* alpha, const float* A, int lda,
+                                 const float* Cbar, float* Abar, int ldabar) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (n < 0 || k < 0 || lda < 1 || ldabar < 1 || !alpha) return CURFP_STATUS_INVALID_VALUE;
+  if (n == 0 || k == 0) return CURFP_STATUS_SUCCESS;
+  const int tt = trans == CURFP_OP_T;
+  if (lda < (tt ? k : n) || ldabar < (tt ? k : n)) return CURFP_STATUS_INVALID_VALUE;
+  rfp::View X = tt ? rfp::View{const_cast<float*>(A), lda, 1}
+                   : rfp::View{const_cast<float*>(A), 1, lda};
+  rfp::View Y = tt ? rfp::View{Abar, ldabar, 1} : rfp::View{Abar, 1, ldabar};
+  CudaExec ex(handle);
+  return status_of(rfp::plan::rfp_symm_dbl(ex, transr == CURFP_OP_T,
+                                           uplo == CURFP_FILL_MODE_LOWER, n, Cbar, X, Y, k,
+                                           *alpha, 0.0f));
+}
+
+// Cotangent of the stored elements of A from that of its Cholesky factor
+// (rfp::plan::spftrf_backward), packed to RFP with the diagonal halved.
+curfpStatus_t curfpSpftrfBackward(curfpHandle_t handle, curfpOperation_t transr,
+                                  curfpFillMode_t uplo, int n, const float* L,
+                                  const float* Lbar, float* Abar, curfpMath_t math) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (n < 0) return CURFP_STATUS_INVALID_VALUE;
+  if (math != CURFP_MATH_FP32 && math != CURFP_MATH_SPLIT_BF16) return CURFP_STATUS_INVALID_VALUE;
+  if (n == 0) return CURFP_STATUS_SUCCESS;
+  const int tr = transr == CURFP_OP_T, lower = uplo == CURFP_FILL_MODE_LOWER;
+  const int64_t ldd = n;
+  float* D = static_cast<float*>(rfp::grow_buffer(handle, &handle->wsg, &handle->wsg_bytes,
+                                                  (size_t)n * n * sizeof(float)));
+  if (!D) return CURFP_STATUS_ALLOC_FAILED;
+  CudaExec ex(handle);
+  rfp::View S{};
+  int rc = rfp::plan::spftrf_backward(ex, tr, lower, n, L, Lbar, D, ldd, &S, (int)math);
+  if (rc) return status_of(rc);
+  return pack_strided(handle, tr, lower, n, S.p, Abar, S.rs, S.cs, 1, 0.5f);
+}
+
+// X = A^-1 B with A = L L^T:  Bbar := A^-1 Xbar and
+// Lbar := -tril(Bbar (L^T X)^T + X (L^T Bbar)^T) on the factor's stored elements.
+curfpStatus_t curfpSpftrsBackward(curfpHandle_t handle, curfpOperation_t transr,
+                                  curfpFillMode_t uplo, int n, int nrhs, const float* L,
+                                  const float* X, int ldx, const float* Xbar, int ldxbar,
+                                  float* Bbar, int ldbbar, float* Lbar) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (n < 0 || nrhs < 0) return CURFP_STATUS_INVALID_VALUE;
+  if (n == 0) return CURFP_STATUS_SUCCESS;
+  if (ldx < n || ldxbar < n || ldbbar < n) return CURFP_STATUS_INVALID_VALUE;
+  const int tr = transr == CURFP_OP_T, lower = uplo == CURFP_FILL_MODE_LOWER;
+  if (nrhs == 0) {
+    if (!Lbar) return CURFP_STATUS_SUCCESS;
+    return cudaMemsetAsync(Lbar, 0, (size_t)n * (n + 1) / 2 * sizeof(float),
+                           handle->stream) == cudaSuccess
+               ? CURFP_STATUS_SUCCESS
+               : CURFP_STATUS_EXECUTION_FAILED;
+  }
+  cudaStream_t st = handle->stream;
+  const int cb = (int)(((int64_t)n * nrhs + 255) / 256 < 4096 ? ((int64_t)n * nrhs + 255) / 256
+                                                               : 4096);
+  if (Bbar != Xbar) {
+    rfp::kref::copy_block<<<cb, 256, 0, st>>>(Bbar, ldbbar, Xbar, ldxbar, n, nrhs);
+    ++handle->launches;
+    if (!ok_launch()) return CURFP_STATUS_EXECUTION_FAILED;
+  }
+  CudaExec ex(handle);
+  int rc = rfp::plan::spftrs(ex, tr, lower, n, nrhs, L, Bbar, ldbbar);
+  if (rc || !Lbar) return status_of(rc);
+  // W = [L^T X | L^T Bbar]  (n x 2 nrhs, column-major)
+  float* W = static_cast<float*>(rfp::grow_buffer(handle, &handle->wsg, &handle->wsg_bytes,
+                                                  (size_t)2 * n * nrhs * sizeof(float)));
+  if (!W) return CURFP_STATUS_ALLOC_FAILED;
+  float* W2 = W + (size_t)n * nrhs;
+  rfp::kref::copy_block<<<cb, 256, 0, st>>>(W, n, X, ldx, n, nrhs);
+  rfp::kref::copy_block<<<cb, 256, 0, st>>>(W2, n, Bbar, ldbbar, n, nrhs);
+  handle->launches += 2;
+  if (!ok_launch()) return CURFP_STATUS_EXECUTION_FAILED;
+  rfp::View Wv{W, 1, n};
+  if ((rc = rfp::plan::rfp_trmm_t(ex, tr, lower, n, L, Wv, 2 * nrhs))) return status_of(rc);
+  rfp::View Bb{Bbar, 1, ldbbar}, Xv{const_cast<float*>(X), 1, ldx};
+  return status_of(rfp::plan::rfp_gemm_lower2(ex, tr, lower, n, Lbar, Bb, rfp::tr(Wv), Xv,
+                                              rfp::tr(rfp::View{W2, 1, n}), nrhs, -1.0f,
+                                              0.0f));
 }
 
 // Mixed-precision refinement around spftrs (see include/curfp.h).

@@ -32,6 +32,8 @@ struct curfpContext {
   rfp::Profiler prof;      // optional per-class event timing
   void* tsv = nullptr;     // wavefront solve flags / tickets
   size_t tsv_bytes = 0;
+  void* wsg = nullptr;     // dense n x n scratch of the Cholesky adjoint
+  size_t wsg_bytes = 0;
 };
 
 namespace rfp {
@@ -50,6 +52,7 @@ class CudaExec : public Exec {
   int gemm_shared(View X, int rows, int k, const SharedTask* t, int count,
                   int math) override;
   int trsm_wave(View L, int n, View B, int m, float alpha, const float* W) override;
+  int mirror_lower(View D, int n) override;
 
  protected:
   curfpContext* ctx_;

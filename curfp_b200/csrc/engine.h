@@ -85,6 +85,9 @@ class Exec {
     (void)L; (void)n; (void)B; (void)m; (void)alpha; (void)W;
     return kNotSupported;
   }
+  // D(j,i) := D(i,j) for i > j (n x n view): the stored lower triangle is
+  // mirrored into the upper one.
+  virtual int mirror_lower(View D, int n) = 0;
   // Contractions sharing one operand matrix.  The default lowers them to
   // gemm(); the CUDA executor stages X once for the tensor-core path.
   virtual int gemm_shared(View X, int rows, int k, const SharedTask* t, int count,
@@ -139,6 +142,8 @@ int spftrf(Exec& ex, int transr, int lower, int n, float* A, int math = 0);
 int spftrs(Exec& ex, int transr, int lower, int n, int nrhs, const float* A,
            float* B, int ldb);
 int spftri(Exec& ex, int transr, int lower, int n, float* A);
+// In place: the RFP factor L := L^-1 (the first half of spftri).
+int rfp_trtri(Exec& ex, int transr, int lower, int n, float* A, int math = 0);
 
 // Building blocks of the adjoints, on the logical lower factor L held in an
 // RFP array (all 8 variants):
@@ -155,6 +160,19 @@ int rfp_ltl(Exec& ex, int transr, int lower, int n, const float* L, const float*
 // + beta C with A1, A2 n x k and B1, B2 k x n dense views.
 int rfp_gemm_lower2(Exec& ex, int transr, int lower, int n, float* C, View A1, View B1,
                     View A2, View B2, int k, float alpha, float beta);
+// L^T X = B for the lower triangle of X only (diagonal included): reads the
+// lower triangle of B and overwrites it with that of X; above the diagonal B
+// may hold anything and is left undefined.  n^3/3 flops instead of n^3.
+int trsm_lt_lowerout(Exec& ex, View L, int n, View B, int math = 0);
+// Adjoint of the Cholesky factorization.  Given the factor L and the cotangent
+// Lbar of its stored lower triangle (both RFP, same variant), leaves in the
+// view S (n x n, dense, anything may alias nothing) the lower triangle of
+// S = L^-T Q L^-1 with Q the symmetric matrix whose lower triangle is that of
+// L^T Lbar.  The cotangent of the stored triangle of A is then S(p,q) for
+// p > q and S(p,p)/2 on the diagonal.  D is an n x n column-major scratch;
+// S is returned as a view into D.
+int spftrf_backward(Exec& ex, int transr, int lower, int n, const float* L,
+                    const float* Lbar, float* D, int64_t ldd, View* S, int math = 0);
 // Y := alpha (G_L + G_L^T) X + beta Y where G_L is the stored lower triangle
 // (diagonal included, so the diagonal counts twice) of the RFP array G; X, Y
 // dense n x m views.

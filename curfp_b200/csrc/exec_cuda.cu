@@ -139,6 +139,15 @@ int CudaExec::gemm(const GemmProb* p, int count) {
   return launch_gemm<64, 64>(p, count, abort_, ctx_);
 }
 
+int CudaExec::mirror_lower(View D, int n) {
+  if (n <= 1) return 0;
+  const int t = (n + ktile::MTS - 1) / ktile::MTS;
+  ProfScope ps(ctx_->prof, ctx_->stream, K_PACK, 0, 4.0 * n * (double)(n - 1));
+  ktile::mirror_lower<<<t * (t + 1) / 2, dim3(ktile::MTS, ktile::MTY), 0, ctx_->stream>>>(D, n);
+  ++ctx_->launches;
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
 int CudaExec::potrf_tile(View L, int n, int info_base) {
   if (n <= 0) return 0;
   ProfScope ps(ctx_->prof, ctx_->stream, K_POTRF, (double)n * n * n / 3.0, 0);

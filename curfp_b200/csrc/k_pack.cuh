@@ -36,8 +36,10 @@ struct PackArgs {
   PackBlock b[3];
   int nblocks;
   int total_tiles;
-  int upper;               // UPLO=U: dense element of logical (P,Q) is A[Q][P]
-  int64_t lda;
+  // Dense element of logical (P,Q) at P*drs + Q*dcs: row-major A[P][Q] for
+  // UPLO=L (drs = lda, dcs = 1), A[Q][P] for UPLO=U (drs = 1, dcs = lda).
+  int64_t drs, dcs;
+  float diag_scale;        // dense -> RFP: diagonal elements are multiplied by this
 };
 
 __device__ __forceinline__ void pack_tile_coords(const PackBlock& B, int lt,
@@ -70,14 +72,14 @@ __global__ void __launch_bounds__(TS * TY) pack_kernel(const PackArgs args,
   const int tx = threadIdx.x, ty = threadIdx.y;
 
   // Contiguous dimension of each side: 0 -> p, 1 -> q.
-  const int dense_q = args.upper ? 0 : 1;  // row-major A[P][Q]
+  const int dense_q = (args.dcs == 1 || args.dcs == -1) ? 1 : 0;
   const int rfp_q = (B.rs == 1 || B.rs == -1) ? 0 : 1;
   const int src_q = to_rfp ? dense_q : rfp_q;
   const int dst_q = to_rfp ? rfp_q : dense_q;
 
   auto dense_ptr = [&](int p, int q) -> int64_t {
     int64_t P = (int64_t)B.p_base + p, Q = (int64_t)B.q_base + q;
-    return args.upper ? Q * args.lda + P : P * args.lda + Q;
+    return P * args.drs + Q * args.dcs;
   };
   auto rfp_ptr = [&](int p, int q) -> int64_t {
     return B.off + (int64_t)p * B.rs + (int64_t)q * B.cs;
@@ -102,8 +104,11 @@ __global__ void __launch_bounds__(TS * TY) pack_kernel(const PackArgs args,
     if (dst_q) { lq = tx; lp = ty + r * TY; }
     else       { lp = tx; lq = ty + r * TY; }
     int p = p0 + lp, q = q0 + lq;
-    if (inside(p, q))
-      dst[to_rfp ? rfp_ptr(p, q) : dense_ptr(p, q)] = tile[lp][lq];
+    if (inside(p, q)) {
+      T v = tile[lp][lq];
+      if (to_rfp && B.p_base + p == B.q_base + q) v *= (T)args.diag_scale;
+      dst[to_rfp ? rfp_ptr(p, q) : dense_ptr(p, q)] = v;
+    }
   }
 }
 

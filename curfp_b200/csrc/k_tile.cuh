@@ -248,5 +248,35 @@ __global__ void __launch_bounds__(256) lauum_tile(View L, int n) {
   }
 }
 
+constexpr int MTS = 32, MTY = 8;  // mirror tile edge, thread rows
+
+// D(q,p) := D(p,q) for p > q on an n x n view: one 32 x 32 tile of the lower
+// tile triangle per CTA, read along the view's contiguous dimension and
+// written transposed through shared memory, so both sides coalesce.
+__global__ void __launch_bounds__(MTS * MTY) mirror_lower(View D, int n) {
+  __shared__ float tile[MTS][MTS + 1];
+  const int lt = blockIdx.x;
+  int tp = (int)((sqrt(8.0 * (double)lt + 1.0) - 1.0) * 0.5);
+  while ((tp + 1) * (tp + 2) / 2 <= lt) ++tp;
+  while (tp * (tp + 1) / 2 > lt) --tp;
+  const int tq = lt - tp * (tp + 1) / 2;
+  const int p0 = tp * MTS, q0 = tq * MTS;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const bool pc = (D.rs == 1 || D.rs == -1);
+#pragma unroll
+  for (int r = 0; r < MTS / MTY; ++r) {
+    const int lp = pc ? tx : ty + r * MTY, lq = pc ? ty + r * MTY : tx;
+    const int p = p0 + lp, q = q0 + lq;
+    if (p < n && p > q) tile[lp][lq] = D.p[(int64_t)p * D.rs + (int64_t)q * D.cs];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < MTS / MTY; ++r) {
+    const int lq = pc ? tx : ty + r * MTY, lp = pc ? ty + r * MTY : tx;
+    const int p = p0 + lp, q = q0 + lq;
+    if (p < n && p > q) D.p[(int64_t)q * D.rs + (int64_t)p * D.cs] = tile[lp][lq];
+  }
+}
+
 }  // namespace ktile
 }  // namespace rfp

@@ -261,18 +261,27 @@ int spftrs(Exec& ex, int transr, int lower, int n, int nrhs, const float* A,
   return trsm(ex, 1, 1, 1, V11, B1, g.n1, nrhs, 1.0f);
 }
 
-int spftri(Exec& ex, int transr, int lower, int n, float* A) {
+int rfp_trtri(Exec& ex, int transr, int lower, int n, float* A, int math) {
   Geometry g = geometry(n, transr, lower);
   View V11 = block_view(A, g.b11), V21 = block_view(A, g.b21),
        V22 = block_view(A, g.b22);
   int rc;
   // inv(L) = [M11 0; -M22 L21 M11  M22]
-  if ((rc = trtri_lower(ex, V11, g.n1))) return rc;
-  if ((rc = trtri_lower(ex, V22, g.n2))) return rc;
+  if ((rc = trtri_lower(ex, V11, g.n1, math))) return rc;
+  if ((rc = trtri_lower(ex, V22, g.n2, math))) return rc;
   if (g.n1 > 0 && g.n2 > 0) {
-    if ((rc = trmm(ex, 0, 1, 0, V11, V21, g.n2, g.n1, 1.0f))) return rc;
-    if ((rc = trmm(ex, 1, 1, 0, V22, V21, g.n2, g.n1, -1.0f))) return rc;
+    if ((rc = trmm(ex, 0, 1, 0, V11, V21, g.n2, g.n1, 1.0f, math))) return rc;
+    if ((rc = trmm(ex, 1, 1, 0, V22, V21, g.n2, g.n1, -1.0f, math))) return rc;
   }
+  return 0;
+}
+
+int spftri(Exec& ex, int transr, int lower, int n, float* A) {
+  Geometry g = geometry(n, transr, lower);
+  View V11 = block_view(A, g.b11), V21 = block_view(A, g.b21),
+       V22 = block_view(A, g.b22);
+  int rc;
+  if ((rc = rfp_trtri(ex, transr, lower, n, A, 0))) return rc;
   // inv(A) = M^T M:  (11) = M11^T M11 + M21^T M21, (21) = M22^T M21,
   //                  (22) = M22^T M22
   if ((rc = lauum_lower(ex, V11, g.n1))) return rc;
@@ -397,6 +406,57 @@ int rfp_gemm_lower2(Exec& ex, int transr, int lower, int n, float* C, View A1, V
     p[cnt++] = q;
   }
   return ex.gemm(p, cnt);
+}
+
+int trsm_lt_lowerout(Exec& ex, View L, int n, View B, int math) {
+  if (n <= 0) return 0;
+  if (n <= kWaveLeaf) return trsm(ex, 1, 1, 1, L, B, n, n, 1.0f, math);
+  // L = [L11 0; L21 L22]:  L22^T X22 = B22 (lower part), L22^T X21 = B21,
+  // L11^T X11 = B11 - L21^T X21 (lower part).
+  const int n1 = split(n, kTriTile), n2 = n - n1;
+  View L11 = L, L21 = sub(L, n1, 0), L22 = sub(L, n1, n1);
+  View B11 = B, B21 = sub(B, n1, 0), B22 = sub(B, n1, n1);
+  int rc;
+  if ((rc = trsm_lt_lowerout(ex, L22, n2, B22, math))) return rc;
+  if ((rc = trsm(ex, 1, 1, 1, L22, B21, n2, n1, 1.0f, math))) return rc;
+  GemmProb p = gemm_prob(tr(L21), B21, B11, n1, n1, n2, -1.0f, 1.0f, math);
+  p.c_lower = 1;
+  if ((rc = ex.gemm(&p, 1))) return rc;
+  return trsm_lt_lowerout(ex, L11, n1, B11, math);
+}
+
+namespace {
+// trsm_lt_lowerout with L the logical factor of an RFP array.
+int rfp_trsm_lowerout(Exec& ex, int transr, int lower, int n, const float* L, View B,
+                      int math) {
+  Blocks b = blocks(transr, lower, n, L);
+  const int n1 = b.g.n1, n2 = b.g.n2;
+  View B11 = B, B21 = sub(B, n1, 0), B22 = sub(B, n1, n1);
+  int rc;
+  if ((rc = trsm_lt_lowerout(ex, b.V22, n2, B22, math))) return rc;
+  if (n1 > 0 && n2 > 0) {
+    if ((rc = trsm(ex, 1, 1, 1, b.V22, B21, n2, n1, 1.0f, math))) return rc;
+    GemmProb p = gemm_prob(tr(b.V21), B21, B11, n1, n1, n2, -1.0f, 1.0f, math);
+    p.c_lower = 1;
+    if ((rc = ex.gemm(&p, 1))) return rc;
+  }
+  return trsm_lt_lowerout(ex, b.V11, n1, B11, math);
+}
+}  // namespace
+
+int spftrf_backward(Exec& ex, int transr, int lower, int n, const float* L,
+                    const float* Lbar, float* D, int64_t ldd, View* S, int math) {
+  View Dv{D, 1, ldd};
+  int rc;
+  // lower(Q) = lower(L^T Lbar); Q symmetric
+  if ((rc = rfp_ltl(ex, transr, lower, n, L, Lbar, Dv))) return rc;
+  if ((rc = ex.mirror_lower(Dv, n))) return rc;
+  // Z = L^-T Q, then S = L^-T Z^T (= Z L^-1, symmetric): lower part only
+  if ((rc = rfp_trsm(ex, transr, lower, n, L, 1, Dv, n, 1.0f, math))) return rc;
+  View St = tr(Dv);
+  if ((rc = rfp_trsm_lowerout(ex, transr, lower, n, L, St, math))) return rc;
+  *S = St;
+  return 0;
 }
 
 int rfp_symm_dbl(Exec& ex, int transr, int lower, int n, const float* G, View X, View Y,

@@ -193,6 +193,56 @@ curfpStatus_t curfpSpftrsNoAlloc(curfpHandle_t handle, curfpOperation_t transr,
                                  curfpFillMode_t uplo, int n, int nrhs,
                                  const float *A, float *B, int ldb);
 
+/* ---- Differentiation form: adjoints (no counterpart in the reference) ----
+ * Cotangents of RFP arrays are RFP arrays of the same variant holding the
+ * derivative with respect to each STORED element (an off-diagonal stored
+ * element stands for two entries of the symmetric matrix). */
+
+/* Adjoint of curfpSsfrk with respect to A:
+ *   Abar := alpha * (tril(Cbar) + tril(Cbar)^T) * op(A),
+ * stored like A (n x k column-major for trans = N, k x n for trans = T). */
+curfpStatus_t curfpSsfrkBackward(curfpHandle_t handle, curfpOperation_t transr,
+                                 curfpFillMode_t uplo, curfpOperation_t trans,
+                                 int n, int k, const float *alpha,
+                                 const float *A, int lda, const float *Cbar,
+                                 float *Abar, int ldabar);
+
+/* Adjoint of curfpSpftrf: L is the factor (as curfpSpftrf leaves it), Lbar
+ * the cotangent of its stored elements; Abar receives the cotangent of the
+ * stored elements of A (Abar may alias L or Lbar).  Uses n*n floats of
+ * handle-owned scratch; math selects the arithmetic of its triangular
+ * solves (CURFP_MATH_SPLIT_BF16: split-BF16 tensor-core updates). */
+curfpStatus_t curfpSpftrfBackward(curfpHandle_t handle, curfpOperation_t transr,
+                                  curfpFillMode_t uplo, int n, const float *L,
+                                  const float *Lbar, float *Abar,
+                                  curfpMath_t math);
+
+/* Adjoint of curfpSpftrs (X = A^-1 B, A = L L^T; X, Xbar, Bbar column-major
+ * n x nrhs): Bbar := A^-1 Xbar (Bbar may alias Xbar) and Lbar (RFP, written;
+ * NULL skips it) := -tril(Bbar (L^T X)^T + X (L^T Bbar)^T). */
+curfpStatus_t curfpSpftrsBackward(curfpHandle_t handle, curfpOperation_t transr,
+                                  curfpFillMode_t uplo, int n, int nrhs,
+                                  const float *L, const float *X, int ldx,
+                                  const float *Xbar, int ldxbar, float *Bbar,
+                                  int ldbbar, float *Lbar);
+
+/* Fused gradient of the Gaussian-process negative log marginal likelihood
+ *   f = 1/2 y^T C^-1 y + sum_i log L_ii,  C = s X X^T + sigma2 I = L L^T,
+ * from the factor L (RFP), X (n x d row-major, ldx >= d) and
+ * alpha = C^-1 y (device, n), scaled by the device scalar *g (the incoming
+ * gradient of f):
+ *   Xbar    := g s (C^-1 X - alpha (X^T alpha)^T)   (n x d row-major, ldxbar)
+ *   sums[0] := g/2 (|L^-1 X|_F^2 - |X^T alpha|^2)   (df/ds)
+ *   sums[1] := g/2 (|L^-1|_F^2 - |alpha|^2)          (df/dsigma2)
+ * sums is device memory (2 doubles).  Inner products are accumulated in
+ * FP64.  Uses n*d + n(n+1)/2 floats of handle-owned scratch. */
+curfpStatus_t curfpSgpnllBackward(curfpHandle_t handle, curfpOperation_t transr,
+                                  curfpFillMode_t uplo, int n, int d, float s,
+                                  const float *L, const float *X, int ldx,
+                                  const float *alpha, const float *g,
+                                  float *Xbar, int ldxbar, double *sums,
+                                  curfpMath_t math);
+
 /* Number of kernels launched through this handle since its creation. */
 curfpStatus_t curfpGetKernelLaunchCount(curfpHandle_t handle, long long *count);
 

@@ -156,6 +156,12 @@ class CpuExec : public Exec {
     return 0;
   }
 
+  int mirror_lower(View D, int n) override {
+    for (int q = 0; q < n; ++q)
+      for (int p = q + 1; p < n; ++p) at(D, q, p) = at(D, p, q);
+    return 0;
+  }
+
   float* workspace(size_t nfloats) override {
     if (ws.size() < nfloats) ws.resize(nfloats);
     return ws.data();
@@ -197,6 +203,55 @@ int hs_spftrs(int transr, int lower, int n, int nrhs, const float* A, float* B, 
 int hs_spftri(int transr, int lower, int n, float* A) {
   CpuExec ex;
   return plan::spftri(ex, transr, lower, n, A);
+}
+
+// Lower triangle of S = L^-T Q L^-1 (Cholesky adjoint) written to S[p*n+q]
+// (row-major, p >= q).
+int hs_spftrf_backward(int transr, int lower, int n, const float* L, const float* Lbar,
+                       float* S, int math) {
+  CpuExec ex;
+  std::vector<float> D((size_t)n * n, 0.0f);
+  View Sv{};
+  int rc = plan::spftrf_backward(ex, transr, lower, n, L, Lbar, D.data(), n, &Sv, math);
+  if (rc) return rc;
+  for (int p = 0; p < n; ++p)
+    for (int q = 0; q <= p; ++q) S[(size_t)p * n + q] = at(Sv, p, q);
+  return 0;
+}
+
+// Same arithmetic as curfpSsfrkBackward.
+int hs_ssfrk_backward(int transr, int lower, int trans, int n, int k, float alpha,
+                      const float* A, int lda, const float* Cbar, float* Abar, int ldabar) {
+  CpuExec ex;
+  View X = trans ? View{const_cast<float*>(A), lda, 1} : View{const_cast<float*>(A), 1, lda};
+  View Y = trans ? View{Abar, ldabar, 1} : View{Abar, 1, ldabar};
+  return plan::rfp_symm_dbl(ex, transr, lower, n, Cbar, X, Y, k, alpha, 0.0f);
+}
+
+// Same sequence as curfpSpftrsBackward (column-major n x nrhs blocks, ld n).
+int hs_spftrs_backward(int transr, int lower, int n, int nrhs, const float* L, const float* X,
+                       const float* Xbar, float* Bbar, float* Lbar) {
+  CpuExec ex;
+  for (size_t e = 0; e < (size_t)n * nrhs; ++e) Bbar[e] = Xbar[e];
+  int rc = plan::spftrs(ex, transr, lower, n, nrhs, L, Bbar, n);
+  if (rc) return rc;
+  std::vector<float> W((size_t)2 * n * nrhs);
+  for (size_t e = 0; e < (size_t)n * nrhs; ++e) {
+    W[e] = X[e];
+    W[(size_t)n * nrhs + e] = Bbar[e];
+  }
+  View Wv{W.data(), 1, n};
+  if ((rc = plan::rfp_trmm_t(ex, transr, lower, n, L, Wv, 2 * nrhs))) return rc;
+  return plan::rfp_gemm_lower2(ex, transr, lower, n, Lbar, View{Bbar, 1, n}, tr(Wv),
+                               View{const_cast<float*>(X), 1, n},
+                               tr(View{W.data() + (size_t)n * nrhs, 1, n}), nrhs, -1.0f, 0.0f);
+}
+
+// rfp_trsm: L X = alpha B (trans 0) or L^T X = alpha B (trans 1); B column-major ld n.
+int hs_rfp_trsm(int transr, int lower, int n, const float* L, int trans, float* B, int m,
+                float alpha) {
+  CpuExec ex;
+  return plan::rfp_trsm(ex, transr, lower, n, L, trans, View{B, 1, n}, m, alpha, 0);
 }
 
 int hs_geometry(int n, int transr, int lower, int64_t* out) {
