@@ -14,6 +14,12 @@ The RFP matrix (2.1 GB) is larger than L2 (126 MB): no extra L2 flush.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--math bf16x3|fp32] [--n 32768] [--k 1024] [--nrhs 64]
 
+  python bench.py --case NAME [--n N] [--k K] [--nrhs R]
+      runs one small workload of one kernel family a few times and exits (no
+      timing): the commands the ncu summaries under profiles/ were made with.
+      Cases: ssfrk-bf16, ssfrk-fp32, chol-bf16, chol-fp32, solve, refine, pack,
+      nll-fused.
+
 --impl reference times the reference's algorithm on the host cores: LAPACK's
 RFP routines (spftrf/spftrs via scipy/OpenBLAS, all threads), which the
 reference's GPU code translates call for call; each step is a bounded sample
@@ -326,8 +332,12 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
 
     l0 = L.launches()
+    # cudaProfilerStart/Stop bracket the timed steps so that a launch list
+    # taken with ncu --profile-from-start off covers exactly these launches
+    torch.cuda.cudart().cudaProfilerStart()
     with ClockSampler(local) as clk:
         times = timed_steps(step_head, prep, args.steps, world)
+    torch.cuda.cudart().cudaProfilerStop()
     launches = L.launches() - l0
     total_ms = max_over_ranks(sum(times), world)
     ms_step = total_ms / args.steps
@@ -444,6 +454,70 @@ def run_ours(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+CASES = ("ssfrk-bf16", "ssfrk-fp32", "chol-bf16", "chol-fp32", "solve", "refine", "pack",
+         "nll-fused")
+
+
+def run_case(args):
+    """Small single-family workloads for kernel profiles (no timing, no JSON):
+    the library call is made `reps` times on seeded inputs larger than L2."""
+    import torch
+
+    import curfp_b200 as curfp
+    from curfp_b200 import autograd as ag
+    from curfp_b200 import precision as P
+
+    n, k, nrhs, reps = args.n, args.k, args.nrhs, 3
+    g = torch.Generator(device="cuda").manual_seed(7)
+    nt = n * (n + 1) // 2
+
+    def spd():
+        A = torch.randn(n, k, device="cuda", generator=g) / k ** 0.5
+        C = torch.empty(nt, device="cuda")
+        curfp.ssfrk(A, C)
+        curfp.add_to_diagonal(C, 1.0)
+        return C
+
+    case = args.case
+    if case in ("ssfrk-bf16", "ssfrk-fp32"):
+        A = torch.randn(n, k, device="cuda", generator=g) / k ** 0.5
+        C = torch.empty(nt, device="cuda")
+        for _ in range(reps):
+            P.ssfrk(A, C, math="bf16x3" if case == "ssfrk-bf16" else "fp32")
+    elif case in ("chol-bf16", "chol-fp32"):
+        C0 = spd()
+        C = torch.empty_like(C0)
+        for _ in range(reps):
+            C.copy_(C0)
+            P.spftrf(C, math="bf16x3" if case == "chol-bf16" else "fp32")
+    elif case == "solve":
+        C = spd()
+        curfp.spftrf(C)
+        B0 = torch.randn(n, nrhs, device="cuda", generator=g)
+        for _ in range(reps):
+            curfp.spftrs(C, B0.clone())
+    elif case == "refine":
+        C = spd()
+        X = torch.randn(n, nrhs, device="cuda", generator=g)
+        for _ in range(reps):
+            P.ssfmm_acc64(C, X)
+    elif case == "pack":
+        D = torch.randn(n, n, device="cuda", generator=g)
+        for _ in range(reps):
+            arf = curfp.strttf(D)
+            curfp.stfttr(arf)
+    elif case == "nll-fused":
+        X = torch.randn(n, k, device="cuda", generator=g)
+        y = torch.randn(n, device="cuda", generator=g)
+        for _ in range(reps):
+            Xt = X.clone().requires_grad_(True)
+            st = torch.tensor(1.0 / k, device="cuda", requires_grad=True)
+            vt = torch.tensor(0.1, device="cuda", requires_grad=True)
+            ag.nll(Xt, st, vt, y).backward()
+    torch.cuda.synchronize()
+    print(json.dumps({"case": case, "n": n, "k": k, "nrhs": nrhs, "reps": reps, "ok": True}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -459,7 +533,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-other", action="store_true")
     ap.add_argument("--no-nll", action="store_true")
+    ap.add_argument("--case", choices=CASES, default=None)
     args = ap.parse_args()
+    if args.case:
+        run_case(args)
+        return
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))
