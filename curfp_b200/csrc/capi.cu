@@ -111,7 +111,7 @@ curfpStatus_t pack_strided(curfpHandle_t h, int transr, int lower, int n, const 
   if (tiles == 0) return CURFP_STATUS_SUCCESS;
   rfp::ProfScope ps(h->prof, h->stream, rfp::K_PACK, 0, 4.0 * n * ((double)n + 1));
   rfp::kpack::pack_kernel<float>
-      <<<tiles, dim3(rfp::kpack::TS, rfp::kpack::TY), 0, h->stream>>>(a, src, dst,
+      <<<tiles, dim3(rfp::kpack::TX, rfp::kpack::TY), 0, h->stream>>>(a, src, dst,
                                                                      to_rfp);
   ++h->launches;
   return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;

@@ -6,11 +6,14 @@
 // contiguous one, so RFP blocks (T1, S, T2 in any of the 8 variants, their
 // transposes and their index reversals) are addressed in place, never
 // unpacked.  One CTA computes a BM x BN tile with 256 threads, each holding a
-// (BM/16) x (BN/16) register tile; A and B tiles of depth 16 are staged in
-// shared memory by 4-byte cp.async with zero fill (RFP leading dimensions are
-// often odd, so 16-byte vector loads are not generally legal), double
-// buffered.  The global-load thread mapping follows the contiguous dimension
-// of each operand so every warp-wide load is coalesced.
+// (BM/16) x (BN/16) register tile; A and B tiles of depth 16 are loaded into
+// registers one tile ahead (float4 loads where the operand's unit stride,
+// base and other stride allow it -- RFP leading dimensions are often odd --
+// scalar loads with zero fill otherwise) and stored to double-buffered,
+// swizzled shared memory after the FMAs of the current tile.  The
+// global-load thread mapping follows the contiguous dimension of each
+// operand so every warp-wide load is coalesced.  Triangular operand masks
+// also shrink the k range of a tile to the k-tiles they leave non-zero.
 //
 // c_lower problems enumerate only tiles on or below the diagonal and mask the
 // diagonal tiles element-wise, which is how SYRK updates of the RFP triangles
@@ -25,8 +28,6 @@ namespace rfp {
 namespace kgemm {
 
 constexpr int kThreads = 256;
-constexpr int kBK = 16;
-constexpr int kPad = 4;
 
 struct Prob {
   const float* A; int64_t a_rs, a_cs;
@@ -49,24 +50,6 @@ struct Batch {
   const int* abort_flag;  // if non-null and *abort_flag != INT_MAX: no-op
 };
 
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void cp_async4(void* smem, const float* g, bool pred) {
-  unsigned s = smem_u32(smem);
-  int sz = pred ? 4 : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s),
-               "l"(g), "r"(sz));
-}
-__device__ __forceinline__ void cp_commit() {
-  asm volatile("cp.async.commit_group;\n" ::);
-}
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
 // Map a linear tile index of a problem to (ti, tj).
 __device__ __forceinline__ void tile_coords(const Prob& P, int lt, int& ti,
                                             int& tj) {
@@ -83,47 +66,104 @@ __device__ __forceinline__ void tile_coords(const Prob& P, int lt, int& ti,
   tj = lt - (int)((int64_t)r * (r + 1) / 2);
 }
 
-template <int BM, int BN>
-struct Smem {
-  float a[2][kBK][BM + kPad];
-  float b[2][kBK][BN + kPad];
+// Shared-memory operand tiles are k-major, s[kk][r] with r the tile row (m
+// for A, n for B).  Groups of 4 consecutive r are permuted within aligned
+// groups of 8 by kk: the inner loop still reads aligned float4 runs, and the
+// transposing stores of k-contiguous operands hit 32 distinct banks (depth
+// 16: 4 threads per row, 8 rows per warp, col4 ^ 2*((kk>>2)&3); depth 8: 2
+// threads per row, 16 rows per warp, col4 ^ 4*((kk>>2)&1)).
+template <int BK>
+__device__ __forceinline__ int swz(int r, int kk) {
+  const int h = BK == 8 ? (((kk >> 2) & 1) << 2) : (((kk >> 2) & 3) << 1);
+  return (((r >> 2) ^ h) << 2) | (r & 3);
+}
+
+// One operand of one product is seen as rows r (m of A or n of B) by kk:
+// element (r, kk) at p[r*sr + kk*sk]; tri in the (r, kk) convention: 1 keeps
+// kk <= r, 2 keeps kk >= r.  Flags: bit 0 = kk is the unit-stride dimension
+// (else r), bit 1 = float4 loads allowed (unit stride +1, 16-byte aligned
+// base, other stride a multiple of 4).
+__device__ __forceinline__ int operand_flags(const float* p, int64_t sr, int64_t sk) {
+  const bool kcont = (sk == 1 || sk == -1) && !(sr == 1 || sr == -1);
+  const int64_t unit = kcont ? sk : sr, other = kcont ? sr : sk;
+  const bool vec = unit == 1 && (other & 3) == 0 && ((reinterpret_cast<uintptr_t>(p) & 15) == 0);
+  return (kcont ? 1 : 0) | (vec ? 2 : 0);
+}
+
+// Register staging of one R x BK tile: NG groups of 4 elements along the
+// operand's unit-stride dimension, G per thread.
+template <int R, int BK>
+struct Stage {
+  static constexpr int NG = R * BK / 4;
+  static constexpr int G = (NG + kThreads - 1) / kThreads;
+  float v[G][4];
 };
 
-// Stage one BK-deep slice of product (A, B) into shared memory.
-template <int BM, int BN>
-__device__ __forceinline__ void load_stage(Smem<BM, BN>& sm, int buf,
-                                           const float* A, int64_t a_rs,
-                                           int64_t a_cs, const float* B,
-                                           int64_t b_rs, int64_t b_cs, int m,
-                                           int n, int k, int m0, int n0,
-                                           int k0, int a_tri, int b_tri) {
+template <int R, int BK>
+__device__ __forceinline__ void stage_load(Stage<R, BK>& st, const float* p, int64_t sr, int64_t sk,
+                                           int rows, int depth, int tri, int flags, int r0,
+                                           int k0) {
   const int tid = threadIdx.x;
-  constexpr int LA = BM * kBK / kThreads;
-  constexpr int LB = BN * kBK / kThreads;
-  const bool a_mcont = (a_rs == 1 || a_rs == -1);
+  const bool kcont = flags & 1;
+  constexpr int KG = BK / 4;  // groups per row along k
 #pragma unroll
-  for (int r = 0; r < LA; ++r) {
-    int e = tid + kThreads * r;
-    int i, kk;
-    if (a_mcont) { i = e % BM; kk = e / BM; }
-    else         { i = e / kBK; kk = e % kBK; }
-    int gi = m0 + i, gk = k0 + kk;
-    bool ok = gi < m && gk < k && (a_tri != 1 || gk <= gi) && (a_tri != 2 || gk >= gi);
-    const float* src = ok ? A + (int64_t)gi * a_rs + (int64_t)gk * a_cs : A;
-    cp_async4(&sm.a[buf][kk][i], src, ok);
-  }
-  const bool b_ncont = (b_cs == 1 || b_cs == -1);
+  for (int u = 0; u < Stage<R, BK>::G; ++u) {
+    const int e = tid + kThreads * u;
+    if (Stage<R, BK>::NG % kThreads != 0 && e >= Stage<R, BK>::NG) break;
+    int r, kk;  // first element of the group
+    if (kcont) { r = e / KG; kk = (e % KG) << 2; }
+    else       { r = (e % (R / 4)) << 2; kk = e / (R / 4); }
+    const int gr = r0 + r, gk = k0 + kk;
+    const int lim_r = rows - gr, lim_k = depth - gk;
+    const bool full = tri == 0 && (kcont ? (lim_r > 0 && lim_k >= 4) : (lim_k > 0 && lim_r >= 4));
+    if ((flags & 2) && full) {
+      const float4 x =
+          __ldg(reinterpret_cast<const float4*>(p + (int64_t)gr * sr + (int64_t)gk * sk));
+      st.v[u][0] = x.x; st.v[u][1] = x.y; st.v[u][2] = x.z; st.v[u][3] = x.w;
+    } else {
 #pragma unroll
-  for (int r = 0; r < LB; ++r) {
-    int e = tid + kThreads * r;
-    int j, kk;
-    if (b_ncont) { j = e % BN; kk = e / BN; }
-    else         { j = e / kBK; kk = e % kBK; }
-    int gj = n0 + j, gk = k0 + kk;
-    bool ok = gj < n && gk < k && (b_tri != 1 || gk >= gj) && (b_tri != 2 || gk <= gj);
-    const float* src = ok ? B + (int64_t)gk * b_rs + (int64_t)gj * b_cs : B;
-    cp_async4(&sm.b[buf][kk][j], src, ok);
+      for (int c = 0; c < 4; ++c) {
+        const int rr = gr + (kcont ? 0 : c), kc = gk + (kcont ? c : 0);
+        const bool ok = rr < rows && kc < depth && (tri != 1 || kc <= rr) && (tri != 2 || kc >= rr);
+        st.v[u][c] = ok ? __ldg(p + (int64_t)rr * sr + (int64_t)kc * sk) : 0.f;
+      }
+    }
   }
+}
+
+template <int R, int BK>
+__device__ __forceinline__ void stage_store(const Stage<R, BK>& st, float (*s)[R], bool kcont) {
+  const int tid = threadIdx.x;
+  constexpr int KG = BK / 4;
+#pragma unroll
+  for (int u = 0; u < Stage<R, BK>::G; ++u) {
+    const int e = tid + kThreads * u;
+    if (Stage<R, BK>::NG % kThreads != 0 && e >= Stage<R, BK>::NG) break;
+    if (kcont) {
+      const int r = e / KG, kk = (e % KG) << 2;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) s[kk + c][swz<BK>(r, kk + c)] = st.v[u][c];
+    } else {
+      const int r = (e % (R / 4)) << 2, kk = e / (R / 4);
+      *reinterpret_cast<float4*>(&s[kk][swz<BK>(r, kk)]) =
+          make_float4(st.v[u][0], st.v[u][1], st.v[u][2], st.v[u][3]);
+    }
+  }
+}
+
+// k range [kb, ke) of a product that the triangular masks leave non-zero for
+// the tile at (m0, n0), rounded out to BK.
+template <int BK>
+__device__ __forceinline__ void k_range(int k, int a_tri, int b_tri, int m0, int n0, int BM,
+                                        int BN, int& kb, int& ke) {
+  kb = 0;
+  ke = k;
+  if (a_tri == 1) ke = min(ke, m0 + BM);   // kk <= i
+  if (a_tri == 2) kb = max(kb, m0);        // kk >= i
+  if (b_tri == 1) kb = max(kb, n0);        // kk >= j
+  if (b_tri == 2) ke = min(ke, n0 + BN);   // kk <= j
+  kb = (kb / BK) * BK;
+  if (ke < kb) ke = kb;
 }
 
 template <int BM, int BN>
@@ -131,7 +171,11 @@ __global__ void __launch_bounds__(kThreads, 2) sgemm_batch(const Batch batch) {
   if (batch.abort_flag && *batch.abort_flag != INT_MAX) return;
   constexpr int TM = BM / 16, TN = BN / 16;
   constexpr int GM = TM / 4, GN = TN / 4;
-  __shared__ __align__(16) Smem<BM, BN> sm;
+  // depth 8 for the 128 x 128 tile keeps the register staging within the
+  // 128-register budget of two CTAs per SM
+  constexpr int BK = BM >= 128 ? 8 : 16;
+  __shared__ __align__(16) float sa[2][BK][BM];
+  __shared__ __align__(16) float sb[2][BK][BN];
 
   // Locate the problem and tile.
   int t = blockIdx.x, pi = 0;
@@ -151,48 +195,63 @@ __global__ void __launch_bounds__(kThreads, 2) sgemm_batch(const Batch batch) {
 #pragma unroll
     for (int j = 0; j < TN; ++j) acc[i][j] = 0.f;
 
-  const int kt1 = (P.k + kBK - 1) / kBK;
-  const int kt2 = (P.k2 + kBK - 1) / kBK;
+  // B's mask codes map to the (r = j, kk) convention: lower B keeps kk >= j
+  // (code 2 there), upper keeps kk <= j (code 1).
+  auto bcode = [](int b) { return b == 1 ? 2 : (b == 2 ? 1 : 0); };
+  const int fl = operand_flags(P.A, P.a_rs, P.a_cs) | (operand_flags(P.B, P.b_cs, P.b_rs) << 2) |
+                 (operand_flags(P.A2, P.a2_rs, P.a2_cs) << 4) |
+                 (operand_flags(P.B2, P.b2_cs, P.b2_rs) << 6);
+  int kb1, ke1, kb2, ke2;
+  k_range<BK>(P.k, P.a_tri, P.b_tri, m0, n0, BM, BN, kb1, ke1);
+  k_range<BK>(P.k2, P.a2_tri, P.b2_tri, m0, n0, BM, BN, kb2, ke2);
+  const int kt1 = (ke1 - kb1 + BK - 1) / BK;
+  const int kt2 = (ke2 - kb2 + BK - 1) / BK;
   const int ktiles = kt1 + kt2;
 
-  auto issue = [&](int kt, int buf) {
-    if (kt < kt1)
-      load_stage<BM, BN>(sm, buf, P.A, P.a_rs, P.a_cs, P.B, P.b_rs, P.b_cs,
-                         P.m, P.n, P.k, m0, n0, kt * kBK, P.a_tri, P.b_tri);
-    else
-      load_stage<BM, BN>(sm, buf, P.A2, P.a2_rs, P.a2_cs, P.B2, P.b2_rs,
-                         P.b2_cs, P.m, P.n, P.k2, m0, n0, (kt - kt1) * kBK, P.a2_tri, P.b2_tri);
+  Stage<BM, BK> ra;
+  Stage<BN, BK> rb;
+  auto load = [&](int kt) {
+    if (kt < kt1) {
+      const int k0 = kb1 + kt * BK;
+      stage_load<BM, BK>(ra, P.A, P.a_rs, P.a_cs, P.m, P.k, P.a_tri, fl & 3, m0, k0);
+      stage_load<BN, BK>(rb, P.B, P.b_cs, P.b_rs, P.n, P.k, bcode(P.b_tri), (fl >> 2) & 3, n0, k0);
+    } else {
+      const int k0 = kb2 + (kt - kt1) * BK;
+      stage_load<BM, BK>(ra, P.A2, P.a2_rs, P.a2_cs, P.m, P.k2, P.a2_tri, (fl >> 4) & 3, m0, k0);
+      stage_load<BN, BK>(rb, P.B2, P.b2_cs, P.b2_rs, P.n, P.k2, bcode(P.b2_tri), (fl >> 6) & 3, n0,
+                     k0);
+    }
+  };
+  auto store = [&](int kt, int buf) {
+    const int f = kt >= kt1 ? fl >> 4 : fl;
+    stage_store<BM, BK>(ra, sa[buf], f & 1);
+    stage_store<BN, BK>(rb, sb[buf], (f >> 2) & 1);
   };
 
   if (ktiles > 0) {
-    issue(0, 0);
-    cp_commit();
+    load(0);
+    store(0, 0);
+    __syncthreads();
   }
 #pragma unroll 1
   for (int kt = 0; kt < ktiles; ++kt) {
     const int buf = kt & 1;
-    if (kt + 1 < ktiles) {
-      issue(kt + 1, buf ^ 1);
-      cp_commit();
-      cp_wait<1>();
-    } else {
-      cp_wait<0>();
-    }
-    __syncthreads();
+    const bool more = kt + 1 < ktiles;
+    if (more) load(kt + 1);  // global loads in flight during the FMAs
 #pragma unroll
-    for (int kk = 0; kk < kBK; ++kk) {
+    for (int kk = 0; kk < BK; ++kk) {
       float a[TM], b[TN];
 #pragma unroll
       for (int g = 0; g < GM; ++g) {
-        float4 v = *reinterpret_cast<const float4*>(
-            &sm.a[buf][kk][g * (BM / GM) + tr * 4]);
+        const float4 v = *reinterpret_cast<const float4*>(
+            &sa[buf][kk][swz<BK>(g * (BM / GM) + tr * 4, kk)]);
         a[g * 4 + 0] = v.x; a[g * 4 + 1] = v.y;
         a[g * 4 + 2] = v.z; a[g * 4 + 3] = v.w;
       }
 #pragma unroll
       for (int g = 0; g < GN; ++g) {
-        float4 v = *reinterpret_cast<const float4*>(
-            &sm.b[buf][kk][g * (BN / GN) + tc * 4]);
+        const float4 v = *reinterpret_cast<const float4*>(
+            &sb[buf][kk][swz<BK>(g * (BN / GN) + tc * 4, kk)]);
         b[g * 4 + 0] = v.x; b[g * 4 + 1] = v.y;
         b[g * 4 + 2] = v.z; b[g * 4 + 3] = v.w;
       }
@@ -201,6 +260,7 @@ __global__ void __launch_bounds__(kThreads, 2) sgemm_batch(const Batch batch) {
 #pragma unroll
         for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
     }
+    if (more) store(kt + 1, buf ^ 1);
     __syncthreads();
   }
 

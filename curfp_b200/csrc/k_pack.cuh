@@ -20,7 +20,8 @@
 namespace rfp {
 namespace kpack {
 
-constexpr int TS = 32;     // tile edge
+constexpr int TS = 64;     // tile edge
+constexpr int TX = 32;     // threads along the contiguous dimension
 constexpr int TY = 8;      // thread rows (block = 32 x 8)
 
 struct PackBlock {
@@ -56,12 +57,50 @@ __device__ __forceinline__ void pack_tile_coords(const PackBlock& B, int lt,
   tq = lt - (int)((int64_t)r * (r + 1) / 2);
 }
 
-// to_rfp = 1: strttf (dense -> RFP); 0: stfttr (RFP -> dense).
+// One side of a tile copy: element (p, q) of the tile at base[p*sp + q*sq];
+// the warp runs along the side's contiguous dimension (qc = 1: q, else p).
+// 16 elements per thread, addressed by pointer increments.  dpq = p0 - q0 of
+// the tile (the stored-triangle test of a triangular block is p >= q).
+template <typename T, bool kLoad, bool kChecked>
+__device__ __forceinline__ void tile_pass(T (*tile)[TS + 1], T* base, int64_t sp, int64_t sq,
+                                          int qc, int prow, int qcol, int tri, int dpq,
+                                          T dscale, bool diag) {
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int64_t sc = qc ? sq : sp, so = qc ? sp : sq;  // contiguous / other stride
+  T* ptr = base + (int64_t)tx * sc + (int64_t)ty * so;
+#pragma unroll
+  for (int r = 0; r < TS / TY; ++r) {
+#pragma unroll
+    for (int h = 0; h < TS / TX; ++h) {
+      const int c = tx + TX * h, o = ty + TY * r;
+      const int lp = qc ? o : c, lq = qc ? c : o;
+      T* e = ptr + (int64_t)(TX * h) * sc + (int64_t)(TY * r) * so;
+      bool ok = true;
+      if (kChecked) ok = lp < prow && lq < qcol && (!tri || lp + dpq >= lq);  // p >= q
+      if (ok) {
+        if (kLoad) {
+          tile[lp][lq] = *e;
+        } else {
+          T v = tile[lp][lq];
+          if (kChecked && diag && lp == lq) v *= dscale;
+          *e = v;
+        }
+      }
+    }
+  }
+}
+
+// to_rfp = 1: strttf (dense -> RFP); 0: stfttr (RFP -> dense).  A 64 x 64
+// tile of an RFP block is read with the warp along the source's contiguous
+// dimension, transposed through shared memory when the two sides disagree,
+// and written with the warp along the destination's contiguous dimension,
+// so both HBM streams coalesce.  Tiles strictly inside their block (and, in
+// the triangles, strictly below the diagonal) take a path without per-element
+// bounds tests.
 template <typename T>
-__global__ void __launch_bounds__(TS * TY) pack_kernel(const PackArgs args,
+__global__ void __launch_bounds__(TX * TY) pack_kernel(const PackArgs args,
                                                        const T* __restrict__ src,
-                                                       T* __restrict__ dst,
-                                                       int to_rfp) {
+                                                       T* __restrict__ dst, int to_rfp) {
   __shared__ T tile[TS][TS + 1];
   int t = blockIdx.x, bi = 0;
   while (bi + 1 < args.nblocks && t >= args.b[bi + 1].tile_begin) ++bi;
@@ -69,45 +108,34 @@ __global__ void __launch_bounds__(TS * TY) pack_kernel(const PackArgs args,
   int tp, tq;
   pack_tile_coords(B, t - B.tile_begin, tp, tq);
   const int p0 = tp * TS, q0 = tq * TS;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-
-  // Contiguous dimension of each side: 0 -> p, 1 -> q.
+  const int prow = B.rows - p0, qcol = B.cols - q0;  // extent left in the block
+  const int64_t P0 = (int64_t)B.p_base + p0, Q0 = (int64_t)B.q_base + q0;
+  T* dense = const_cast<T*>(to_rfp ? src : dst) + P0 * args.drs + Q0 * args.dcs;
+  T* rfp = const_cast<T*>(to_rfp ? dst : src) + B.off + (int64_t)p0 * B.rs + (int64_t)q0 * B.cs;
   const int dense_q = (args.dcs == 1 || args.dcs == -1) ? 1 : 0;
-  const int rfp_q = (B.rs == 1 || B.rs == -1) ? 0 : 1;
-  const int src_q = to_rfp ? dense_q : rfp_q;
-  const int dst_q = to_rfp ? rfp_q : dense_q;
-
-  auto dense_ptr = [&](int p, int q) -> int64_t {
-    int64_t P = (int64_t)B.p_base + p, Q = (int64_t)B.q_base + q;
-    return P * args.drs + Q * args.dcs;
-  };
-  auto rfp_ptr = [&](int p, int q) -> int64_t {
-    return B.off + (int64_t)p * B.rs + (int64_t)q * B.cs;
-  };
-  auto inside = [&](int p, int q) -> bool {
-    return p < B.rows && q < B.cols && (!B.tri || p >= q);
-  };
-
-#pragma unroll
-  for (int r = 0; r < TS / TY; ++r) {
-    int lp, lq;
-    if (src_q) { lq = tx; lp = ty + r * TY; }
-    else       { lp = tx; lq = ty + r * TY; }
-    int p = p0 + lp, q = q0 + lq;
-    if (inside(p, q))
-      tile[lp][lq] = src[to_rfp ? dense_ptr(p, q) : rfp_ptr(p, q)];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int r = 0; r < TS / TY; ++r) {
-    int lp, lq;
-    if (dst_q) { lq = tx; lp = ty + r * TY; }
-    else       { lp = tx; lq = ty + r * TY; }
-    int p = p0 + lp, q = q0 + lq;
-    if (inside(p, q)) {
-      T v = tile[lp][lq];
-      if (to_rfp && B.p_base + p == B.q_base + q) v *= (T)args.diag_scale;
-      dst[to_rfp ? rfp_ptr(p, q) : dense_ptr(p, q)] = v;
+  const int rfp_q = (B.cs == 1 || B.cs == -1) ? 1 : 0;
+  const bool interior = prow >= TS && qcol >= TS && (!B.tri || q0 + TS <= p0);
+  const bool diag = to_rfp && B.tri && tp == tq && args.diag_scale != 1.0f;
+  const T ds = (T)args.diag_scale;
+  if (interior) {
+    if (to_rfp) {
+      tile_pass<T, true, false>(tile, dense, args.drs, args.dcs, dense_q, prow, qcol, B.tri, p0 - q0, ds, false);
+      __syncthreads();
+      tile_pass<T, false, false>(tile, rfp, B.rs, B.cs, rfp_q, prow, qcol, B.tri, p0 - q0, ds, false);
+    } else {
+      tile_pass<T, true, false>(tile, rfp, B.rs, B.cs, rfp_q, prow, qcol, B.tri, p0 - q0, ds, false);
+      __syncthreads();
+      tile_pass<T, false, false>(tile, dense, args.drs, args.dcs, dense_q, prow, qcol, B.tri, p0 - q0, ds, false);
+    }
+  } else {
+    if (to_rfp) {
+      tile_pass<T, true, true>(tile, dense, args.drs, args.dcs, dense_q, prow, qcol, B.tri, p0 - q0, ds, false);
+      __syncthreads();
+      tile_pass<T, false, true>(tile, rfp, B.rs, B.cs, rfp_q, prow, qcol, B.tri, p0 - q0, ds, diag);
+    } else {
+      tile_pass<T, true, true>(tile, rfp, B.rs, B.cs, rfp_q, prow, qcol, B.tri, p0 - q0, ds, false);
+      __syncthreads();
+      tile_pass<T, false, true>(tile, dense, args.drs, args.dcs, dense_q, prow, qcol, B.tri, p0 - q0, ds, false);
     }
   }
 }
