@@ -50,6 +50,10 @@ struct SharedTask {
 // Block sizes of the recursive algorithms.
 constexpr int kPotrfTile = 128;  // diagonal Cholesky tiles
 constexpr int kTrsmLeaf = 64;    // TRSM diagonal blocks (inverted, then multiplied)
+// Workspace record per 64-row TRSM block: [W_b | M_b], 64 x 64 each
+// (W_b = inv(L_bb); M_b = W_b L_{b,b-1}, written by executors whose
+// wavefront solve uses it).
+constexpr int kInvStride = 2 * kTrsmLeaf * kTrsmLeaf;
 constexpr int kTriTile = 64;     // trtri / lauum tiles
 constexpr int kTrmmLeaf = 64;    // TRMM leaves (masked in-place multiply)
 constexpr int kTrsvMaxRhs = 512; // wavefront solve for at most this many RHS
@@ -68,6 +72,7 @@ class Exec {
   virtual int potrf_tile(View L, int n, int info_base) = 0;
   // Inverses of the diagonal nb x nb blocks of lower L (n x n): block b is
   // written to W + b*nb*nb, column-major with ld nb, zeros above the diagonal.
+  // (W: nblk records of kInvStride floats, see kInvStride)
   virtual int trtri_blocks(View L, int n, int nb, float* W) = 0;
   // In-place inverse of lower L (n <= kTriTile).
   virtual int trtri_tile(View L, int n) = 0;

@@ -190,14 +190,18 @@ __global__ void __launch_bounds__(256) potrf_tile(View L, int n, int info_base, 
 // Inverse of lower-triangular diagonal blocks.  Block b = blockIdx.x covers
 // rows/cols [b*64, min(n, b*64+64)).  Thread c computes column c of the
 // inverse by forward substitution (all threads walk the same (i,k) so the
-// reads of the tile are broadcasts).  W != nullptr: block b is written to
-// W + b*64*64 (column-major, ld 64, zeros above the diagonal and outside the
-// block); W == nullptr: the inverse replaces the lower triangle in place.
+// reads of the tile are broadcasts).  W != nullptr: block b writes the record
+// W + b*kInvStride = [W_b | M_b], both 64 x 64 column-major (ld 64, zeros
+// outside the block): W_b = inv(L_bb) and, for b >= 1, M_b = W_b L_{b,b-1}
+// (the block left of the diagonal block), which lets the wavefront solve
+// finish a block row with one product after its predecessor is published.
+// W == nullptr: the inverse replaces the lower triangle in place.
 __global__ void __launch_bounds__(T) trtri_blocks(View L, int n, float* W,
                                                   const int* abort_flag) {
   if (abort_flag && *abort_flag != INT_MAX) return;
   __shared__ float s[T][LD];
   __shared__ float x[T][LD];
+  __shared__ float rd[T];
   const int b = blockIdx.x, r0 = b * T;
   const int sz = min(T, n - r0);
   const int c = threadIdx.x;
@@ -205,20 +209,48 @@ __global__ void __launch_bounds__(T) trtri_blocks(View L, int n, float* W,
   for (int i = 0; i < T; ++i) x[i][c] = 0.f;
   load_lower<LD>(Lb, sz, &s[0][0]);
   __syncthreads();
-  if (c < sz) {
-    x[c][c] = 1.0f / s[c][c];
-    for (int i = c + 1; i < sz; ++i) {
-      float acc = 0.f;
-      for (int k = c; k < i; ++k) acc = fmaf(s[i][k], x[k][c], acc);
-      x[i][c] = -acc / s[i][i];
+  if (c < sz) rd[c] = 1.0f / s[c][c];
+  __syncthreads();
+  // Column c by forward substitution with loop bounds uniform across the
+  // warp (x[k][c] = 0 for k < c) and four partial sums per row.
+  if (c < sz) x[c][c] = rd[c];
+  for (int i = 1; i < sz; ++i) {
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    int k = 0;
+    for (; k + 4 <= i; k += 4) {
+      a0 = fmaf(s[i][k], x[k][c], a0);
+      a1 = fmaf(s[i][k + 1], x[k + 1][c], a1);
+      a2 = fmaf(s[i][k + 2], x[k + 2][c], a2);
+      a3 = fmaf(s[i][k + 3], x[k + 3][c], a3);
     }
+    for (; k < i; ++k) a0 = fmaf(s[i][k], x[k][c], a0);
+    if (c < i) x[i][c] = -((a0 + a1) + (a2 + a3)) * rd[i];
   }
   __syncthreads();
-  if (W) {
-    float* Wb = W + (int64_t)b * T * T;
-    for (int j = 0; j < T; ++j) Wb[(int64_t)j * T + c] = (c < sz && j < sz) ? x[c][j] : 0.f;
-  } else {
+  if (!W) {
     store_lower<LD>(Lb, sz, &x[0][0]);
+    return;
+  }
+  float* Wb = W + (int64_t)b * kInvStride;
+  for (int j = 0; j < T; ++j) Wb[(int64_t)j * T + c] = (c < sz && j < sz) ? x[c][j] : 0.f;
+  if (b == 0) return;
+  // M_b = W_b L_{b,b-1}: the 64 x 64 block left of the diagonal block (rows
+  // beyond sz are zero); thread c forms column c, four rows at a time
+  // (independent accumulation chains; x is zero above its diagonal).
+  const View Lp = sub(L, r0, r0 - T);
+  for (int i = 0; i < T; ++i)
+    s[i][c] = i < sz ? Lp.p[(int64_t)i * Lp.rs + (int64_t)c * Lp.cs] : 0.f;
+  __syncthreads();
+  float* Mb = Wb + T * T;
+  for (int i0 = 0; i0 < T; i0 += 4) {
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int k = 0; k <= i0 + 3; ++k) {
+      const float sk = s[k][c];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = fmaf(x[i0 + q][k], sk, acc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) Mb[(int64_t)c * T + i0 + q] = i0 + q < sz ? acc[q] : 0.f;
   }
 }
 

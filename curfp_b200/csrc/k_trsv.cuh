@@ -1,16 +1,22 @@
-// k_trsv.cuh — wavefront triangular solve for few right-hand sides.
+// k_trsv.cuh — wavefront triangular solve.
 //
 // Solves L X = alpha B in place (L n x n lower, non-unit, any strided view;
-// B n x m view, m small) in ONE launch.  The rows are cut into 64-row blocks;
-// CTA tickets are handed out in (block row, 64-column RHS chunk) order by an
-// atomic counter, so a CTA only ever waits on CTAs holding smaller tickets,
-// which are already running or done: the scheme needs no co-residency and
-// cannot deadlock.  CTA (j, c) accumulates L_ji X_ic for i < j as soon as each
-// X_ic is published (flag per block, release/acquire through L2), then forms
-// X_jc = inv(L_jj) (alpha B_jc - acc) with the inverse of the diagonal block
-// precomputed by trtri_blocks, stores it and publishes its own flag.  Each
-// L tile is read once; the sequential chain is one tile product, one inverse
-// product and one flag hand-off per block row.
+// B n x m view) in ONE launch.  The rows are cut into 64-row blocks and the
+// right-hand sides into 64-column chunks; CTA tickets are handed out in
+// (block row, chunk) order by an atomic counter, so a CTA only ever waits on
+// CTAs holding smaller tickets, which are already running or done: the scheme
+// needs no co-residency and cannot deadlock.
+//
+// CTA (j, c) accumulates acc = sum_{i < j-1} L_ji X_ic as each X_ic is
+// published (flag per block, release/acquire through L2), with the L and X
+// tiles double-buffered in shared memory (the next pair is in flight while
+// the current one is multiplied: L by cp.async, X through registers with
+// L2-only loads, requested as soon as its flag is seen).  Then, still before
+// its predecessor is done, it forms Y = W_j (alpha B_jc - acc) with
+// W_j = inv(L_jj).  The one product left after X_{j-1,c} is published is
+// X_jc = Y - M_j X_{j-1,c} with M_j = W_j L_{j,j-1} (both from trtri_blocks),
+// so the sequential chain per block row is a flag hand-off, one tile load and
+// one 64^3 product.
 //
 // Waits are bounded (~2 s of wall time); on timeout a CTA records an error
 // code, publishes a poisoned flag (-1) so that every dependent CTA stops
@@ -19,14 +25,18 @@
 #include <climits>
 #include <cstdint>
 
+#include "engine.h"
 #include "rfp.h"
 
 namespace rfp {
 namespace ktrsv {
 
 constexpr int NB = 64;
+constexpr int LDL = NB + 1;  // L / W / M tiles: scalar reads down a row, conflict-free both ways
+constexpr int LDX = NB + 4;  // X / T tiles: float4 reads along a row
 constexpr uint64_t WAIT_NS = 2000000000ull;
-constexpr int SMEM = (NB * (NB + 1) * 2 + NB * (NB + 4)) * 4;  // Ls, Ws, Xs
+// Ls[2], Ws (L tiles; W_j; M_j reuses Ls[0]) and Xs[2], Ts (X tiles; B_jc / T)
+constexpr int SMEM = (3 * NB * LDL + 3 * NB * LDX) * 4;
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -41,18 +51,107 @@ __device__ __forceinline__ uint64_t gtimer() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+__device__ __forceinline__ void cp4(float* smem, const float* g, bool pred) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(g),
+               "r"(pred ? 4 : 0));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Read-only tile (rows x cols of a strided view; L) -> s[a][b] (row stride
+// LD) by cp.async, zero fill outside; the thread mapping follows the view's
+// contiguous dimension.  (cp.async of 4 bytes caches in L1, which is not
+// coherent with other CTAs' stores: only data that no CTA of this launch
+// writes goes this way.)
+template <int LD>
+__device__ __forceinline__ void load_tile(float* s, View v, int rows, int cols) {
+  const bool rowcont = (v.cs == 1 || v.cs == -1) && !(v.rs == 1 || v.rs == -1);
+#pragma unroll 4
+  for (int u = 0; u < 16; ++u) {
+    const int e = threadIdx.x + 256 * u;
+    const int a = rowcont ? e / NB : e % NB, b = rowcont ? e % NB : e / NB;
+    const bool ok = a < rows && b < cols;
+    cp4(s + a * LD + b, ok ? v.p + (int64_t)a * v.rs + (int64_t)b * v.cs : v.p, ok);
+  }
+}
+// Tile of B / X (written by CTAs of this launch): L2-only loads into
+// registers (ld.global.cg), stored to shared memory by store_regs.
+__device__ __forceinline__ void load_regs(float (&r)[16], View v, int rows, int cols) {
+  const bool rowcont = (v.cs == 1 || v.cs == -1) && !(v.rs == 1 || v.rs == -1);
+#pragma unroll
+  for (int u = 0; u < 16; ++u) {
+    const int e = threadIdx.x + 256 * u;
+    const int a = rowcont ? e / NB : e % NB, b = rowcont ? e % NB : e / NB;
+    r[u] = (a < rows && b < cols) ? __ldcg(v.p + (int64_t)a * v.rs + (int64_t)b * v.cs) : 0.f;
+  }
+}
+__device__ __forceinline__ void store_regs(float* s, const float (&r)[16], View v) {
+  const bool rowcont = (v.cs == 1 || v.cs == -1) && !(v.rs == 1 || v.rs == -1);
+#pragma unroll
+  for (int u = 0; u < 16; ++u) {
+    const int e = threadIdx.x + 256 * u;
+    const int a = rowcont ? e / NB : e % NB, b = rowcont ? e % NB : e / NB;
+    s[a * LDX + b] = r[u];
+  }
+}
+// 64 x 64 column-major workspace tile -> s[a][b] (row stride LDL).
+__device__ __forceinline__ void load_ws(float* s, const float* w) {
+#pragma unroll 4
+  for (int u = 0; u < 16; ++u) {
+    const int e = threadIdx.x + 256 * u;
+    cp4(s + (e % NB) * LDL + e / NB, w + e, true);
+  }
+}
+// acc (+)= sign * A(64 x 64, row stride LDL) * X(64 x 64, row stride LDX) on
+// the thread's 4 x 4 register tile (rows tr*4.., columns tc*4..).
+template <bool kSub>
+__device__ __forceinline__ void tile_mma(float (&acc)[4][4], const float* A, const float* X,
+                                         int tr, int tc) {
+#pragma unroll 8
+  for (int k = 0; k < NB; ++k) {
+    float a4[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) a4[q] = A[(tr * 4 + q) * LDL + k];
+    const float4 x = *reinterpret_cast<const float4*>(X + k * LDX + tc * 4);
+    const float x4[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        acc[p][q] = kSub ? fmaf(-a4[p], x4[q], acc[p][q]) : fmaf(a4[p], x4[q], acc[p][q]);
+  }
+}
+
+// Bounded wait by thread 0 for a flag to become non-zero; returns the flag
+// (-1 on timeout or poison).
+__device__ __forceinline__ int wait_flag(const int* f, int* err) {
+  int st = ld_acquire(f);
+  const uint64_t t0 = gtimer();
+  while (st == 0) {
+    st = ld_acquire(f);
+    if (st == 0 && gtimer() - t0 > WAIT_NS) {
+      atomicExch(err, 5);
+      st = -1;
+    }
+  }
+  return st;
+}
 
 // sync layout: sync[0] = ticket counter, sync[1 + b*nchunk + c] = flag of
 // block row b, chunk c (0 = not ready, 1 = ready, -1 = poisoned).
-// All zero at launch.
-__global__ void __launch_bounds__(256) trsm_wave(View L, int n, View B, int m, float alpha,
-                                                 const float* __restrict__ W, int* sync,
-                                                 int* err, const int* abort_flag) {
-  extern __shared__ float dyn_tsv[];
-  float (*Ls)[NB + 1] = reinterpret_cast<float (*)[NB + 1]>(dyn_tsv);
-  float (*Ws)[NB + 1] = reinterpret_cast<float (*)[NB + 1]>(dyn_tsv + NB * (NB + 1));
-  float (*Xs)[NB + 4] = reinterpret_cast<float (*)[NB + 4]>(dyn_tsv + 2 * NB * (NB + 1));
-  __shared__ int sh_ticket, sh_state;
+// All zero at launch.  W: kInvStride floats per block row ([W_j | M_j]).
+__global__ void __launch_bounds__(256, 2) trsm_wave(View L, int n, View B, int m, float alpha,
+                                                    const float* __restrict__ W, int* sync,
+                                                    int* err, const int* abort_flag) {
+  extern __shared__ __align__(16) float dyn_tsv[];
+  float* Ls0 = dyn_tsv;
+  float* Ls1 = Ls0 + NB * LDL;
+  float* Ws = Ls1 + NB * LDL;
+  float* Xs0 = Ws + NB * LDL;
+  float* Xs1 = Xs0 + NB * LDX;
+  float* Ts = Xs1 + NB * LDX;
+  __shared__ int sh_ticket, sh_state, sh_ready[2], sh_last;
   if (abort_flag && *abort_flag != INT_MAX) return;
   const int tid = threadIdx.x;
   const int nchunk = (m + NB - 1) / NB;
@@ -64,135 +163,113 @@ __global__ void __launch_bounds__(256) trsm_wave(View L, int n, View B, int m, f
   const int rows = min(NB, n - r0), cols = min(NB, m - c0);
   const int tr = tid / 16, tc = tid % 16;  // 4 x 4 register tile
   int* flags = sync + 1;
-  const bool l_rowcont = (L.cs == 1 || L.cs == -1);  // consecutive columns adjacent
-  const bool x_rowcont = (B.cs == 1 || B.cs == -1) && !(B.rs == 1 || B.rs == -1);
+  const View Bt = sub(B, r0, c0);
+  const float* Wj = W + (int64_t)j * kInvStride;
+  auto xview = [&](int i) { return sub(B, (int64_t)i * NB, c0); };
+  auto lview = [&](int i) { return sub(L, r0, (int64_t)i * NB); };
+
   float acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
 
-  // Loads that do not depend on other CTAs are issued up front / one tile
-  // ahead: the inverse W_j, the right-hand side block B_jc, the next L tile.
-  const View Bt = sub(B, r0, c0);
-  const float* Wj = W + (int64_t)j * NB * NB;
-  float br[16], lr[16];
-#pragma unroll
-  for (int u = 0; u < 16; ++u) {
-    const int e = tid + 256 * u;
-    Ws[e % NB][e / NB] = __ldg(Wj + e);
-  }
-#pragma unroll
-  for (int u = 0; u < 16; ++u) {
-    const int e = tid + 256 * u;
-    const int a = x_rowcont ? e / NB : e % NB, b = x_rowcont ? e % NB : e / NB;
-    br[u] = (a < rows && b < cols) ? __ldcg(Bt.p + (int64_t)a * Bt.rs + (int64_t)b * Bt.cs) : 0.f;
-  }
-  auto load_l = [&](int i) {
-    const View Lt = sub(L, r0, (int64_t)i * NB);
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-      const int e = tid + 256 * u;
-      const int a = l_rowcont ? e / NB : e % NB, b = l_rowcont ? e % NB : e / NB;
-      lr[u] = (a < rows) ? __ldg(Lt.p + (int64_t)a * Lt.rs + (int64_t)b * Lt.cs) : 0.f;
-    }
-  };
-  if (j > 0) load_l(0);
-
+  // Loads that depend on no other CTA: W_j, B_jc, the first L tile.
+  float xr[16];
+  load_ws(Ws, Wj);
+  load_regs(xr, Bt, rows, cols);
+  store_regs(Ts, xr, Bt);
+  const int iend = j - 1;  // products in the loop: i < iend
   bool poisoned = false;
-  for (int i = 0; i < j; ++i) {
-    if (tid == 0) {
-      int st = ld_acquire(&flags[i * nchunk + c]);
-      const uint64_t t0 = gtimer();
-      while (st == 0) {
-        st = ld_acquire(&flags[i * nchunk + c]);
-        if (st == 0 && gtimer() - t0 > WAIT_NS) {
-          atomicExch(err, 5);
-          st = -1;
+  if (iend > 0) {
+    load_tile<LDL>(Ls0, lview(0), rows, NB);
+    if (tid == 0) sh_state = wait_flag(&flags[c], err);
+    __syncthreads();
+    if (sh_state < 0) {
+      poisoned = true;
+    } else {
+      load_regs(xr, xview(0), NB, cols);
+      store_regs(Xs0, xr, xview(0));
+    }
+  }
+  cp_commit();
+
+  for (int i = 0; i < iend && !poisoned; ++i) {
+    float* Lb = (i & 1) ? Ls1 : Ls0;
+    float* Xb = (i & 1) ? Xs1 : Xs0;
+    float* Ln = (i & 1) ? Ls0 : Ls1;
+    float* Xn = (i & 1) ? Xs0 : Xs1;
+    const bool more = i + 1 < iend;
+    if (tid == 0) sh_ready[i & 1] = more ? ld_acquire(&flags[(i + 1) * nchunk + c]) : 0;
+    cp_wait_all();
+    __syncthreads();  // tile i landed; every thread is done with the other buffers
+    const bool ready = more && sh_ready[i & 1] > 0;
+    if (more) load_tile<LDL>(Ln, lview(i + 1), rows, NB);
+    cp_commit();
+    if (ready) load_regs(xr, xview(i + 1), NB, cols);
+    tile_mma<false>(acc, Lb, Xb, tr, tc);
+    if (more) {
+      if (!ready) {
+        if (tid == 0) sh_state = wait_flag(&flags[(i + 1) * nchunk + c], err);
+        __syncthreads();
+        if (sh_state < 0) {
+          poisoned = true;
+          break;
         }
+        load_regs(xr, xview(i + 1), NB, cols);
       }
-      sh_state = st;
+      store_regs(Xn, xr, xview(i + 1));
     }
-    __syncthreads();
-    if (sh_state < 0) { poisoned = true; break; }
-    const View Xt = sub(B, (int64_t)i * NB, c0);
-    float xr[16];
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-      const int e = tid + 256 * u;
-      const int a = x_rowcont ? e / NB : e % NB, b = x_rowcont ? e % NB : e / NB;
-      xr[u] = (b < cols) ? __ldcg(Xt.p + (int64_t)a * Xt.rs + (int64_t)b * Xt.cs) : 0.f;
-    }
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-      const int e = tid + 256 * u;
-      const int a = l_rowcont ? e / NB : e % NB, b = l_rowcont ? e % NB : e / NB;
-      Ls[a][b] = lr[u];
-    }
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-      const int e = tid + 256 * u;
-      const int a = x_rowcont ? e / NB : e % NB, b = x_rowcont ? e % NB : e / NB;
-      Xs[a][b] = xr[u];
-    }
-    __syncthreads();
-    if (i + 1 < j) load_l(i + 1);
-#pragma unroll 8
-    for (int k = 0; k < NB; ++k) {
-      float a4[4], x4[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        a4[q] = Ls[tr * 4 + q][k];
-        x4[q] = Xs[k][tc * 4 + q];
-      }
-#pragma unroll
-      for (int p = 0; p < 4; ++p)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[p][q] = fmaf(a4[p], x4[q], acc[p][q]);
-    }
-    __syncthreads();
   }
   if (poisoned) {
+    cp_wait_all();
+    __syncthreads();
     if (tid == 0) st_release(&flags[j * nchunk + c], -1);
     return;
   }
-  // T = alpha B_jc - acc (into Xs); W_j is already in Ws (column-major source)
-#pragma unroll
-  for (int u = 0; u < 16; ++u) {
-    const int e = tid + 256 * u;
-    const int a = x_rowcont ? e / NB : e % NB, b = x_rowcont ? e % NB : e / NB;
-    Xs[a][b] = alpha * br[u];
-  }
+
+  // T = alpha B_jc - acc, then Y = W_j T (into acc).  M_j goes to Ls0 and,
+  // if already published, X_{j-1} to registers while Y is formed.
+  if (tid == 0) sh_last = j > 0 ? ld_acquire(&flags[(j - 1) * nchunk + c]) : 0;
+  cp_wait_all();
   __syncthreads();
+  const bool ready = j > 0 && sh_last > 0;
+  if (j > 0) load_ws(Ls0, Wj + NB * NB);
+  cp_commit();
+  if (ready) load_regs(xr, xview(j - 1), NB, cols);
 #pragma unroll
   for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) Xs[tr * 4 + p][tc * 4 + q] -= acc[p][q];
-  __syncthreads();
-  float out[4][4];
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) out[p][q] = 0.f;
-#pragma unroll 8
-  for (int k = 0; k < NB; ++k) {
-    float w4[4], x4[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      w4[q] = Ws[tr * 4 + q][k];
-      x4[q] = Xs[k][tc * 4 + q];
+      float* tp = Ts + (tr * 4 + p) * LDX + tc * 4 + q;
+      *tp = fmaf(alpha, *tp, -acc[p][q]);
+      acc[p][q] = 0.f;
     }
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) out[p][q] = fmaf(w4[p], x4[q], out[p][q]);
+  __syncthreads();
+  tile_mma<false>(acc, Ws, Ts, tr, tc);
+  if (j > 0) {
+    if (!ready) {
+      if (tid == 0) sh_state = wait_flag(&flags[(j - 1) * nchunk + c], err);
+      __syncthreads();
+      if (sh_state < 0) {
+        cp_wait_all();
+        __syncthreads();
+        if (tid == 0) st_release(&flags[j * nchunk + c], -1);
+        return;
+      }
+      load_regs(xr, xview(j - 1), NB, cols);
+    }
+    store_regs(Xs0, xr, xview(j - 1));
+    cp_wait_all();
+    __syncthreads();
+    tile_mma<true>(acc, Ls0, Xs0, tr, tc);  // X_j = Y - M_j X_{j-1}
   }
 #pragma unroll
   for (int p = 0; p < 4; ++p)
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int a = tr * 4 + p, b = tc * 4 + q;
-      if (a < rows && b < cols) Bt.p[(int64_t)a * Bt.rs + (int64_t)b * Bt.cs] = out[p][q];
+      if (a < rows && b < cols) Bt.p[(int64_t)a * Bt.rs + (int64_t)b * Bt.cs] = acc[p][q];
     }
   __threadfence();
   __syncthreads();

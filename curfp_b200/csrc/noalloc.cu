@@ -11,7 +11,7 @@
 // variant takes that scratch from one file-scope device array instead.
 //
 // Scratch: g_solve_scratch holds kInvFloats floats of diagonal-block inverses
-// followed by kSyncWords 32-bit words of solve flags (2 MiB + 4 KiB), which
+// followed by kSyncWords 32-bit words of solve flags (4 MiB + 4 KiB), which
 // every GPU that loads the library keeps until the process exits.  Limits:
 // n <= 16384 (so each half is <= 8192 rows) and nrhs <= 512.  Every call
 // shares the array and leaves its contents behind; the flag words are
@@ -33,7 +33,7 @@ namespace {
 constexpr int kNoAllocMaxN = 16384;
 constexpr int kNoAllocMaxRhs = 512;
 constexpr size_t kHalfMax = kNoAllocMaxN / 2;
-constexpr size_t kInvFloats = kHalfMax * rfp::kTrsmLeaf;  // 64 x 64 inverses of one half
+constexpr size_t kInvFloats = (kHalfMax / rfp::kTrsmLeaf) * rfp::kInvStride;  // [W | M] records of one half
 constexpr size_t kWaveRows = 64;  // row / column block of the wavefront solve
 constexpr size_t kSyncWords = 1 + (kHalfMax / kWaveRows) * (kNoAllocMaxRhs / kWaveRows);
 

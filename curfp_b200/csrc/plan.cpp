@@ -38,7 +38,7 @@ inline GemmProb gemm_prob(View A, View B, View C, int m, int n, int k,
 int trsm_rec(Exec& ex, View L, int n, View B, int m, float alpha,
              const float* W, int blk0, int math) {
   if (n <= 0 || m <= 0) return 0;
-  const float* Wb = W + (int64_t)blk0 * kTrsmLeaf * kTrsmLeaf;
+  const float* Wb = W + (int64_t)blk0 * kInvStride;
   if (n <= kTrsmLeaf) {
     View Wv{const_cast<float*>(Wb), 1, kTrsmLeaf};
     GemmProb p = gemm_prob(Wv, B, B, n, m, n, alpha, 0.0f, 0);
@@ -67,7 +67,7 @@ int trsm_rec(Exec& ex, View L, int n, View B, int m, float alpha,
 int trsm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math) {
   if (n <= 0 || m <= 0) return 0;
   int nblk = (n + kTrsmLeaf - 1) / kTrsmLeaf;
-  float* W = ex.workspace((size_t)nblk * kTrsmLeaf * kTrsmLeaf);
+  float* W = ex.workspace((size_t)nblk * kInvStride);
   if (!W) return 2;
   int rc = ex.trtri_blocks(L, n, kTrsmLeaf, W);
   if (rc) return rc;

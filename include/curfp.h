@@ -184,7 +184,7 @@ curfpStatus_t curfpSsfmmAcc64(curfpHandle_t handle, curfpOperation_t transr,
  * another allocator, or a cudaMalloc's possible synchronisation or failure
  * is not acceptable in their loop).  The solve's scratch (inverted diagonal
  * blocks and wavefront flags) lives in one static device array of
- * 2 MiB + 4 KiB that each GPU loading the library keeps until exit.
+ * 4 MiB + 4 KiB that each GPU loading the library keeps until exit.
  * Limits: n <= 16384, nrhs <= 512 (larger sizes return
  * CURFP_STATUS_INVALID_VALUE).  The array's device address is fetched on the
  * first call per device (make that call before any stream capture).  All

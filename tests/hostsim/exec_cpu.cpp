@@ -98,7 +98,7 @@ class CpuExec : public Exec {
     for (int b = 0; b * nb < n; ++b) {
       int r0 = b * nb, sz = std::min(nb, n - r0);
       inv_lower(L, r0, sz, X);
-      float* Wb = W + (int64_t)b * nb * nb;
+      float* Wb = W + (int64_t)b * kInvStride;
       for (int j = 0; j < nb; ++j)
         for (int i = 0; i < nb; ++i)
           Wb[(int64_t)j * nb + i] = (i < sz && j < sz && i >= j) ? (float)X[(size_t)i * sz + j] : 0.f;
@@ -145,7 +145,7 @@ class CpuExec : public Exec {
           for (int k = 0; k < r0; ++k) s -= (double)at(L, r0 + a, k) * at(B, k, c);
           T[(size_t)a * m + c] = s;
         }
-      const float* Wj = W + (int64_t)j * NB * NB;
+      const float* Wj = W + (int64_t)j * kInvStride;
       for (int a = 0; a < rows; ++a)
         for (int c = 0; c < m; ++c) {
           double s = 0;
