@@ -4,37 +4,41 @@
 // power of two s_i >= max_k |x_ik| and written as three integer digits,
 //     x_ik = s_i * 2^-7 * (d0 + d1 * 2^-8 + d2 * 2^-16),  |d_t| <= 128,
 // each digit exact in BF16 (8 significant bits); the truncation is at most
-// 2^-24 s_i.  The six products whose weight is >= 2^-16,
-//     level 0: d0*d0     level 1: d0*d1 + d1*d0     level 2: d0*d2 + d2*d0 + d1*d1,
-// are BF16 tensor-core products summed in three FP32 accumulators in tensor
-// memory.  Digit products are integers <= 2^14, so over a chunk of 1024 of
-// the K dimension the level-0 sum is an integer of magnitude <= 2^24 and its
-// tensor-core accumulation is EXACT (the accumulator's truncation never drops
-// a bit); the level-1 / level-2 sums may exceed 2^24 by a few bits, and the
-// bits their truncation can drop weigh at most 2^-30 of the result.  After
-// each chunk the epilogue warps fold the three level sums into an FP32
-// register accumulator with round-to-nearest:
-//     acc += L0 + (L1 + L2 * 2^-8) * 2^-8,
-// and at the end C := alpha * s_i s_j 2^-14 * acc + beta * C.  Rounding errors
-// are then those of K/1024 round-to-nearest additions plus the 2^-24 s digit
-// truncation: FP32-level accuracy from BF16 tensor cores.  (Summing floating
-// BF16 splits directly in one accumulator loses several bits: tcgen05
-// accumulation rounds toward zero at every step.)
+// 2^-24 s_i.  The staged BF16 planes are  h = d0, m = d1, l' = 2^-8 d2 and
+// m' = 2^-8 d1 (power-of-two scalings of small integers: exact).  The six
+// products whose weight is >= 2^-16 go to two FP32 accumulators in tensor
+// memory:
+//     L0  = h*h
+//     L12 = h*m + m*h + h*l' + l'*h + m*m'   (= level 1 + 2^-8 level 2)
+// Digit products are integers <= 2^14, so over a chunk of 1024 of the K
+// dimension L0 is an integer of magnitude <= 2^24 and its tensor-core
+// accumulation is EXACT; L12 carries 2^-8 of the result's weight, so the bits
+// its round-toward-zero accumulation drops weigh at most ~2^-23 of the result
+// over a chunk (typically far less).  After each chunk the epilogue warps fold
+// the two sums into an FP32 register accumulator with round-to-nearest,
+//     acc += L0 + L12 * 2^-8,
+// and at the end C := alpha * s_i s_j 2^-14 * acc + beta * C: FP32-level
+// accuracy from BF16 tensor cores.  (Summing floating BF16 splits directly in
+// one accumulator loses several bits: tcgen05 accumulation rounds toward zero
+// at every step, which is why L0 is kept apart and exact.)
 //
-// Kernel shape: one CTA per 128 x 128 output tile, 256 threads.
-//   warp 0   : TMA producer — per K-block of 32, six boxes (A d0/d1/d2 and
-//              B d0/d1/d2, 128 x 32 BF16 each, SWIZZLE_64B) into a 4-stage
-//              shared-memory ring, completion on an mbarrier;
+// Kernel shape: persistent, one CTA of 256 threads per SM walking a static
+// list of 128 x 128 output tiles (triangular tasks list only the tiles of
+// their triangle).
+//   warp 0   : TMA producer — per K-block of 32, seven boxes (A h/m/l' and
+//              B h/m/l'/m', 128 x 32 BF16 each, SWIZZLE_64B) into a 4-stage
+//              shared-memory ring that runs across tiles;
 //   warp 1   : MMA issuer — one elected thread issues, per 16-deep K step,
-//              the six digit products as four tcgen05.mma.cta_group::1.kind::f16
-//              (two M=128 N=256 over adjacent B planes, two M=128 N=128) into
-//              the level accumulators; tcgen05.commit frees the stage and
-//              signals the end of each 1024-deep chunk;
-//   warp 2   : allocates / frees the tensor memory (3 x 128 columns used);
-//   warps 4-7: epilogue — per chunk, tcgen05.ld of the three level sums of
-//              their TMEM lane quarter into registers; at the end C is
-//              written through an arbitrary strided FP32 view (RFP block,
-//              any variant) with lower/upper masking.
+//              five tcgen05.mma.cta_group::1.kind::f16 (one M=128 N=256 over
+//              the adjacent B planes h|m, four M=128 N=128); tcgen05.commit
+//              frees the stage and signals the end of each 1024-deep chunk;
+//   warp 2   : allocates / frees the tensor memory: two accumulator buffers
+//              of 256 columns (L0 | L12), chunk g using buffer g & 1, so the
+//              MMAs of one chunk overlap the epilogue of the previous one;
+//   warps 4-7: epilogue — per chunk, tcgen05.ld of the two sums of their TMEM
+//              lane quarter into registers, then release of the buffer; per
+//              tile, C is written through an arbitrary strided FP32 view (RFP
+//              block, any variant) with lower/upper masking.
 // Operands come from dense K-major staging buffers written by digits_kernel,
 // so every TMA box is 16-byte aligned whatever the RFP variant's leading
 // dimension or block offset.
@@ -55,13 +59,16 @@
 namespace rfp {
 namespace ktc {
 
-constexpr int BM = 128, BN = 128, BK = 32, STAGES = 4, PLANES = 3;
-constexpr int CHUNK_KB = 32;                                // 32 x 32 = 1024 deep
-constexpr int A_BYTES = BM * BK * 2;                        // 8 KB
-constexpr int B_BYTES = BN * BK * 2;                        // 8 KB
-constexpr int STAGE_BYTES = PLANES * (A_BYTES + B_BYTES);   // 48 KB
+constexpr int BM = 128, BN = 128, BK = 32, STAGES = 4;
+constexpr int PLANES = 4;    // staged digit planes: h, m, l' = 2^-8 d2, m' = 2^-8 d1
+constexpr int PLANES_A = 3;  // planes read for the A side: h, m, l'
+constexpr int CHUNK_KB = 32;                                    // 32 x 32 = 1024 deep
+constexpr int A_BYTES = BM * BK * 2;                            // 8 KB
+constexpr int B_BYTES = BN * BK * 2;                            // 8 KB
+constexpr int STAGE_BYTES = PLANES_A * A_BYTES + PLANES * B_BYTES;  // 56 KB
 constexpr int THREADS = 256;
-constexpr int TMEM_COLS = 512;                              // 3 x 128 used
+constexpr int ACC_COLS = 2 * BN;                                // one buffer: L0 | L12
+constexpr int TMEM_COLS = 512;                                  // two buffers
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 constexpr int MAX_TASKS = 4;
 constexpr uint32_t WAIT_LIMIT = 1u << 24;          // polls per wait
@@ -83,12 +90,14 @@ struct Task {
   int64_t c_rs, c_cs;
   float alpha, beta;
   int c_mask;  // 0 full, 1: write i >= j only, 2: write i <= j only
+  int tri;     // 1: square task whose tile list is its mask's triangle only
   int tiles_m, tiles_n, tile_begin;
 };
 
 struct Batch {
   Task t[MAX_TASKS];
   int count;
+  int total_tiles;
   int kblocks;
   const float* a_scale;   // per staged row of A: s_i (power of two)
   const float* b_scale;   // per staged row of B
@@ -203,27 +212,40 @@ __device__ __forceinline__ void tmem_wait() {
 }
 
 
+// Tile g of the batch's tile list -> task index, m0, n0.
+__device__ __forceinline__ int tile_of(const Batch& batch, int g, int& m0, int& n0) {
+  int ti = 0;
+  while (ti + 1 < batch.count && g >= batch.t[ti + 1].tile_begin) ++ti;
+  const Task& T = batch.t[ti];
+  const int lt = g - T.tile_begin;
+  int r, c;
+  if (T.tri) {
+    r = (int)((sqrtf(8.0f * (float)lt + 1.0f) - 1.0f) * 0.5f);
+    while ((r + 1) * (r + 2) / 2 <= lt) ++r;
+    while (r * (r + 1) / 2 > lt) --r;
+    c = lt - r * (r + 1) / 2;  // c <= r
+    if (T.c_mask == 2) { const int x = r; r = c; c = x; }
+  } else {
+    r = lt % T.tiles_m;
+    c = lt / T.tiles_m;
+  }
+  m0 = r * BM;
+  n0 = c * BN;
+  return ti;
+}
+
 __global__ void __launch_bounds__(THREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
                    const __grid_constant__ CUtensorMap tmB, const Batch batch) {
   if (batch.abort_flag && *batch.abort_flag != INT_MAX) return;
-  // Locate task and tile; tiles entirely outside a triangular mask exit.
-  int t = blockIdx.x, ti_ = 0;
-  while (ti_ + 1 < batch.count && t >= batch.t[ti_ + 1].tile_begin) ++ti_;
-  const Task& T = batch.t[ti_];
-  const int lt = t - T.tile_begin;
-  const int m0 = (lt % T.tiles_m) * BM, n0 = (lt / T.tiles_m) * BN;
-  if (T.c_mask == 1 && m0 + BM - 1 < n0) return;       // all i < j
-  if (T.c_mask == 2 && n0 + BN - 1 < m0) return;       // all i > j
-
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
   uint64_t* empty = full + STAGES;
-  uint64_t* chunk_full = empty + STAGES;
-  uint64_t* drained = chunk_full + 1;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
+  uint64_t* acc_full = empty + STAGES;   // [2]: MMA -> epilogue, per chunk
+  uint64_t* acc_empty = acc_full + 2;    // [2]: epilogue -> MMA, per chunk
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
   volatile int* abort_sh = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -232,8 +254,10 @@ __global__ void __launch_bounds__(THREADS, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(chunk_full, 1);
-    mbar_init(drained, 128);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 128);
+    }
     *abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -249,100 +273,122 @@ __global__ void __launch_bounds__(THREADS, 1)
   const uint32_t tmem = *tmem_slot;
   const int KB = batch.kblocks;
   const int NCHUNK = (KB + CHUNK_KB - 1) / CHUNK_KB;
+  const int G = gridDim.x;
 
   if (warp == 0) {
     if (lane == 0) {
       // ---------------- TMA producer ----------------
-      for (int kb = 0; kb < KB; ++kb) {
-        const int s = kb % STAGES;
-        const uint32_t ph = (kb / STAGES) & 1;
-        if (kb >= STAGES && !mbar_wait(&empty[s], ph ^ 1, abort_sh, batch.err_flag, 1)) break;
-        uint8_t* st = smem + s * STAGE_BYTES;
-        mbar_expect_tx(&full[s], STAGE_BYTES);
-        const int k0 = kb * BK;
+      uint32_t it = 0;  // ring position over all tiles of this CTA
+      bool ok = true;
+      for (int g = blockIdx.x; g < batch.total_tiles && ok; g += G) {
+        int m0, n0;
+        const Task& T = batch.t[tile_of(batch, g, m0, n0)];
+        for (int kb = 0; kb < KB; ++kb, ++it) {
+          const int s = it % STAGES;
+          const uint32_t ph = (it / STAGES) & 1;
+          if (it >= STAGES && !mbar_wait(&empty[s], ph ^ 1, abort_sh, batch.err_flag, 1)) {
+            ok = false;
+            break;
+          }
+          uint8_t* st = smem + s * STAGE_BYTES;
+          mbar_expect_tx(&full[s], STAGE_BYTES);
+          const int k0 = kb * BK;
 #pragma unroll
-        for (int p = 0; p < PLANES; ++p) {
-          tma_load_3d(st + p * A_BYTES, &tmA, k0, T.a_row0 + m0, p, &full[s]);
-          tma_load_3d(st + PLANES * A_BYTES + p * B_BYTES, &tmB, k0, T.b_row0 + n0, p,
-                      &full[s]);
+          for (int p = 0; p < PLANES_A; ++p)
+            tma_load_3d(st + p * A_BYTES, &tmA, k0, T.a_row0 + m0, p, &full[s]);
+#pragma unroll
+          for (int p = 0; p < PLANES; ++p)
+            tma_load_3d(st + PLANES_A * A_BYTES + p * B_BYTES, &tmB, k0, T.b_row0 + n0, p,
+                        &full[s]);
         }
       }
       // Drain: no copy may still be landing when the CTA exits.
-      for (int kb = KB - STAGES < 0 ? 0 : KB - STAGES; kb < KB; ++kb)
-        mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, abort_sh, nullptr, 0);
+      for (uint32_t j = it > (uint32_t)STAGES ? it - STAGES : 0u; j < it; ++j)
+        mbar_wait(&full[j % STAGES], (j / STAGES) & 1, abort_sh, nullptr, 0);
     }
   } else if (warp == 1) {
     if (lane == 0) {
       // ---------------- MMA issuer ----------------
-      int kb = 0;
-      for (int c = 0; c < NCHUNK; ++c) {
-        if (c > 0) {
-          if (!mbar_wait(drained, (c - 1) & 1, abort_sh, batch.err_flag, 4)) break;
-          tc_fence_after();
-        }
-        uint32_t started = 0;  // 0 until the chunk's first K-step is issued
-        const int kb_end = (kb + CHUNK_KB < KB) ? kb + CHUNK_KB : KB;
-        bool ok = true;
-        for (; kb < kb_end; ++kb) {
-          const int s = kb % STAGES;
-          const uint32_t ph = (kb / STAGES) & 1;
-          if (!mbar_wait(&full[s], ph, abort_sh, batch.err_flag, 2)) { ok = false; break; }
-          tc_fence_after();
-          const uint32_t a0 = su32(smem + s * STAGE_BYTES);
-          const uint32_t b0 = a0 + PLANES * A_BYTES;
-          // Six digit products in four instructions.  The B digit planes are
-          // adjacent in shared memory, so B_hi|B_mid is one 256-row operand and
-          // an N=256 MMA writes two neighbouring 128-column level sums:
-          //   A_hi  x [B_hi|B_mid] -> L0 (cols 0..127), L1 (128..255)
-          //   A_hi  x  B_lo        -> L2 (256..383)
-          //   A_mid x [B_hi|B_mid] -> L1, L2   (accumulating)
-          //   A_lo  x  B_hi        -> L2       (accumulating)
-          // The first two start a chunk (accumulate flag 0 initialises
-          // L0, L1 and L2); the last two always accumulate.
-#pragma unroll
-          for (int kk = 0; kk < BK / 16; ++kk) {
-            const uint32_t ak = a0 + kk * 32, bk = b0 + kk * 32;
-            mma_bf16(tmem, sdesc(ak), sdesc(bk), IDESC2, started);
-            mma_bf16(tmem + 2 * BN, sdesc(ak), sdesc(bk + 2 * B_BYTES), IDESC, started);
-            mma_bf16(tmem + BN, sdesc(ak + A_BYTES), sdesc(bk), IDESC2, 1u);
-            mma_bf16(tmem + 2 * BN, sdesc(ak + 2 * A_BYTES), sdesc(bk), IDESC, 1u);
-            started = 1u;
+      uint32_t it = 0, gc = 0;  // ring position, chunk counter
+      bool ok = true;
+      for (int g = blockIdx.x; g < batch.total_tiles && ok; g += G) {
+        int kb = 0;
+        for (int c = 0; c < NCHUNK && ok; ++c, ++gc) {
+          const uint32_t b = gc & 1, use = gc >> 1;
+          if (use > 0) {
+            if (!mbar_wait(&acc_empty[b], (use - 1) & 1, abort_sh, batch.err_flag, 4)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
           }
-          mma_commit(&empty[s]);
+          const uint32_t tb = tmem + b * ACC_COLS;  // L0 at tb, L12 at tb + BN
+          uint32_t started = 0;  // 0 until the chunk's first K-step is issued
+          const int kb_end = (kb + CHUNK_KB < KB) ? kb + CHUNK_KB : KB;
+          for (; kb < kb_end; ++kb, ++it) {
+            const int s = it % STAGES;
+            const uint32_t ph = (it / STAGES) & 1;
+            if (!mbar_wait(&full[s], ph, abort_sh, batch.err_flag, 2)) { ok = false; break; }
+            tc_fence_after();
+            const uint32_t a0 = su32(smem + s * STAGE_BYTES);
+            const uint32_t b0 = a0 + PLANES_A * A_BYTES;
+            // Planes: A h, m, l' at a0 + {0,1,2} * A_BYTES; B h, m, l', m' at
+            // b0 + {0,1,2,3} * B_BYTES.  B h|m is one 256-row operand, so the
+            // first MMA writes L0 and starts L12 in one N = 256 instruction:
+            //   A_h  x [B_h|B_m] -> L0, L12
+            //   A_h  x  B_l'     -> L12
+            //   A_m  x  B_h      -> L12
+            //   A_m  x  B_m'     -> L12
+            //   A_l' x  B_h      -> L12
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk) {
+              const uint32_t ak = a0 + kk * 32, bk = b0 + kk * 32;
+              mma_bf16(tb, sdesc(ak), sdesc(bk), IDESC2, started);
+              mma_bf16(tb + BN, sdesc(ak), sdesc(bk + 2 * B_BYTES), IDESC, 1u);
+              mma_bf16(tb + BN, sdesc(ak + A_BYTES), sdesc(bk), IDESC, 1u);
+              mma_bf16(tb + BN, sdesc(ak + A_BYTES), sdesc(bk + 3 * B_BYTES), IDESC, 1u);
+              mma_bf16(tb + BN, sdesc(ak + 2 * A_BYTES), sdesc(bk), IDESC, 1u);
+              started = 1u;
+            }
+            mma_commit(&empty[s]);
+          }
+          mma_commit(&acc_full[b]);
         }
-        mma_commit(chunk_full);
-        if (!ok) break;
       }
     }
   } else if (warp >= 4) {
     // ---------------- epilogue ----------------
     const int q = warp - 4;
-    const uint32_t tq = tmem + ((uint32_t)(q * 32) << 16);
-    float acc[BN];
-#pragma unroll
-    for (int j = 0; j < BN; ++j) acc[j] = 0.f;
+    const uint32_t lane_off = (uint32_t)(q * 32) << 16;
+    uint32_t gc = 0;
     bool ok = true;
-    for (int c = 0; c < NCHUNK; ++c) {
-      bool w = mbar_wait(chunk_full, c & 1, abort_sh, batch.err_flag, 3);
-      ok = __all_sync(0xffffffffu, w && !*abort_sh);
-      if (!ok) break;
-      tc_fence_after();
+    for (int g = blockIdx.x; g < batch.total_tiles && ok; g += G) {
+      int m0, n0;
+      const Task& T = batch.t[tile_of(batch, g, m0, n0)];
+      float acc[BN];
 #pragma unroll
-      for (int c0 = 0; c0 < BN; c0 += 16) {
-        uint32_t l0[16], l1[16], l2[16];
-        tmem_ld16(tq + (uint32_t)c0, l0);
-        tmem_ld16(tq + (uint32_t)(BN + c0), l1);
-        tmem_ld16(tq + (uint32_t)(2 * BN + c0), l2);
-        tmem_wait();
+      for (int j = 0; j < BN; ++j) acc[j] = 0.f;
+      for (int c = 0; c < NCHUNK; ++c, ++gc) {
+        const uint32_t b = gc & 1, use = gc >> 1;
+        const bool w = mbar_wait(&acc_full[b], use & 1, abort_sh, batch.err_flag, 3);
+        ok = __all_sync(0xffffffffu, w && !*abort_sh);
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t tq = tmem + b * ACC_COLS + lane_off;
 #pragma unroll
-        for (int j = 0; j < 16; ++j)
-          acc[c0 + j] += __uint_as_float(l0[j]) +
-                         (__uint_as_float(l1[j]) + __uint_as_float(l2[j]) * 0x1p-8f) * 0x1p-8f;
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+          uint32_t l0[16], l12[16];
+          tmem_ld16(tq + (uint32_t)c0, l0);
+          tmem_ld16(tq + (uint32_t)(BN + c0), l12);
+          tmem_wait();
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            acc[c0 + j] += __uint_as_float(l0[j]) + __uint_as_float(l12[j]) * 0x1p-8f;
+        }
+        tc_fence_before();
+        mbar_arrive(&acc_empty[b]);
       }
-      tc_fence_before();
-      mbar_arrive(drained);
-    }
-    if (ok) {
+      if (!ok) break;
       const int r = q * 32 + lane;
       const int gi = m0 + r;
       if (gi < T.m) {
@@ -354,10 +400,10 @@ __global__ void __launch_bounds__(THREADS, 1)
           if (gj >= T.n) break;
           if (T.c_mask == 1 && gj > gi) break;
           if (T.c_mask == 2 && gj < gi) continue;
-          float* c = crow + (int64_t)gj * T.c_cs;
+          float* cp = crow + (int64_t)gj * T.c_cs;
           float out = T.alpha * (acc[j] * (sa * batch.b_scale[T.b_row0 + gj]));
-          if (T.beta != 0.f) out = fmaf(T.beta, *c, out);
-          *c = out;
+          if (T.beta != 0.f) out = fmaf(T.beta, *cp, out);
+          *cp = out;
         }
       }
     }
@@ -446,15 +492,16 @@ __global__ void __launch_bounds__(256) rowscale_kernel(View X, int rows, int k,
   }
 }
 
-// Digits of X (see the header): three BF16 planes, row-major with K
-// contiguous, out[p][i][j], plane stride rows_pad * k_pad; zero padding.
-// A block stages a 32 x 64 tile through shared memory (the warp reads along
-// X's contiguous dimension) and writes BF16 pairs (128 bytes per warp store).
-// Grid (k_pad/64, rows_pad/32), block (32, 8); k_pad is a multiple of 64.
+// Digits of X (see the header): nplanes (3 or 4) BF16 planes h = d0, m = d1,
+// l' = 2^-8 d2 and m' = 2^-8 d1, row-major with K contiguous, out[p][i][j],
+// plane stride rows_pad * k_pad; zero padding.  A block stages a 32 x 64 tile
+// through shared memory (the warp reads along X's contiguous dimension) and
+// writes BF16 pairs (128 bytes per warp store).  Grid (k_pad/64, rows_pad/32),
+// block (32, 8); k_pad is a multiple of 64.
 __global__ void __launch_bounds__(256) digits_kernel(View X, int rows, int k,
                                                      const float* __restrict__ scale,
                                                      __nv_bfloat16* out, int rows_pad,
-                                                     int k_pad) {
+                                                     int k_pad, int nplanes) {
   __shared__ float t[32][65];
   const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 64;
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -473,7 +520,7 @@ __global__ void __launch_bounds__(256) digits_kernel(View X, int rows, int k,
   for (int r = 0; r < 4; ++r) {
     const int lr = ty + 8 * r;
     const float inv = 1.0f / scale[r0 + lr];            // power of two: exact
-    float d[3][2];
+    float d[4][2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const float y0 = t[lr][2 * tx + h] * inv * 128.0f;  // |y0| <= 128, exact
@@ -483,13 +530,15 @@ __global__ void __launch_bounds__(256) digits_kernel(View X, int rows, int k,
       const float y2 = (y1 - d1) * 256.0f;                // exact
       d[0][h] = d0;
       d[1][h] = d1;
-      d[2][h] = rintf(y2);
+      d[2][h] = rintf(y2) * 0x1p-8f;                      // exact scalings
+      d[3][h] = d1 * 0x1p-8f;
     }
     const int64_t o = (int64_t)(r0 + lr) * k_pad + c0 + 2 * tx;
 #pragma unroll
-    for (int p = 0; p < 3; ++p)  // integers <= 128: exact in BF16
-      *reinterpret_cast<__nv_bfloat162*>(out + o + p * plane) =
-          __floats2bfloat162_rn(d[p][0], d[p][1]);
+    for (int p = 0; p < 4; ++p)  // integers <= 128 times powers of two: exact in BF16
+      if (p < nplanes)
+        *reinterpret_cast<__nv_bfloat162*>(out + o + p * plane) =
+            __floats2bfloat162_rn(d[p][0], d[p][1]);
   }
 }
 

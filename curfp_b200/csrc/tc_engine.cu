@@ -1,6 +1,6 @@
 // tc_engine.cu — host side of the split-BF16 tensor-core contraction:
-// operand staging (FP32 -> 3 BF16 planes), TMA descriptors, task tiling and
-// the launch of ktc::tc_gemm_kernel on the handle's stream.
+// operand staging (FP32 -> BF16 digit planes), TMA descriptors, the tile list
+// and the persistent launch of ktc::tc_gemm_kernel on the handle's stream.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -36,32 +36,34 @@ EncodeTiledFn encode_fn() {
 inline int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
 struct Staged {
-  __nv_bfloat16* p;   // 3 digit planes
+  __nv_bfloat16* p;   // digit planes
   float* scale;       // per-row power-of-two scales
   int rows_pad;
   int k_pad;
+  int planes;
 };
 
-// Stage X (rows x k) as row scales + 3 BF16 digit planes in a context
+// Stage X (rows x k) as row scales + `planes` BF16 digit planes in a context
 // staging buffer (two kernels: row maxima, then digits).
-int stage(curfpContext* ctx, void** buf, size_t* cur, View X, int rows, int k,
+int stage(curfpContext* ctx, void** buf, size_t* cur, View X, int rows, int k, int planes,
           Staged* out) {
   out->rows_pad = (int)(round_up(rows, ktc::BN) + ktc::BN);
   out->k_pad = (int)round_up(k, 64);
+  out->planes = planes;
   const size_t plane_bytes =
-      (size_t)3 * out->rows_pad * out->k_pad * sizeof(__nv_bfloat16);
+      (size_t)planes * out->rows_pad * out->k_pad * sizeof(__nv_bfloat16);
   const size_t off = (size_t)round_up((int64_t)plane_bytes, 256);
   void* p = grow_buffer(ctx, buf, cur, off + (size_t)out->rows_pad * sizeof(float));
   if (!p) return 2;
   out->p = static_cast<__nv_bfloat16*>(p);
   out->scale = reinterpret_cast<float*>(static_cast<char*>(p) + off);
   ProfScope ps(ctx->prof, ctx->stream, K_TC_STAGE, 0,
-               (double)rows * k * 8.0 + (double)out->rows_pad * out->k_pad * 6.0);
+               (double)rows * k * 8.0 + (double)out->rows_pad * out->k_pad * 2.0 * planes);
   ktc::rowscale_kernel<<<out->rows_pad / 32, 256, 0, ctx->stream>>>(X, rows, k, out->scale,
                                                                    out->rows_pad);
   dim3 grid(out->k_pad / 64, out->rows_pad / 32);
   ktc::digits_kernel<<<grid, dim3(32, 8), 0, ctx->stream>>>(X, rows, k, out->scale, out->p,
-                                                            out->rows_pad, out->k_pad);
+                                                            out->rows_pad, out->k_pad, planes);
   ctx->launches += 2;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
@@ -69,7 +71,7 @@ int stage(curfpContext* ctx, void** buf, size_t* cur, View X, int rows, int k,
 int make_map(const Staged& s, int box_rows, CUtensorMap* map) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return 4;
-  cuuint64_t dims[3] = {(cuuint64_t)s.k_pad, (cuuint64_t)s.rows_pad, 3};
+  cuuint64_t dims[3] = {(cuuint64_t)s.k_pad, (cuuint64_t)s.rows_pad, (cuuint64_t)s.planes};
   cuuint64_t strides[2] = {(cuuint64_t)s.k_pad * 2, (cuuint64_t)s.k_pad * 2 * s.rows_pad};
   cuuint32_t box[3] = {(cuuint32_t)ktc::BK, (cuuint32_t)box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
@@ -89,11 +91,15 @@ int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, Vie
                 int brows, int k, const SharedTask* tasks, int count) {
   if (count <= 0 || k <= 0) return 0;
   if (count > ktc::MAX_TASKS) return 3;
+  // The A side reads planes h, m, l'; the B side also m'.  A shared operand
+  // is staged once with all four.
   Staged sa, sb;
-  int rc = stage(ctx, &ctx->stage, &ctx->stage_bytes, A, arows, k, &sa);
+  int rc = stage(ctx, &ctx->stage, &ctx->stage_bytes, A, arows, k,
+                 B.p ? ktc::PLANES_A : ktc::PLANES, &sa);
   if (rc) return rc;
   if (B.p) {
-    if ((rc = stage(ctx, &ctx->stage2, &ctx->stage2_bytes, B, brows, k, &sb))) return rc;
+    if ((rc = stage(ctx, &ctx->stage2, &ctx->stage2_bytes, B, brows, k, ktc::PLANES, &sb)))
+      return rc;
   } else {
     sb = sa;
   }
@@ -114,11 +120,14 @@ int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, Vie
     t.c_mask = s.c_lower;  // 0 full, 1 lower, 2 upper
     t.tiles_m = (s.m + ktc::BM - 1) / ktc::BM;
     t.tiles_n = (s.n + ktc::BN - 1) / ktc::BN;
+    // a masked square task lists only the tiles of its triangle
+    t.tri = (t.c_mask != 0 && s.m == s.n) ? 1 : 0;
     t.tile_begin = tiles;
-    tiles += t.tiles_m * t.tiles_n;
+    tiles += t.tri ? t.tiles_m * (t.tiles_m + 1) / 2 : t.tiles_m * t.tiles_n;
   }
   if (cnt == 0) return 0;
   b.count = cnt;
+  b.total_tiles = tiles;
   b.kblocks = sa.k_pad / ktc::BK;
   b.a_scale = sa.scale;
   b.b_scale = sb.scale;
@@ -131,8 +140,14 @@ int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, Vie
       return 4;
     attr_set = true;
   }
+  static int sms = 0;
+  if (!sms && (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) !=
+                   cudaSuccess ||
+               sms <= 0))
+    return 4;
+  const int grid = tiles < sms ? tiles : sms;  // persistent: one CTA per SM
   ProfScope ps(ctx->prof, ctx->stream, K_TC_GEMM, flops, 0);
-  ktc::tc_gemm_kernel<<<tiles, ktc::THREADS, ktc::SMEM_BYTES, ctx->stream>>>(mA, mB, b);
+  ktc::tc_gemm_kernel<<<grid, ktc::THREADS, ktc::SMEM_BYTES, ctx->stream>>>(mA, mB, b);
   ++ctx->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
