@@ -23,6 +23,7 @@
 #include <cstdint>
 
 #include "engine.h"
+#include "k_order.cuh"
 
 namespace rfp {
 namespace kgemm {
@@ -50,20 +51,12 @@ struct Batch {
   const int* abort_flag;  // if non-null and *abort_flag != INT_MAX: no-op
 };
 
-// Map a linear tile index of a problem to (ti, tj).
+// Map a linear tile index of a problem to (ti, tj), in the L2-friendly
+// orders of k_order.cuh (c_lower problems: lower tile triangle).
 __device__ __forceinline__ void tile_coords(const Prob& P, int lt, int& ti,
                                             int& tj) {
-  if (!P.c_lower) {
-    ti = lt % P.tiles_m;
-    tj = lt / P.tiles_m;
-    return;
-  }
-  // Lower triangle of a square tile grid, row-major: lt = ti(ti+1)/2 + tj.
-  int r = (int)((sqrt(8.0 * (double)lt + 1.0) - 1.0) * 0.5);
-  while ((int64_t)(r + 1) * (r + 2) / 2 <= lt) ++r;
-  while ((int64_t)r * (r + 1) / 2 > lt) --r;
-  ti = r;
-  tj = lt - (int)((int64_t)r * (r + 1) / 2);
+  if (!P.c_lower) order::grouped_tile(P.tiles_m, P.tiles_n, lt, ti, tj);
+  else order::tri_band_tile(P.tiles_m, lt, ti, tj);
 }
 
 // Shared-memory operand tiles are k-major, s[kk][r] with r the tile row (m

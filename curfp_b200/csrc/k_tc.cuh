@@ -24,7 +24,7 @@
 //
 // Kernel shape: persistent, one CTA of 256 threads per SM walking a static
 // list of 128 x 128 output tiles (triangular tasks list only the tiles of
-// their triangle).
+// their triangle) in the L2-friendly orders of k_order.cuh.
 //   warp 0   : TMA producer — per K-block of 32, seven boxes (A h/m/l' and
 //              B h/m/l'/m', 128 x 32 BF16 each, SWIZZLE_64B) into a 4-stage
 //              shared-memory ring that runs across tiles;
@@ -54,6 +54,7 @@
 #include <climits>
 #include <cstdint>
 
+#include "k_order.cuh"
 #include "rfp.h"
 
 namespace rfp {
@@ -220,14 +221,10 @@ __device__ __forceinline__ int tile_of(const Batch& batch, int g, int& m0, int& 
   const int lt = g - T.tile_begin;
   int r, c;
   if (T.tri) {
-    r = (int)((sqrtf(8.0f * (float)lt + 1.0f) - 1.0f) * 0.5f);
-    while ((r + 1) * (r + 2) / 2 <= lt) ++r;
-    while (r * (r + 1) / 2 > lt) --r;
-    c = lt - r * (r + 1) / 2;  // c <= r
+    order::tri_band_tile(T.tiles_m, lt, r, c);  // c <= r
     if (T.c_mask == 2) { const int x = r; r = c; c = x; }
   } else {
-    r = lt % T.tiles_m;
-    c = lt / T.tiles_m;
+    order::grouped_tile(T.tiles_m, T.tiles_n, lt, r, c);
   }
   m0 = r * BM;
   n0 = c * BN;
@@ -394,16 +391,27 @@ __global__ void __launch_bounds__(THREADS, 1)
       if (gi < T.m) {
         const float sa = batch.a_scale[T.a_row0 + gi] * 0x1p-14f;
         float* crow = T.C + (int64_t)gi * T.c_rs;
+        const bool rd = T.beta != 0.f;
+        // 16-column slices: all loads of a slice (C for beta != 0, column
+        // scales) are issued before its stores, so their latencies overlap.
 #pragma unroll
-        for (int j = 0; j < BN; ++j) {
-          const int gj = n0 + j;
-          if (gj >= T.n) break;
-          if (T.c_mask == 1 && gj > gi) break;
-          if (T.c_mask == 2 && gj < gi) continue;
-          float* cp = crow + (int64_t)gj * T.c_cs;
-          float out = T.alpha * (acc[j] * (sa * batch.b_scale[T.b_row0 + gj]));
-          if (T.beta != 0.f) out = fmaf(T.beta, *cp, out);
-          *cp = out;
+        for (int j0 = 0; j0 < BN; j0 += 16) {
+          float cv[16], bs[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int gj = n0 + j0 + j;
+            const bool v = gj < T.n && (T.c_mask != 1 || gj <= gi) && (T.c_mask != 2 || gj >= gi);
+            bs[j] = v ? batch.b_scale[T.b_row0 + gj] : 0.f;
+            cv[j] = (v && rd) ? crow[(int64_t)gj * T.c_cs] : 0.f;
+          }
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int gj = n0 + j0 + j;
+            const bool v = gj < T.n && (T.c_mask != 1 || gj <= gi) && (T.c_mask != 2 || gj >= gi);
+            float out = T.alpha * (acc[j0 + j] * (sa * bs[j]));
+            if (rd) out = fmaf(T.beta, cv[j], out);
+            if (v) crow[(int64_t)gj * T.c_cs] = out;
+          }
         }
       }
     }
