@@ -168,7 +168,7 @@ int CudaExec::trtri_blocks(View L, int n, int nb, float* W) {
   if (nb != ktile::T) return 3;
   int nblk = (n + nb - 1) / nb;
   ProfScope ps(ctx_->prof, ctx_->stream, K_TRTRI, (double)n * nb * nb / 3.0, 0);
-  ktile::trtri_blocks<<<nblk, ktile::T, 0, ctx_->stream>>>(L, n, W, abort_);
+  ktile::trtri_blocks<<<nblk, ktile::TRTRI_THREADS, 0, ctx_->stream>>>(L, n, W, abort_);
   ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
@@ -177,7 +177,7 @@ int CudaExec::trtri_tile(View L, int n) {
   if (n <= 0) return 0;
   if (n > ktile::T) return 3;
   ProfScope ps(ctx_->prof, ctx_->stream, K_TRTRI, (double)n * n * n / 3.0, 0);
-  ktile::trtri_blocks<<<1, ktile::T, 0, ctx_->stream>>>(L, n, nullptr, abort_);
+  ktile::trtri_blocks<<<1, ktile::TRTRI_THREADS, 0, ctx_->stream>>>(L, n, nullptr, abort_);
   ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }

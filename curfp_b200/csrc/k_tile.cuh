@@ -188,70 +188,132 @@ __global__ void __launch_bounds__(256) potrf_tile(View L, int n, int info_base, 
 }
 
 // Inverse of lower-triangular diagonal blocks.  Block b = blockIdx.x covers
-// rows/cols [b*64, min(n, b*64+64)).  Thread c computes column c of the
-// inverse by forward substitution (all threads walk the same (i,k) so the
-// reads of the tile are broadcasts).  W != nullptr: block b writes the record
+// rows/cols [b*64, min(n, b*64+64)); 256 threads.  The two 32 x 32 diagonal
+// quarters are inverted in registers by warps 0 and 1 (lane = row, right-
+// looking: row j of the inverse is final once scaled by 1/D_jj, then is
+// broadcast to the rows below), and the off-diagonal quarter follows as
+// inv([D0 0; B D1]) = [inv(D0) 0; -inv(D1) (B inv(D0))  inv(D1)] by two
+// 32 x 32 products over all threads.  W != nullptr: block b writes the record
 // W + b*kInvStride = [W_b | M_b], both 64 x 64 column-major (ld 64, zeros
 // outside the block): W_b = inv(L_bb) and, for b >= 1, M_b = W_b L_{b,b-1}
 // (the block left of the diagonal block), which lets the wavefront solve
 // finish a block row with one product after its predecessor is published.
 // W == nullptr: the inverse replaces the lower triangle in place.
-__global__ void __launch_bounds__(T) trtri_blocks(View L, int n, float* W,
-                                                  const int* abort_flag) {
+constexpr int TRTRI_THREADS = 256;
+
+__global__ void __launch_bounds__(TRTRI_THREADS) trtri_blocks(View L, int n, float* W,
+                                                              const int* abort_flag) {
   if (abort_flag && *abort_flag != INT_MAX) return;
-  __shared__ float s[T][LD];
-  __shared__ float x[T][LD];
-  __shared__ float rd[T];
+  __shared__ float s[T][LD];  // L_bb, later the block left of it
+  __shared__ float x[T][LD];  // the inverse (upper-right quarter: scratch)
   const int b = blockIdx.x, r0 = b * T;
   const int sz = min(T, n - r0);
-  const int c = threadIdx.x;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   const View Lb = sub(L, r0, r0);
-  for (int i = 0; i < T; ++i) x[i][c] = 0.f;
-  load_lower<LD>(Lb, sz, &s[0][0]);
-  __syncthreads();
-  if (c < sz) rd[c] = 1.0f / s[c][c];
-  __syncthreads();
-  // Column c by forward substitution with loop bounds uniform across the
-  // warp (x[k][c] = 0 for k < c) and four partial sums per row.
-  if (c < sz) x[c][c] = rd[c];
-  for (int i = 1; i < sz; ++i) {
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-    int k = 0;
-    for (; k + 4 <= i; k += 4) {
-      a0 = fmaf(s[i][k], x[k][c], a0);
-      a1 = fmaf(s[i][k + 1], x[k + 1][c], a1);
-      a2 = fmaf(s[i][k + 2], x[k + 2][c], a2);
-      a3 = fmaf(s[i][k + 3], x[k + 3][c], a3);
-    }
-    for (; k < i; ++k) a0 = fmaf(s[i][k], x[k][c], a0);
-    if (c < i) x[i][c] = -((a0 + a1) + (a2 + a3)) * rd[i];
+  // both buffers start at zero: the quarter products read whole 32 x 32
+  // quarters, also rows beyond a partial last block
+  for (int e = tid; e < T * LD; e += TRTRI_THREADS) {
+    (&x[0][0])[e] = 0.f;
+    (&s[0][0])[e] = 0.f;
   }
   __syncthreads();
+  load_lower<LD>(Lb, sz, &s[0][0]);
+  __syncthreads();
+  if (warp < 2) {
+    const int q0 = warp * 32, w = min(32, sz - q0);
+    if (w > 0) {
+      float a[32], xr[32];
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        a[k] = (lane < w && k <= lane) ? s[q0 + lane][q0 + k] : 0.f;
+        xr[k] = (k == lane && lane < w) ? 1.f : 0.f;
+      }
+      const float rl = lane < w ? 1.0f / s[q0 + lane][q0 + lane] : 0.f;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        if (j < w) {
+          const float sc = lane == j ? rl : 1.f;
+#pragma unroll
+          for (int k = 0; k <= j; ++k) {
+            xr[k] *= sc;
+            const float v = __shfl_sync(0xffffffffu, xr[k], j);
+            if (lane > j) xr[k] = fmaf(-a[j], v, xr[k]);
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 32; ++k) x[q0 + lane][q0 + k] = xr[k];
+    }
+  }
+  __syncthreads();
+  if (sz > 32) {
+    // T = B inv(D0) into the upper-right quarter (inv(D0) zero above its
+    // diagonal, so the sums may run over all k)
+    for (int e = tid; e < 1024; e += TRTRI_THREADS) {
+      const int i = e >> 5, j = e & 31;
+      float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+      for (int k = 0; k < 32; k += 2) {
+        a0 = fmaf(s[32 + i][k], x[k][j], a0);
+        a1 = fmaf(s[32 + i][k + 1], x[k + 1][j], a1);
+      }
+      x[i][32 + j] = a0 + a1;
+    }
+    __syncthreads();
+    // lower-left = -inv(D1) T
+    for (int e = tid; e < 1024; e += TRTRI_THREADS) {
+      const int i = e >> 5, j = e & 31;
+      float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+      for (int k = 0; k < 32; k += 2) {
+        a0 = fmaf(x[32 + i][32 + k], x[k][32 + j], a0);
+        a1 = fmaf(x[32 + i][33 + k], x[k + 1][32 + j], a1);
+      }
+      x[32 + i][j] = -(a0 + a1);
+    }
+    __syncthreads();
+    for (int e = tid; e < 1024; e += TRTRI_THREADS) x[e >> 5][32 + (e & 31)] = 0.f;
+    __syncthreads();
+  }
   if (!W) {
     store_lower<LD>(Lb, sz, &x[0][0]);
     return;
   }
   float* Wb = W + (int64_t)b * kInvStride;
-  for (int j = 0; j < T; ++j) Wb[(int64_t)j * T + c] = (c < sz && j < sz) ? x[c][j] : 0.f;
+  for (int e = tid; e < T * T; e += TRTRI_THREADS) Wb[e] = x[e & 63][e >> 6];
   if (b == 0) return;
   // M_b = W_b L_{b,b-1}: the 64 x 64 block left of the diagonal block (rows
-  // beyond sz are zero); thread c forms column c, four rows at a time
-  // (independent accumulation chains; x is zero above its diagonal).
+  // beyond sz are zero), 4 x 4 outputs per thread.
   const View Lp = sub(L, r0, r0 - T);
-  for (int i = 0; i < T; ++i)
+  for (int e = tid; e < T * T; e += TRTRI_THREADS) {
+    const int i = e >> 6, c = e & 63;
     s[i][c] = i < sz ? Lp.p[(int64_t)i * Lp.rs + (int64_t)c * Lp.cs] : 0.f;
+  }
   __syncthreads();
-  float* Mb = Wb + T * T;
-  for (int i0 = 0; i0 < T; i0 += 4) {
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    for (int k = 0; k <= i0 + 3; ++k) {
-      const float sk = s[k][c];
+  const int ri = (tid >> 4) * 4, ci = (tid & 15) * 4;
+  float acc[4][4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) acc[q] = fmaf(x[i0 + q][k], sk, acc[q]);
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[p][q] = 0.f;
+#pragma unroll 4
+  for (int k = 0; k < T; ++k) {
+    float x4[4], s4[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      x4[p] = x[ri + p][k];
+      s4[p] = s[k][ci + p];
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) Mb[(int64_t)c * T + i0 + q] = i0 + q < sz ? acc[q] : 0.f;
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[p][q] = fmaf(x4[p], s4[q], acc[p][q]);
   }
+  float* Mb = Wb + T * T;
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) Mb[(int64_t)(ci + q) * T + ri + p] = acc[p][q];
 }
 
 // In-place L := L^T L (lower part) for an n x n tile, n <= 64.
