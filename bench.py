@@ -131,6 +131,18 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
+def profiled_traffic():
+    """DRAM bytes per tc_gemm_kernel launch of this step, from the ncu capture
+    summarised in profiles/tc_gemm_kernel-bench-n32768-traffic.txt (None if
+    the summary is absent)."""
+    import re
+    f = ROOT / "profiles" / "tc_gemm_kernel-bench-n32768-traffic.txt"
+    if not f.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch\s+([0-9.eE+]+)", f.read_text())
+    return float(m.group(1)) if m else None
+
+
 def measured_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -384,7 +396,7 @@ def run_ours(args, rank, world, local):
             peak = peaks["bf16_tflops"] / 6.0
             roof = {"kernel": "tc_gemm_kernel (split-BF16 tcgen05)", "bound": "tensor",
                     "achieved": round(ach, 2), "peak": round(peak, 2), "unit": "TFLOP/s",
-                    "frac": round(ach / peak, 4), "traffic": None,
+                    "frac": round(ach / peak, 4), "traffic": profiled_traffic(),
                     "note": f"FP32-equivalent flops; peak = {peaks['source']} bf16 "
                             f"{peaks['bf16_tflops']} TFLOP/s / 6 products",
                     "share_of_step": round(prof[dom]["ms"] / sum(t for t in times), 3)}
