@@ -100,18 +100,29 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+_COLL_DEVICE = "cuda"  # device of collective tensors: cuda (NCCL) or cpu (gloo)
+
+
 def dist_setup():
+    """One process per GPU (torchrun env vars).  NCCL when CUDA is present,
+    gloo otherwise (the replica logic is exercised on CPU that way)."""
+    global _COLL_DEVICE
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
+    cuda = torch.cuda.is_available()
+    if cuda:
+        torch.cuda.set_device(local)
     if world > 1:
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        # short timeout: ranks that wait for each other fail instead of hanging
+        kw = {"device_id": torch.device("cuda", local)} if cuda else {}
+        dist.init_process_group("nccl" if cuda else "gloo",
+                                timeout=datetime.timedelta(seconds=120), **kw)
+        _COLL_DEVICE = "cuda" if cuda else "cpu"
     return rank, world, local
 
 
@@ -126,7 +137,7 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_COLL_DEVICE)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -175,20 +186,21 @@ def cpu_baseline(n_sample: int = CPU_SAMPLE_N, nrhs: int = 64, reps: int = 2) ->
 def run_reference(args, rank, world):
     if rank != 0:
         return
+    ns = args.cpu_n
     for _ in range(max(0, args.warmup)):
-        cpu_baseline(reps=1)
-    vals = [cpu_baseline(reps=1)["value"] for _ in range(args.steps)]
-    cb = cpu_baseline(reps=1)
+        cpu_baseline(ns, reps=1)
+    vals = [cpu_baseline(ns, reps=1)["value"] for _ in range(args.steps)]
+    cb = cpu_baseline(ns, reps=1)
     v = statistics.median(vals)
-    ms = chol_solve_flops(CPU_SAMPLE_N, args.nrhs) / (v * 1e12) * 1e3
+    ms = chol_solve_flops(ns, args.nrhs) / (v * 1e12) * 1e3
     cb["value"] = v
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "TFLOP/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"RFP Cholesky+solve on host LAPACK, sample n={CPU_SAMPLE_N}, "
+            "config": {"workload": f"RFP Cholesky+solve on host LAPACK, sample n={ns}, "
                                    f"nrhs={args.nrhs}, transr=T, uplo=U",
-                       "n": CPU_SAMPLE_N, "nrhs": args.nrhs, "parallelism": "host"},
+                       "n": ns, "nrhs": args.nrhs, "parallelism": "host"},
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -438,7 +450,7 @@ def run_ours(args, rank, world, local):
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cb = cpu_baseline()
+        cb = cpu_baseline(args.cpu_n)
     fb = None
     if not args.no_nll:
         fb = nll_fwd_bwd(local)
@@ -555,6 +567,8 @@ def main():
     ap.add_argument("--no-other", action="store_true")
     ap.add_argument("--no-nll", action="store_true")
     ap.add_argument("--case", choices=CASES, default=None)
+    ap.add_argument("--cpu-n", type=int, default=CPU_SAMPLE_N,
+                    help="host LAPACK sample size (cpu_baseline and --impl reference)")
     args = ap.parse_args()
     if args.case:
         run_case(args)
