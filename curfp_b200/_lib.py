@@ -42,6 +42,7 @@ SIGNATURES = {
     "curfpSsfmmAcc64": [_h, _i, _i, _i, _i, ctypes.POINTER(_f), _p, _p, _i,
                         ctypes.POINTER(_f), _p, _i],
     "curfpGetKernelLaunchCount": [_h, ctypes.POINTER(ctypes.c_longlong)],
+    "curfpReleaseWorkspace": [_h],
     "curfpSpftrsNoAlloc": [_h, _i, _i, _i, _i, _p, _p, _i],
     "curfpSsfrkBackward": [_h, _i, _i, _i, _i, _i, ctypes.POINTER(_f), _p, _i, _p, _p, _i],
     "curfpSpftrfBackward": [_h, _i, _i, _i, _p, _p, _p, _i],

@@ -196,6 +196,32 @@ curfpStatus_t curfpDestroy(curfpHandle_t handle) {
   return CURFP_STATUS_SUCCESS;
 }
 
+// Not in the reference (its workspace is allocated and freed per call,
+// src/curfp_spftrf.cpp:231-232); here workspaces are handle-owned and grow.
+curfpStatus_t curfpReleaseWorkspace(curfpHandle_t handle) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (cudaStreamSynchronize(handle->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return CURFP_STATUS_EXECUTION_FAILED;
+  }
+  void** bufs[] = {&handle->ws, &handle->stage, &handle->stage2, &handle->ws2,
+                   &handle->ws3, &handle->tsv, &handle->wsg};
+  size_t* sizes[] = {&handle->ws_bytes, &handle->stage_bytes, &handle->stage2_bytes,
+                     &handle->ws2_bytes, &handle->ws3_bytes, &handle->tsv_bytes,
+                     &handle->wsg_bytes};
+  bool ok = true;
+  for (int i = 0; i < 7; ++i) {
+    if (*bufs[i]) ok &= cudaFree(*bufs[i]) == cudaSuccess;
+    *bufs[i] = nullptr;
+    *sizes[i] = 0;
+  }
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, handle->device) == cudaSuccess)
+    ok &= cudaMemPoolTrimTo(pool, 0) == cudaSuccess;
+  cudaGetLastError();
+  return ok ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
+}
+
 // src/curfp_handle.cpp:37-43
 curfpStatus_t curfpSetStream(curfpHandle_t handle, cudaStream_t stream) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;

@@ -35,6 +35,9 @@ EncodeTiledFn encode_fn() {
 
 inline int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
+constexpr size_t kStageBudget = (size_t)4 << 30;  // staged bytes per operand
+constexpr int64_t kStageSlab = 1024;              // k granularity of a split
+
 struct Staged {
   __nv_bfloat16* p;   // digit planes
   float* scale;       // per-row power-of-two scales
@@ -87,10 +90,10 @@ bool tc_worthwhile(int m, int n, int k) {
   return m >= 128 && n >= 128 && k >= 128 && (double)m * n * k >= 6.7e7;
 }
 
-int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, View B,
-                int brows, int k, const SharedTask* tasks, int count) {
-  if (count <= 0 || k <= 0) return 0;
-  if (count > ktc::MAX_TASKS) return 3;
+namespace {
+
+int tc_slab(curfpContext* ctx, const int* abort_flag, View A, int arows, View B, int brows,
+            int k, const SharedTask* tasks, int count) {
   // The A side reads planes h, m, l'; the B side also m'.  A shared operand
   // is staged once with all four.
   Staged sa, sb;
@@ -150,6 +153,38 @@ int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, Vie
   ktc::tc_gemm_kernel<<<grid, ktc::THREADS, ktc::SMEM_BYTES, ctx->stream>>>(mA, mB, b);
   ++ctx->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+}  // namespace
+
+// Contractions whose staged digit planes would exceed kStageBudget bytes per
+// operand are split along k into slabs; C accumulates across the slabs
+// (beta = 1 after the first).  Bounds the staging memory of the large
+// trailing updates (n = 131072: a 65536 x 65536 operand would take 34 GB of
+// planes) at the cost of one extra read-modify-write of C per slab.
+int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, View B,
+                int brows, int k, const SharedTask* tasks, int count) {
+  if (count <= 0 || k <= 0) return 0;
+  if (count > ktc::MAX_TASKS) return 3;
+  const int rows = B.p && brows > arows ? brows : arows;
+  const size_t per_k = (size_t)(round_up(rows, ktc::BN) + ktc::BN) * ktc::PLANES *
+                       sizeof(__nv_bfloat16);
+  int64_t kc = (int64_t)(kStageBudget / per_k) / kStageSlab * kStageSlab;
+  if (kc < kStageSlab) kc = kStageSlab;
+  if (kc >= k) return tc_slab(ctx, abort_flag, A, arows, B, brows, k, tasks, count);
+  const int64_t nslab = (k + kc - 1) / kc;  // balanced slabs
+  kc = round_up((k + nslab - 1) / nslab, kStageSlab);
+  SharedTask t[ktc::MAX_TASKS];
+  for (int i = 0; i < count; ++i) t[i] = tasks[i];
+  for (int64_t k0 = 0; k0 < k; k0 += kc) {
+    const int kk = (int)(k - k0 < kc ? k - k0 : kc);
+    const View As = sub(A, 0, k0);
+    const View Bs = B.p ? sub(B, 0, k0) : B;
+    int rc = tc_slab(ctx, abort_flag, As, arows, Bs, brows, kk, t, count);
+    if (rc) return rc;
+    for (int i = 0; i < count; ++i) t[i].beta = 1.0f;
+  }
+  return 0;
 }
 
 }  // namespace rfp

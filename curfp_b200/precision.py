@@ -133,6 +133,13 @@ def launch_count() -> int:
     return c.value
 
 
+def release_workspace() -> None:
+    """Free the current device handle's workspaces and trim the device pool
+    (they grow again on demand)."""
+    h = _get_handle()
+    check(h._lib.curfpReleaseWorkspace(h.ptr))
+
+
 KERNEL_CLASSES = ["sgemm", "tc_gemm", "tc_stage", "potrf_tile", "trtri", "lauum",
                   "pack", "diag", "symm_acc64", "trsv_wave"]
 

@@ -243,6 +243,13 @@ curfpStatus_t curfpSgpnllBackward(curfpHandle_t handle, curfpOperation_t transr,
                                   float *Xbar, int ldxbar, double *sums,
                                   curfpMath_t math);
 
+/* Release the handle's workspaces (staging planes of the split-BF16 path,
+ * refinement and adjoint scratch): waits for the handle's stream, frees every
+ * buffer and returns the device pool's unused memory to the driver.  The
+ * buffers grow again on demand; the next call of a routine re-allocates what
+ * it needs.  At n = 131072 the split-BF16 Cholesky stages up to ~52 GB. */
+curfpStatus_t curfpReleaseWorkspace(curfpHandle_t handle);
+
 /* Number of kernels launched through this handle since its creation. */
 curfpStatus_t curfpGetKernelLaunchCount(curfpHandle_t handle, long long *count);
 

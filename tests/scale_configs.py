@@ -1,0 +1,629 @@
+#!/usr/bin/env python
+"""Scale workloads of the RFP path on one GPU, one JSON line per result.
+
+Run as a script (pytest does not collect it):
+
+  python tests/scale_configs.py c2 [--n 32768 32767] [--variants all|TU]
+      Plain FP32 drop-in at n in {32767, 32768}, k = 1024, all 8 variants:
+      ssfrk, spftrf, spftrs (64 RHS) and spftri through the C ABI, per-op
+      ms / TFLOP/s / algorithmic GB/s, beside the reference's own GPU build
+      (oracle/_ref/libcurfp_ref.so, cuBLAS/cuSOLVER) on the same input, with
+      FP64 checks of both: ||C - L L^T||_F / ||C||_F, solve backward error,
+      inverse residual, and ours-vs-reference differences.
+  python tests/scale_configs.py lapack [--n 32768 32767]
+      Host LAPACK (scipy/OpenBLAS, all threads) ssfrk / spftrf / spftrs /
+      spftri at the same sizes, transr=T uplo=U, one run each.
+  python tests/scale_configs.py c3 [--lam 0.1 0.001]
+      Precision form at n = 65536, k = 2048, 256 RHS, per shift lambda:
+      split-BF16 ssfrk + spftrf + FP64-residual refined spftrs against the
+      plain FP32 form, errors against the exact FP64 solution.
+  python tests/scale_configs.py c5
+      n = 131072, k = 4096, lambda = 1e-2: split-BF16 ssfrk + spftrf + refined
+      spftrs (64 RHS), then the fused GP NLL forward + backward (X = A, s = 1,
+      sigma2 = lambda), with the loss and gradient against exact FP64 values.
+
+The FP64 oracle of C3 / C5 is exact and needs no n x n factorization: for
+C = A A^T + lam I with A (n x k, its FP32 values, n > k) the Woodbury
+identity gives C^-1 B = (B - A G^-1 A^T B) / lam with G = A^T A + lam I
+(k x k, FP64 Cholesky), the residual B - C X = B - A (A^T X) - lam X, and
+from the eigenvalues s_i of A^T A: ||C||_2 = max s_i + lam,
+cond_2(C) = ||C||_2 / lam, log det C = (n-k) log lam + sum log(s_i + lam),
+tr C^-1 = (n-k)/lam + sum 1/(s_i + lam).  Inputs are seeded numpy
+default_rng draws: A ~ N(0,1)/sqrt(k) (n x k float32), B ~ N(0,1).
+Timing: CUDA events on the default stream (the library handle's stream),
+`--warmup` untimed runs then the median of `--reps`; the input of each
+in-place routine is restored (untimed) before every run.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import statistics
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+
+import curfp_b200 as curfp  # noqa: E402
+from curfp_b200 import autograd as ag  # noqa: E402
+from curfp_b200 import precision  # noqa: E402
+
+VARIANTS = [(tr, ul) for tr in (0, 1) for ul in (0, 1)]  # transr 0=N 1=T, uplo 0=L 1=U
+NAME = lambda tr, ul: "NT"[tr] + "LU"[ul]  # noqa: E731
+
+
+def vp(t) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def chol_flops(n: int) -> float:
+    return n ** 3 / 3.0 + n ** 2 / 2.0 + n / 6.0
+
+
+def emit(d: dict, out) -> None:
+    line = json.dumps(d)
+    print(line, flush=True)
+    if out:
+        with open(out, "a") as f:
+            f.write(line + "\n")
+
+
+class Ours:
+    """This library through its C ABI (the drop-in boundary)."""
+
+    def __init__(self):
+        self.h = curfp._get_handle()
+        self.lib = self.h._lib
+
+    def ssfrk(self, tr, ul, n, k, A, C, math=0):
+        a, b = ctypes.c_float(1.0), ctypes.c_float(0.0)
+        st = self.lib.curfpSsfrkEx(self.h.ptr, tr, ul, 1, n, k, ctypes.byref(a), vp(A), k,
+                                   ctypes.byref(b), vp(C), math)
+        assert st == 0, st
+
+    def add_diag(self, tr, ul, n, v, C):
+        assert self.lib.curfpSaddToDiagonal(self.h.ptr, tr, ul, n, ctypes.c_float(v), vp(C)) == 0
+
+    def spftrf(self, tr, ul, n, C, math=0):
+        info = ctypes.c_int(0)
+        st = self.lib.curfpSpftrfEx(self.h.ptr, tr, ul, n, vp(C), ctypes.byref(info), math)
+        assert st == 0 and info.value == 0, (st, info.value)
+
+    def spftrs(self, tr, ul, n, nrhs, F, X):
+        assert self.lib.curfpSpftrs(self.h.ptr, tr, ul, n, nrhs, vp(F), vp(X), n) == 0
+
+    def refine(self, tr, ul, n, nrhs, C, F, X, max_iter):
+        it = ctypes.c_int(0)
+        st = self.lib.curfpSpftrsRefine(self.h.ptr, tr, ul, n, nrhs, vp(C), vp(F), vp(X), n,
+                                        max_iter, ctypes.byref(it))
+        assert st == 0, st
+        return it.value
+
+    def spftri(self, tr, ul, n, F):
+        assert self.lib.curfpSpftri(self.h.ptr, tr, ul, n, vp(F)) == 0
+
+    def stfttr(self, tr, ul, n, arf, D):
+        assert self.lib.curfpSstfttr(self.h.ptr, tr, ul, n, vp(arf), vp(D), n) == 0
+
+    def release(self):
+        assert self.lib.curfpReleaseWorkspace(self.h.ptr) == 0
+
+
+def cuda_ms(fn, prep=None, warmup=2, reps=5):
+    """Median device milliseconds of fn() over reps runs after warmup runs."""
+    ts = []
+    for i in range(warmup + reps):
+        if prep is not None:
+            prep()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        if i >= warmup:
+            ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts)
+
+
+def rate(ms, flops=None, nbytes=None):
+    d = {"ms": round(ms, 3)}
+    if flops is not None:
+        d["tflops"] = round(flops / (ms * 1e-3) / 1e12, 3)
+    if nbytes is not None:
+        d["gbs"] = round(nbytes / (ms * 1e-3) / 1e9, 1)
+    return d
+
+
+def gen_A(n, k, seed):
+    rng = np.random.default_rng(seed)
+    A = (rng.standard_normal((n, k), dtype=np.float32) / np.float32(math.sqrt(k)))
+    return torch.from_numpy(A).cuda()
+
+
+def gen_B(n, nrhs, seed):
+    """(nrhs, n) row-major = the column-major n x nrhs block of the C ABI."""
+    rng = np.random.default_rng(seed)
+    return torch.from_numpy(rng.standard_normal((nrhs, n), dtype=np.float32)).cuda()
+
+
+# ---------------------------------------------------------------------------
+# FP64 checks
+# ---------------------------------------------------------------------------
+
+class GramOracle:
+    """Exact FP64 facts of C = A A^T + lam I (A n x k, n > k) from A's Gram
+    matrix (Woodbury identity)."""
+
+    def __init__(self, A32, lam):
+        n, k = A32.shape
+        assert n > k
+        self.n, self.k, self.lam = n, k, float(lam)
+        self.A = A32.double()
+        G = self.A.T @ self.A
+        self.s = torch.linalg.eigvalsh(G)
+        G.diagonal().add_(self.lam)
+        self.Lg = torch.linalg.cholesky(G)
+        del G
+        self.norm2 = float(self.s.max()) + self.lam
+        self.cond2 = self.norm2 / self.lam
+
+    def apply(self, X):  # C X
+        return self.A @ (self.A.T @ X) + self.lam * X
+
+    def solve(self, B):  # C^-1 B
+        u = torch.cholesky_solve(self.A.T @ B, self.Lg)
+        return (B - self.A @ u) / self.lam
+
+    def logdet(self) -> float:
+        return (self.n - self.k) * math.log(self.lam) + float(torch.log(self.s + self.lam).sum())
+
+    def trace_inv(self) -> float:
+        return (self.n - self.k) / self.lam + float((1.0 / (self.s + self.lam)).sum())
+
+    def trace_ata_cinv(self) -> float:  # tr(A^T C^-1 A)
+        return float((self.s / (self.s + self.lam)).sum())
+
+    def cinv_a(self):  # C^-1 A = A G^-1
+        return torch.cholesky_solve(self.A.T.contiguous(), self.Lg).T
+
+
+def solve_errors(orc: GramOracle, B32, X32) -> dict:
+    """Normwise backward error max_j ||b_j - C x_j|| / (||C||_2 ||x_j|| + ||b_j||)
+    and forward error max_j ||x_j - x*_j|| / ||x*_j|| against the exact C."""
+    B = B32.double().T
+    X = X32.double().T
+    R = B - orc.apply(X)
+    berr = (R.norm(dim=0) / (orc.norm2 * X.norm(dim=0) + B.norm(dim=0))).max()
+    X64 = orc.solve(B)
+    ferr = ((X - X64).norm(dim=0) / X64.norm(dim=0)).max()
+    return {"backward": float(berr), "forward": float(ferr)}
+
+
+def dense_sym(ours: Ours, tr, ul, n, arf):
+    """FP64 n x n symmetric matrix of an RFP array (exact widening)."""
+    D = torch.zeros(n, n, device="cuda")
+    ours.stfttr(tr, ul, n, arf, D)
+    S = D.double()
+    del D
+    S += S.T.clone()
+    S.diagonal().mul_(0.5)
+    return S
+
+
+def dense_tri(ours: Ours, tr, ul, n, arf):
+    """FP64 stored triangle of an RFP factor: L (uplo=L, row-major lower) or
+    U (uplo=U, row-major upper)."""
+    D = torch.zeros(n, n, device="cuda")
+    ours.stfttr(tr, ul, n, arf, D)
+    T = D.double()
+    del D
+    return T
+
+
+def factor_berr(S, T, ul) -> float:
+    P = (T.T @ T) if ul == 1 else (T @ T.T)
+    P -= S
+    r = float(torch.linalg.norm(P) / torch.linalg.norm(S))
+    del P
+    return r
+
+
+def solve_berr_dense(S, norm2, B32, X32) -> float:
+    B = B32.double().T
+    X = X32.double().T
+    R = B - S @ X
+    return float((R.norm(dim=0) / (norm2 * X.norm(dim=0) + B.norm(dim=0))).max())
+
+
+def inverse_res(S, I_sym) -> float:
+    """||C Z - I||_F / sqrt(n): RMS over columns of ||C z_j - e_j||."""
+    P = S @ I_sym
+    P.diagonal().sub_(1.0)
+    r = float(torch.linalg.norm(P) / math.sqrt(S.shape[0]))
+    del P
+    return r
+
+
+def rel_diff(a, b) -> float:
+    return float(torch.linalg.norm((a - b).double()) / torch.linalg.norm(b.double()))
+
+
+# ---------------------------------------------------------------------------
+# C2: plain FP32 at scale, all variants, beside the reference build
+# ---------------------------------------------------------------------------
+
+def run_c2(args):
+    from helpers import REF_LIB, RefLib
+    ours = Ours()
+    ref = RefLib() if REF_LIB.exists() else None
+    k, nrhs, shift = 1024, 64, 1.0
+    variants = VARIANTS if args.variants == "all" else [
+        (int(args.variants[0] == "T"), int(args.variants[1] == "U"))]
+    for n in args.n:
+        A = gen_A(n, k, seed=n)
+        B0 = gen_B(n, nrhs, seed=n + 1)
+        orc = GramOracle(A, shift)  # only for ||C||_2 of the exact matrix
+        nt = n * (n + 1) // 2
+        f = {"ssfrk": n * (n + 1) * float(k), "spftrf": chol_flops(n),
+             "spftrs": 2.0 * n * n * nrhs, "spftri": 2.0 * n ** 3 / 3.0}
+        by = {"ssfrk": 4.0 * n * k + 4.0 * nt, "spftrf": 8.0 * nt,
+              "spftrs": 8.0 * nt + 16.0 * n * nrhs, "spftri": 8.0 * nt}
+        for tr, ul in variants:
+            res = {"config": "C2", "n": n, "k": k, "nrhs": nrhs, "shift": shift,
+                   "variant": NAME(tr, ul), "transr": "NT"[tr], "uplo": "LU"[ul],
+                   "timing": f"warmup {args.warmup}, median of {args.reps}",
+                   "ours": {}, "reference": {}, "errors": {}}
+            C0 = torch.empty(nt, device="cuda")
+            ms = cuda_ms(lambda: ours.ssfrk(tr, ul, n, k, A, C0), None, args.warmup, args.reps)
+            res["ours"]["ssfrk"] = rate(ms, f["ssfrk"], by["ssfrk"])
+            ours.add_diag(tr, ul, n, shift, C0)
+            F = torch.empty_like(C0)
+            X = torch.empty_like(B0)
+            Z = torch.empty_like(C0)
+            ms = cuda_ms(lambda: ours.spftrf(tr, ul, n, F), lambda: F.copy_(C0),
+                         args.warmup, args.reps)
+            res["ours"]["spftrf"] = rate(ms, f["spftrf"], by["spftrf"])
+            ms = cuda_ms(lambda: ours.spftrs(tr, ul, n, nrhs, F, X), lambda: X.copy_(B0),
+                         args.warmup, args.reps)
+            res["ours"]["spftrs"] = rate(ms, f["spftrs"], by["spftrs"])
+            ms = cuda_ms(lambda: ours.spftri(tr, ul, n, Z), lambda: Z.copy_(F),
+                         args.warmup, args.reps)
+            res["ours"]["spftri"] = rate(ms, f["spftri"], by["spftri"])
+            t = res["ours"]
+            t["chol_solve_tflops"] = round((f["spftrf"] + f["spftrs"]) /
+                                           ((t["spftrf"]["ms"] + t["spftrs"]["ms"]) * 1e-3) / 1e12, 3)
+            if ref is not None:
+                Cr = torch.empty(nt, device="cuda")
+                ms = cuda_ms(lambda: ref.ssfrk(tr, ul, 1, n, k, 1.0, A, k, 0.0, Cr), None,
+                             args.warmup, args.reps)
+                res["reference"]["ssfrk"] = rate(ms, f["ssfrk"], by["ssfrk"])
+                ours.add_diag(tr, ul, n, shift, Cr)
+                res["errors"]["ssfrk_maxabs_ours_vs_ref"] = float((Cr - C0).abs().max())
+                del Cr
+                Fr = torch.empty_like(C0)
+                Xr = torch.empty_like(B0)
+                Zr = torch.empty_like(C0)
+
+                def rf():
+                    st, info = ref.spftrf(tr, ul, n, Fr)
+                    assert st == 0 and info == 0, (st, info)
+                ms = cuda_ms(rf, lambda: Fr.copy_(C0), args.warmup, args.reps)
+                res["reference"]["spftrf"] = rate(ms, f["spftrf"], by["spftrf"])
+                ms = cuda_ms(lambda: ref.spftrs(tr, ul, n, nrhs, Fr, Xr, n), lambda: Xr.copy_(B0),
+                             args.warmup, args.reps)
+                res["reference"]["spftrs"] = rate(ms, f["spftrs"], by["spftrs"])
+                ms = cuda_ms(lambda: ref.spftri(tr, ul, n, Zr), lambda: Zr.copy_(Fr),
+                             args.warmup, args.reps)
+                res["reference"]["spftri"] = rate(ms, f["spftri"], by["spftri"])
+                t = res["reference"]
+                t["chol_solve_tflops"] = round(
+                    (f["spftrf"] + f["spftrs"]) /
+                    ((t["spftrf"]["ms"] + t["spftrs"]["ms"]) * 1e-3) / 1e12, 3)
+                e = res["errors"]
+                e["factor_rel_diff_ours_vs_ref"] = rel_diff(F, Fr)
+                e["solve_rel_diff_ours_vs_ref"] = rel_diff(X, Xr)
+                e["inverse_rel_diff_ours_vs_ref"] = rel_diff(Z, Zr)
+            # FP64 checks on the stored FP32 matrix C0 (the input of both arms)
+            S = dense_sym(ours, tr, ul, n, C0)
+            e = res["errors"]
+            arms = [("ours", F, X, Z)] + ([("reference", Fr, Xr, Zr)] if ref is not None else [])
+            for name, Fa, Xa, Za in arms:
+                T = dense_tri(ours, tr, ul, n, Fa)
+                e[f"{name}_factor_backward"] = factor_berr(S, T, ul)
+                del T
+                e[f"{name}_solve_backward"] = solve_berr_dense(S, orc.norm2, B0, Xa)
+                Zs = dense_sym(ours, tr, ul, n, Za)
+                e[f"{name}_inverse_residual"] = inverse_res(S, Zs)
+                del Zs
+            del S, F, X, Z, C0
+            if ref is not None:
+                del Fr, Xr, Zr
+            torch.cuda.empty_cache()
+            emit(res, args.out)
+        del A, B0, orc
+        torch.cuda.empty_cache()
+
+
+# ---------------------------------------------------------------------------
+# Host LAPACK at the C2 sizes
+# ---------------------------------------------------------------------------
+
+def run_lapack(args):
+    from scipy.linalg import lapack as la
+
+    from oracle import port
+    k, nrhs, shift = 1024, 64, 1.0
+    for n in args.n:
+        rng = np.random.default_rng(n)
+        A = np.asfortranarray(rng.standard_normal((n, k), dtype=np.float32) /
+                              np.float32(math.sqrt(k)))
+        B = np.asfortranarray(np.random.default_rng(n + 1).standard_normal(
+            (n, nrhs), dtype=np.float32))
+        out = {"config": "C2-host-LAPACK", "n": n, "k": k, "nrhs": nrhs, "variant": "TU",
+               "cores": port.threads(),
+               "library": f"scipy {__import__('scipy').__version__} LAPACK (OpenBLAS)",
+               "timing": "one run each", "ops": {}}
+        t0 = time.perf_counter()
+        C = la.ssfrk(n, k, 1.0, A, 0.0, np.zeros(n * (n + 1) // 2, np.float32),
+                     transr="T", uplo="U", trans="N")
+        t1 = time.perf_counter()
+        C[port.diag_indices(n, "T", "U")] += np.float32(shift)
+        t2 = time.perf_counter()
+        F, info = la.spftrf(n, C, transr="T", uplo="U")
+        t3 = time.perf_counter()
+        assert info == 0, info
+        X, info = la.spftrs(n, F, B, transr="T", uplo="U")
+        t4 = time.perf_counter()
+        Z, info = la.spftri(n, F, transr="T", uplo="U")
+        t5 = time.perf_counter()
+        o = out["ops"]
+        o["ssfrk"] = rate((t1 - t0) * 1e3, n * (n + 1) * float(k))
+        o["spftrf"] = rate((t3 - t2) * 1e3, chol_flops(n))
+        o["spftrs"] = rate((t4 - t3) * 1e3, 2.0 * n * n * nrhs)
+        o["spftri"] = rate((t5 - t4) * 1e3, 2.0 * n ** 3 / 3.0)
+        out["chol_solve_tflops"] = round((chol_flops(n) + 2.0 * n * n * nrhs) /
+                                         (t4 - t2) / 1e12, 4)
+        emit(out, args.out)
+        del A, B, C, F, X, Z
+
+
+# ---------------------------------------------------------------------------
+# C3: precision form vs plain at n = 65536
+# ---------------------------------------------------------------------------
+
+def breakdown(fn) -> dict:
+    precision.profile_enable(True)
+    fn()
+    torch.cuda.synchronize()
+    r = precision.profile_read()
+    precision.profile_enable(False)
+    return {k: round(v["ms"], 2) for k, v in r.items()}
+
+
+def run_c3(args):
+    ours = Ours()
+    n, k, nrhs = args.c3_n, args.c3_k, 256
+    tr, ul = 1, 1
+    nt = n * (n + 1) // 2
+    A = gen_A(n, k, seed=65536)
+    B0 = gen_B(n, nrhs, seed=65537)
+    fl = chol_flops(n) + 2.0 * n * n * nrhs
+    for lam in args.lam:
+        orc = GramOracle(A, lam)
+        res = {"config": "C3", "n": n, "k": k, "nrhs": nrhs, "lambda": lam, "variant": "TU",
+               "cond2_exact": orc.cond2, "norm2_exact": orc.norm2,
+               "timing": f"warmup {args.warmup}, median of {args.reps}",
+               "metric": "Cholesky+solve TFLOP/s = (n^3/3 + n^2/2 + n/6 + 2 n^2 nrhs) / t"}
+        for form, math_ in (("plain_fp32", 0), ("split_bf16", 1)):
+            C = torch.empty(nt, device="cuda")
+            ms_s = cuda_ms(lambda: ours.ssfrk(tr, ul, n, k, A, C, math_), None,
+                           args.warmup, args.reps)
+            ours.add_diag(tr, ul, n, lam, C)
+            F = torch.empty_like(C)
+            X = torch.empty_like(B0)
+            ms_f = cuda_ms(lambda: ours.spftrf(tr, ul, n, F, math_), lambda: F.copy_(C),
+                           args.warmup, args.reps)
+            iters = []
+            if math_ == 0:
+                ms_x = cuda_ms(lambda: ours.spftrs(tr, ul, n, nrhs, F, X), lambda: X.copy_(B0),
+                               args.warmup, args.reps)
+            else:
+                ms_x = cuda_ms(lambda: iters.append(
+                    ours.refine(tr, ul, n, nrhs, C, F, X, args.max_iter)),
+                    lambda: X.copy_(B0), args.warmup, args.reps)
+            d = {"ssfrk": rate(ms_s, n * (n + 1) * float(k)),
+                 "spftrf": rate(ms_f, chol_flops(n)),
+                 "spftrs" if math_ == 0 else "spftrs_refined": rate(ms_x, 2.0 * n * n * nrhs),
+                 "chol_solve": rate(ms_f + ms_x, fl)}
+            if iters:
+                d["refine_corrections"] = iters[-1]
+            d["errors_vs_fp64"] = solve_errors(orc, B0, X)
+            # the stored matrix against the exact one on 512 sampled rows
+            d["ssfrk_rel_err_sampled"] = ssfrk_sample_err(ours, tr, ul, n, C, orc, 512)
+            d["breakdown_ms"] = breakdown(lambda: (F.copy_(C), ours.spftrf(tr, ul, n, F, math_)))
+            res[form] = d
+            del C, F, X
+            torch.cuda.empty_cache()
+            ours.release()
+        res["precision_over_plain"] = round(res["split_bf16"]["chol_solve"]["tflops"] /
+                                            res["plain_fp32"]["chol_solve"]["tflops"], 3)
+        emit(res, args.out)
+        del orc
+        torch.cuda.empty_cache()
+
+
+def ssfrk_sample_err(ours: Ours, tr, ul, n, C, orc: GramOracle, nrows: int) -> float:
+    """max |C_stored - C_exact| / max |C_exact| over nrows sampled rows."""
+    rows = torch.from_numpy(np.sort(np.random.default_rng(5).choice(n, nrows, replace=False)))
+    rows = rows.cuda()
+    Ce = orc.A[rows] @ orc.A.T  # nrows x n
+    Ce[torch.arange(nrows, device="cuda"), rows] += orc.lam
+    got = torch.empty_like(Ce)
+    # row r of the symmetric matrix from the RFP array: element (r, j) lives
+    # at the RFP offset of logical lower element (max, min)
+    offs = rfp_offsets(tr, ul, n, rows)
+    got.copy_(C[offs].double())
+    err = float((got - Ce).abs().max() / Ce.abs().max())
+    return err
+
+
+def rfp_offsets(tr, ul, n, rows):
+    """RFP offsets (int64, nrows x n) of the symmetric matrix's rows `rows`:
+    the lower element (max(r, j), min(r, j)) of the logical factor, through the
+    block geometry of the variant (rfp_diag_indices gives the diagonal, the
+    blocks' strides follow from it)."""
+    lower = ul == 0
+    if n % 2:
+        n1, n2 = ((n + 1) // 2, n // 2) if lower else (n // 2, (n + 1) // 2)
+    else:
+        n1 = n2 = n // 2
+    kk = n // 2
+    N = n
+    if n % 2:
+        if tr == 0:
+            g = ((0, 1, N), (n1, 1, N), (N, N, 1)) if lower else ((n2, 1, N), (0, N, 1), (n1, N, 1))
+        else:
+            g = (((0, n1, 1), (n1 * n1, n1, 1), (1, 1, n1)) if lower else
+                 ((n2 * n2, n2, 1), (0, 1, n2), (n1 * n2, 1, n2)))
+    else:
+        if tr == 0:
+            g = (((1, 1, N + 1), (kk + 1, 1, N + 1), (0, N + 1, 1)) if lower else
+                 ((kk + 1, 1, N + 1), (0, N + 1, 1), (kk, N + 1, 1)))
+        else:
+            g = (((kk, kk, 1), (kk * (kk + 1), kk, 1), (0, 1, kk)) if lower else
+                 ((kk * (kk + 1), kk, 1), (0, 1, kk), (kk * kk, 1, kk)))
+    r = rows.view(-1, 1).long()
+    j = torch.arange(n, device=rows.device).view(1, -1)
+    p = torch.maximum(r, j)
+    q = torch.minimum(r, j)
+    o11 = g[0][0] + p * g[0][1] + q * g[0][2]
+    o21 = g[1][0] + (p - n1) * g[1][1] + q * g[1][2]
+    o22 = g[2][0] + (p - n1) * g[2][1] + (q - n1) * g[2][2]
+    return torch.where(q < n1, torch.where(p < n1, o11, o21), o22)
+
+
+# ---------------------------------------------------------------------------
+# C5: n = 131072 precision pipeline + fused NLL fwd/bwd
+# ---------------------------------------------------------------------------
+
+def run_c5(args):
+    ours = Ours()
+    n, k, nrhs, lam = args.c5_n, args.c5_k, 64, 1e-2
+    tr, ul = 1, 1
+    nt = n * (n + 1) // 2
+    A = gen_A(n, k, seed=131072)
+    B0 = gen_B(n, nrhs, seed=131073)
+    orc = GramOracle(A, lam)
+    res = {"config": "C5", "n": n, "k": k, "nrhs": nrhs, "lambda": lam, "variant": "TU",
+           "cond2_exact": orc.cond2, "rfp_gb_per_copy": round(4.0 * nt / 1e9, 2),
+           "timing": f"warmup {args.warmup}, median of {args.reps}"}
+    C = torch.empty(nt, device="cuda")
+    ms_s = cuda_ms(lambda: ours.ssfrk(tr, ul, n, k, A, C, 1), None, args.warmup, args.reps)
+    ours.add_diag(tr, ul, n, lam, C)
+    F = torch.empty_like(C)
+    X = torch.empty_like(B0)
+    ms_f = cuda_ms(lambda: ours.spftrf(tr, ul, n, F, 1), lambda: F.copy_(C), args.warmup,
+                   args.reps)
+    iters = []
+    ms_x = cuda_ms(lambda: iters.append(ours.refine(tr, ul, n, nrhs, C, F, X, args.max_iter)),
+                   lambda: X.copy_(B0), args.warmup, args.reps)
+    fl = chol_flops(n) + 2.0 * n * n * nrhs
+    res["split_bf16"] = {
+        "ssfrk": rate(ms_s, n * (n + 1) * float(k)),
+        "spftrf": rate(ms_f, chol_flops(n)),
+        "spftrs_refined": rate(ms_x, 2.0 * n * n * nrhs),
+        "chol_solve": rate(ms_f + ms_x, fl),
+        "pipeline_ms": round(ms_s + ms_f + ms_x, 1),
+        "refine_corrections": iters[-1],
+        "errors_vs_fp64": solve_errors(orc, B0, X),
+        "ssfrk_rel_err_sampled": ssfrk_sample_err(ours, tr, ul, n, C, orc, 256),
+        "breakdown_ms": breakdown(lambda: (F.copy_(C), ours.spftrf(tr, ul, n, F, 1))),
+        "peak_mem_gb": round(torch.cuda.max_memory_allocated() / 1e9, 1)}
+    del C, F, X
+    torch.cuda.empty_cache()
+    ours.release()
+    if not args.no_nll:
+        res["nll"] = nll_c5(orc, A, lam, args)
+    emit(res, args.out)
+
+
+def nll_c5(orc: GramOracle, A, lam, args) -> dict:
+    """Fused GP NLL (X = A, s = 1, sigma2 = lam) forward + backward, against
+    the exact FP64 loss and gradient."""
+    n, k = A.shape
+    y = torch.from_numpy(np.random.default_rng(7).standard_normal(n, dtype=np.float32)).cuda()
+    out = {"workload": f"loss = 1/2 y^T C^-1 y + sum log diag L, C = s X X^T + sigma2 I, "
+                       f"X = A ({n} x {k}), s = 1, sigma2 = {lam}; fused form, split-BF16"}
+    holder = {}
+
+    def step():
+        Xt = A.clone().requires_grad_(True)
+        st = torch.tensor(1.0, device="cuda", requires_grad=True)
+        vt = torch.tensor(lam, device="cuda", requires_grad=True)
+        loss = ag.nll(Xt, st, vt, y, math="bf16x3", fused=True)
+        loss.backward()
+        holder.update(loss=loss.detach(), gx=Xt.grad, gs=st.grad, gv=vt.grad)
+
+    out["fwd_bwd_ms"] = round(cuda_ms(step, lambda: holder.clear(), args.nll_warmup,
+                                      args.nll_reps), 1)
+    loss64, gx64, gs64, gv64 = nll_exact(orc, y)
+    out["errors_vs_fp64"] = {
+        "loss": abs(float(holder["loss"]) - loss64) / abs(loss64),
+        "grad_X": float(torch.linalg.norm(holder["gx"].double() - gx64) /
+                        torch.linalg.norm(gx64)),
+        "grad_s": abs(float(holder["gs"]) - gs64) / abs(gs64),
+        "grad_sigma2": abs(float(holder["gv"]) - gv64) / abs(gv64)}
+    out["peak_mem_gb"] = round(torch.cuda.max_memory_allocated() / 1e9, 1)
+    return out
+
+
+def nll_exact(orc: GramOracle, y):
+    """Exact FP64 loss and gradients (X, s, sigma2) of the GP NLL at X = A,
+    s = 1, sigma2 = lam:  alpha = C^-1 y, loss = 1/2 y^T alpha + 1/2 log det C,
+    dX = C^-1 A - alpha (A^T alpha)^T, ds = 1/2 (tr(A^T C^-1 A) - |A^T alpha|^2),
+    dsigma2 = 1/2 (tr C^-1 - |alpha|^2)."""
+    y64 = y.double()
+    alpha = orc.solve(y64[:, None])[:, 0]
+    loss64 = 0.5 * float(y64 @ alpha) + 0.5 * orc.logdet()
+    ata = orc.A.T @ alpha
+    gx64 = orc.cinv_a() - alpha[:, None] * ata[None, :]
+    gs64 = 0.5 * (orc.trace_ata_cinv() - float(ata @ ata))
+    gv64 = 0.5 * (orc.trace_inv() - float(alpha @ alpha))
+    return loss64, gx64, gs64, gv64
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("what", choices=["c2", "lapack", "c3", "c5"])
+    ap.add_argument("--n", type=int, nargs="+", default=[32768, 32767])
+    ap.add_argument("--variants", default="all")
+    ap.add_argument("--lam", type=float, nargs="+", default=[0.1, 0.001])
+    ap.add_argument("--c3-n", type=int, default=65536)
+    ap.add_argument("--c3-k", type=int, default=2048)
+    ap.add_argument("--c5-n", type=int, default=131072)
+    ap.add_argument("--c5-k", type=int, default=4096)
+    ap.add_argument("--warmup", type=int, default=2)
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--nll-warmup", type=int, default=1)
+    ap.add_argument("--nll-reps", type=int, default=3)
+    ap.add_argument("--max-iter", type=int, default=3)
+    ap.add_argument("--no-nll", action="store_true")
+    ap.add_argument("--out", default=None, help="also append the JSON lines to this file")
+    args = ap.parse_args()
+    if args.what != "lapack":
+        torch.cuda.init()
+    {"c2": run_c2, "lapack": run_lapack, "c3": run_c3, "c5": run_c5}[args.what](args)
+
+
+if __name__ == "__main__":
+    main()

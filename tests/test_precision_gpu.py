@@ -45,6 +45,29 @@ def test_ssfrk_bf16x3_vs_fp64(curfp, n, k, tr, ul):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("tr,ul", [(1, 1), (0, 0)])
+def test_ssfrk_bf16x3_k_split(curfp, tr, ul):
+    """A contraction whose staged planes exceed the 4 GiB staging budget
+    (n = 16384, k = 36864: 4.9 GiB) runs as two k-slabs; C accumulates across
+    them with beta applied once.  Checked on 256 sampled rows in FP64."""
+    from curfp_b200 import precision as P
+    from scale_configs import rfp_offsets
+    n, k = 16384, 36864
+    g = torch.Generator(device="cuda").manual_seed(k)
+    A = torch.randn(n, k, device="cuda", generator=g) / k ** 0.5
+    C0 = torch.randn(n * (n + 1) // 2, device="cuda", generator=g)
+    C = C0.clone()
+    P.ssfrk(A, C, alpha=0.75, beta=-0.5, transr=TR[tr], uplo=UL[ul])
+    rows = torch.randperm(n, device="cuda", generator=g)[:256].sort().values
+    offs = rfp_offsets(tr, ul, n, rows)
+    Ad = A.double()
+    want = 0.75 * (Ad[rows] @ Ad.T) - 0.5 * C0[offs].double()
+    err = (C[offs].double() - want).abs().max().item()
+    scale = (0.75 * (Ad[rows] @ Ad.T).abs() + 0.5 * C0[offs].double().abs()).max().item()
+    assert err / scale <= 2e-6, err / scale
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("n", [1000, 2049, 4096])
 @pytest.mark.parametrize("tr,ul", VARIANTS)
 def test_spftrf_bf16x3_backward_error(curfp, n, tr, ul):
