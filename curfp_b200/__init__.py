@@ -26,11 +26,15 @@ __all__ = [
     "rfp_diag_indices", "add_to_diagonal", "ssfrk", "ssfrk_raw", "spftrf",
     "spftrf_raw", "spftrs", "spftrs_raw", "spftri", "spftri_raw", "strttf",
     "strttf_raw", "stfttr", "stfttr_raw", "ssfr2k", "ssfr2k_raw", "CurfpError",
+    "NORM_MAX", "NORM_ONE", "NORM_FRO", "slansf", "slansf_raw", "spfcon", "spfcon_raw",
+    "spftrf_rcond", "SIDE_LEFT", "SIDE_RIGHT", "ssfmm", "ssfmm_raw", "ssfmv", "ssfmv_raw",
 ]
 
 # Enum values of include/curfp.h (reference curfp/_ext.cpp:869-877).
 OP_N, OP_T = 0, 1
 FILL_LOWER, FILL_UPPER = 0, 1
+NORM_MAX, NORM_ONE, NORM_FRO = 0, 1, 2
+SIDE_LEFT, SIDE_RIGHT = 0, 1
 
 
 class Handle:
@@ -110,6 +114,28 @@ def _fill(s: str) -> int:
         return _FILL_MAP[s.upper()]
     except KeyError:
         raise ValueError(f"uplo must be 'L' or 'U', got {s!r}")
+
+
+# norm strings of reference curfp/__init__.py:114-123
+_NORM_MAP = {"M": NORM_MAX, "MAX": NORM_MAX, "1": NORM_ONE, "O": NORM_ONE, "I": NORM_ONE,
+             "F": NORM_FRO, "E": NORM_FRO, "FRO": NORM_FRO}
+
+
+def _norm(s: str) -> int:
+    try:
+        return _NORM_MAP[s.upper()]
+    except KeyError:
+        raise ValueError(f"norm must be 'M'/'1'/'F' (or 'O'/'I'/'E'), got {s!r}")
+
+
+_SIDE_MAP = {"L": SIDE_LEFT, "R": SIDE_RIGHT}
+
+
+def _side(s: str) -> int:
+    try:
+        return _SIDE_MAP[s.upper()]
+    except KeyError:
+        raise ValueError(f"side must be 'L' or 'R', got {s!r}")
 
 
 def _n_from_rfp(numel: int) -> int:
@@ -347,3 +373,142 @@ def ssfr2k(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor, *,
         ldb = B.shape[1] if tu == "T" else B.shape[0]
     ssfr2k_raw(_get_handle(), _op(transr), _fill(uplo), _op(trans), n, k,
                alpha, A, lda, B, ldb, beta, C)
+
+
+# ---------------------------------------------------------------------------
+# Norms and condition estimate (reference curfp/__init__.py:784-960)
+# ---------------------------------------------------------------------------
+
+def slansf_raw(handle, norm: int, transr: int, uplo: int, n: int, C: torch.Tensor) -> float:
+    """Norm (NORM_MAX / NORM_ONE / NORM_FRO) of the symmetric RFP matrix C."""
+    _validate(C, "C")
+    out = ctypes.c_float(0.0)
+    check(_lib.load().curfpSlansf(_hp(handle), norm, transr, uplo, n, _ptr(C),
+                                  ctypes.byref(out)))
+    return float(out.value)
+
+
+def slansf(C: torch.Tensor, norm: str = "1", *, transr: str = "T", uplo: str = "U",
+           n: int = None) -> float:
+    """'M' max |A(i,j)|, '1' / 'O' / 'I' max column sum of |A|, 'F' / 'E'
+    Frobenius norm, of the symmetric matrix held in C (RFP, not a factor)."""
+    _validate(C, "C")
+    if n is None:
+        n = _n_from_rfp(C.numel())
+    return slansf_raw(_get_handle(), _norm(norm), _op(transr), _fill(uplo), n, C)
+
+
+def spfcon_raw(handle, transr: int, uplo: int, n: int, C: torch.Tensor, anorm: float) -> float:
+    """rcond = 1 / (||A^-1||_1 anorm) from the RFP Cholesky factor C."""
+    _validate(C, "C")
+    out = ctypes.c_float(0.0)
+    check(_lib.load().curfpSpfcon(_hp(handle), transr, uplo, n, _ptr(C), float(anorm),
+                                  ctypes.byref(out)))
+    return float(out.value)
+
+
+def spfcon(C: torch.Tensor, anorm: float, *, transr: str = "T", uplo: str = "U",
+           n: int = None) -> float:
+    """Reciprocal condition number estimate (Hager-Higham 1-norm estimator)
+    from the factor C left by spftrf; anorm = slansf(A, '1') of the matrix
+    before factorization.  0.0 if anorm == 0."""
+    _validate(C, "C")
+    if n is None:
+        n = _n_from_rfp(C.numel())
+    return spfcon_raw(_get_handle(), _op(transr), _fill(uplo), n, C, anorm)
+
+
+def spftrf_rcond(C: torch.Tensor, *, transr: str = "T", uplo: str = "U", n: int = None,
+                 check: bool = True) -> float:
+    """slansf('1') + in-place spftrf + spfcon: factor C and return its
+    estimated reciprocal condition number (0.0 if not positive definite and
+    check=False)."""
+    _validate(C, "C")
+    if n is None:
+        n = _n_from_rfp(C.numel())
+    h = _get_handle()
+    anorm = slansf_raw(h, NORM_ONE, _op(transr), _fill(uplo), n, C)
+    info = spftrf_raw(h, _op(transr), _fill(uplo), n, C)
+    if check and info != 0:
+        raise torch.linalg.LinAlgError(
+            f"spftrf_rcond: matrix is not positive definite "
+            f"(leading minor of order {info} is not positive definite)")
+    if info != 0 or anorm == 0.0:
+        return 0.0
+    return spfcon_raw(h, _op(transr), _fill(uplo), n, C, anorm)
+
+
+# ---------------------------------------------------------------------------
+# Symmetric (RFP) times dense (reference curfp/__init__.py:568-650, 1203-1340)
+# ---------------------------------------------------------------------------
+
+def ssfmv_raw(handle, transr: int, uplo: int, n: int, alpha: float, arf: torch.Tensor,
+              x: torch.Tensor, incx: int, beta: float, y: torch.Tensor, incy: int) -> None:
+    """y := alpha*A*x + beta*y in place (BLAS increments)."""
+    _validate(arf, "arf")
+    _validate(x, "x")
+    _validate(y, "y")
+    a, b = ctypes.c_float(alpha), ctypes.c_float(beta)
+    check(_lib.load().curfpSsfmv(_hp(handle), transr, uplo, n, ctypes.byref(a), _ptr(arf),
+                                 _ptr(x), incx, ctypes.byref(b), _ptr(y), incy))
+
+
+def ssfmv(arf: torch.Tensor, x: torch.Tensor, y: torch.Tensor = None, *, alpha: float = 1.0,
+          beta: float = 0.0, transr: str = "T", uplo: str = "U", n: int = None) -> torch.Tensor:
+    """y := alpha*A*x + beta*y with A symmetric in RFP; y created (zeros) if
+    not given; returns y."""
+    _validate(arf, "arf")
+    _validate(x, "x")
+    if n is None:
+        n = _n_from_rfp(arf.numel())
+    if y is None:
+        y = torch.zeros(n, dtype=torch.float32, device=arf.device)
+    _validate(y, "y")
+    if x.numel() != n:
+        raise ValueError(f"x has {x.numel()} elements but n={n}")
+    if y.numel() != n:
+        raise ValueError(f"y has {y.numel()} elements but n={n}")
+    ssfmv_raw(_get_handle(), _op(transr), _fill(uplo), n, alpha, arf, x, 1, beta, y, 1)
+    return y
+
+
+def ssfmm_raw(handle, transr: int, uplo: int, side: int, m: int, n: int, alpha: float,
+              arf: torch.Tensor, B: torch.Tensor, ldb: int, beta: float, C: torch.Tensor,
+              ldc: int) -> None:
+    """C := alpha*A*B + beta*C (side LEFT) or alpha*B*A + beta*C (RIGHT);
+    B, C column-major m x n with leading dimensions ldb, ldc."""
+    _validate(arf, "arf")
+    _validate(B, "B")
+    _validate(C, "C")
+    a, b = ctypes.c_float(alpha), ctypes.c_float(beta)
+    check(_lib.load().curfpSsfmm(_hp(handle), transr, uplo, side, m, n, ctypes.byref(a),
+                                 _ptr(arf), _ptr(B), ldb, ctypes.byref(b), _ptr(C), ldc))
+
+
+def ssfmm(arf: torch.Tensor, B: torch.Tensor, C: torch.Tensor = None, *, alpha: float = 1.0,
+          beta: float = 0.0, transr: str = "T", uplo: str = "U", side: str = "L",
+          n_A: int = None) -> torch.Tensor:
+    """side='L': C := alpha*A*B + beta*C (A m x m); side='R': C := alpha*B*A
+    + beta*C (A n x n), B and C of shape (m, n).  As in the reference, the
+    storage of B and C is handed to the column-major kernel with leading
+    dimension m; returns C (zeros if not given)."""
+    _validate(arf, "arf")
+    _validate(B, "B")
+    if B.ndim != 2:
+        raise ValueError(f"B must be a 2-D tensor, got shape {B.shape}")
+    m, n = B.shape[0], B.shape[1]
+    if n_A is None:
+        n_A = _n_from_rfp(arf.numel())
+    su = side.upper()
+    if su == "L" and n_A != m:
+        raise ValueError(f"side='L': A is {n_A}x{n_A} but B has {m} rows")
+    if su == "R" and n_A != n:
+        raise ValueError(f"side='R': A is {n_A}x{n_A} but B has {n} cols")
+    if C is None:
+        C = torch.zeros(m, n, dtype=torch.float32, device=arf.device)
+    _validate(C, "C")
+    if C.shape != (m, n):
+        raise ValueError(f"C must be {m}x{n}, got {tuple(C.shape)}")
+    ssfmm_raw(_get_handle(), _op(transr), _fill(uplo), _side(side), m, n, alpha, arf, B, m,
+              beta, C, m)
+    return C

@@ -43,6 +43,11 @@ SIGNATURES = {
                         ctypes.POINTER(_f), _p, _i],
     "curfpGetKernelLaunchCount": [_h, ctypes.POINTER(ctypes.c_longlong)],
     "curfpReleaseWorkspace": [_h],
+    "curfpSlansf": [_h, _i, _i, _i, _i, _p, ctypes.POINTER(_f)],
+    "curfpSsfmm": [_h, _i, _i, _i, _i, _i, ctypes.POINTER(_f), _p, _p, _i,
+                   ctypes.POINTER(_f), _p, _i],
+    "curfpSsfmv": [_h, _i, _i, _i, ctypes.POINTER(_f), _p, _p, _i, ctypes.POINTER(_f), _p, _i],
+    "curfpSpfcon": [_h, _i, _i, _i, _p, _f, ctypes.POINTER(_f)],
     "curfpSpftrsNoAlloc": [_h, _i, _i, _i, _i, _p, _p, _i],
     "curfpSsfrkBackward": [_h, _i, _i, _i, _i, _i, ctypes.POINTER(_f), _p, _i, _p, _p, _i],
     "curfpSpftrfBackward": [_h, _i, _i, _i, _p, _p, _p, _i],

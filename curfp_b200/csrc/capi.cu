@@ -87,24 +87,7 @@ curfpStatus_t pack_strided(curfpHandle_t h, int transr, int lower, int n, const 
                            float diag_scale) {
   Geometry g = rfp::geometry(n, transr, lower);
   rfp::kpack::PackArgs a{};
-  const rfp::BlockGeom* bg[3] = {&g.b11, &g.b21, &g.b22};
-  const int rows[3] = {g.n1, g.n2, g.n2}, cols[3] = {g.n1, g.n1, g.n2};
-  const int pb[3] = {0, g.n1, g.n1}, qb[3] = {0, 0, g.n1};
-  int tiles = 0, cnt = 0;
-  for (int b = 0; b < 3; ++b) {
-    if (rows[b] <= 0 || cols[b] <= 0) continue;
-    rfp::kpack::PackBlock& B = a.b[cnt++];
-    B.off = bg[b]->off; B.rs = bg[b]->rs; B.cs = bg[b]->cs;
-    B.rows = rows[b]; B.cols = cols[b];
-    B.p_base = pb[b]; B.q_base = qb[b];
-    B.tri = (b != 1);
-    B.tiles_p = (rows[b] + rfp::kpack::TS - 1) / rfp::kpack::TS;
-    B.tiles_q = (cols[b] + rfp::kpack::TS - 1) / rfp::kpack::TS;
-    B.tile_begin = tiles;
-    tiles += B.tri ? B.tiles_p * (B.tiles_p + 1) / 2 : B.tiles_p * B.tiles_q;
-  }
-  a.nblocks = cnt;
-  a.total_tiles = tiles;
+  const int tiles = rfp::kpack::pack_blocks(g, &a);
   a.drs = drs;
   a.dcs = dcs;
   a.diag_scale = diag_scale;
@@ -450,6 +433,50 @@ curfpStatus_t curfpSsfmmAcc64(curfpHandle_t handle, curfpOperation_t transr,
   if (ldx < n || ldy < n) return CURFP_STATUS_INVALID_VALUE;
   Geometry g = rfp::geometry(n, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER);
   return status_of(symm_launch(handle, g, A, X, ldx, Y, ldy, nrhs, *alpha, *beta));
+}
+
+// src/curfp_ssfmm.cpp:108-306.  side = LEFT: C := alpha A B + beta C (A of
+// order m); side = RIGHT: C := alpha B A + beta C (A of order n), computed as
+// C^T = alpha A B^T + beta C^T on transposed views.  B and C are column-major
+// m x n; the leading dimensions must cover m (the bound the reference's cuBLAS
+// calls enforce).  alpha = 0 reads neither A nor B; beta = 0 does not read C.
+curfpStatus_t curfpSsfmm(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                         curfpSideMode_t side, int m, int n, const float* alpha,
+                         const float* arf, const float* B, int ldb, const float* beta,
+                         float* C, int ldc) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (m < 0 || n < 0 || ldb < 1 || ldc < 1) return CURFP_STATUS_INVALID_VALUE;
+  if (!alpha || !beta) return CURFP_STATUS_INVALID_VALUE;
+  if (m == 0 || n == 0) return CURFP_STATUS_SUCCESS;
+  if (side != CURFP_SIDE_LEFT && side != CURFP_SIDE_RIGHT) return CURFP_STATUS_INVALID_VALUE;
+  if (ldb < m || ldc < m) return CURFP_STATUS_INVALID_VALUE;
+  const bool left = side == CURFP_SIDE_LEFT;
+  rfp::View Bv{const_cast<float*>(B), 1, ldb}, Cv{C, 1, ldc};
+  if (!left) {
+    Bv = rfp::tr(Bv);
+    Cv = rfp::tr(Cv);
+  }
+  CudaExec ex(handle);
+  return status_of(rfp::plan::rfp_symm(ex, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER,
+                                       left ? m : n, arf, Bv, Cv, left ? n : m, *alpha,
+                                       *beta));
+}
+
+// src/curfp_ssfmv.cpp:134-255: y := alpha A x + beta y.  Increments follow
+// BLAS (a negative increment walks the vector backwards); zero is rejected.
+curfpStatus_t curfpSsfmv(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                         int n, const float* alpha, const float* arf, const float* x,
+                         int incx, const float* beta, float* y, int incy) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (n < 0) return CURFP_STATUS_INVALID_VALUE;
+  if (n == 0) return CURFP_STATUS_SUCCESS;
+  if (!alpha || !beta || incx == 0 || incy == 0) return CURFP_STATUS_INVALID_VALUE;
+  const int64_t ox = incx < 0 ? -(int64_t)(n - 1) * incx : 0;
+  const int64_t oy = incy < 0 ? -(int64_t)(n - 1) * incy : 0;
+  rfp::View X{const_cast<float*>(x) + ox, incx, 1}, Y{y + oy, incy, 1};
+  CudaExec ex(handle);
+  return status_of(rfp::plan::rfp_symm(ex, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER,
+                                       n, arf, X, Y, 1, *alpha, *beta));
 }
 
 // ---------------------------------------------------------------------------

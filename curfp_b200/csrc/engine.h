@@ -23,10 +23,11 @@ struct GemmProb {
   float alpha, beta;
   int c_lower;  // write only C(i,j) with i >= j (tiles above the diagonal skipped)
   // Triangular operands: 0 = full, 1 = lower (incl. diagonal), 2 = upper
-  // (incl. diagonal); elements outside are treated as 0 and never read.
-  // For A (m x k): lower keeps kk <= i, upper kk >= i.  For B (k x n): lower
-  // keeps kk >= j, upper kk <= j.  a_tri/b_tri apply to product 1,
-  // a2_tri/b2_tri to product 2.
+  // (incl. diagonal), 3 = strictly upper (A operands only); elements outside
+  // are treated as 0 and never read.  For A (m x k): lower keeps kk <= i,
+  // upper kk >= i, strictly upper kk > i.  For B (k x n): lower keeps
+  // kk >= j, upper kk <= j.  a_tri/b_tri apply to product 1, a2_tri/b2_tri
+  // to product 2.
   int a_tri, b_tri, a2_tri, b2_tri;
   int inplace;  // C aliases B: the executor must read all of B's column block
                 // before writing it (the planner guarantees m <= inplace_rows())
@@ -178,6 +179,10 @@ int trsm_lt_lowerout(Exec& ex, View L, int n, View B, int math = 0);
 // S is returned as a view into D.
 int spftrf_backward(Exec& ex, int transr, int lower, int n, const float* L,
                     const float* Lbar, float* D, int64_t ldd, View* S, int math = 0);
+// Y := alpha A X + beta Y for the symmetric matrix A held in the RFP array
+// (any variant); X, Y dense n x m views.  alpha == 0 reads neither A nor X.
+int rfp_symm(Exec& ex, int transr, int lower, int n, const float* A, View X, View Y, int m,
+             float alpha, float beta);
 // Y := alpha (G_L + G_L^T) X + beta Y where G_L is the stored lower triangle
 // (diagonal included, so the diagonal counts twice) of the RFP array G; X, Y
 // dense n x m views.

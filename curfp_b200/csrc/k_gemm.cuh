@@ -73,7 +73,7 @@ __device__ __forceinline__ int swz(int r, int kk) {
 
 // One operand of one product is seen as rows r (m of A or n of B) by kk:
 // element (r, kk) at p[r*sr + kk*sk]; tri in the (r, kk) convention: 1 keeps
-// kk <= r, 2 keeps kk >= r.  Flags: bit 0 = kk is the unit-stride dimension
+// kk <= r, 2 keeps kk >= r, 3 keeps kk > r.  Flags: bit 0 = kk is the unit-stride dimension
 // (else r), bit 1 = float4 loads allowed (unit stride +1, 16-byte aligned
 // base, other stride a multiple of 4).
 __device__ __forceinline__ int operand_flags(const float* p, int64_t sr, int64_t sk) {
@@ -117,7 +117,8 @@ __device__ __forceinline__ void stage_load(Stage<R, BK>& st, const float* p, int
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         const int rr = gr + (kcont ? 0 : c), kc = gk + (kcont ? c : 0);
-        const bool ok = rr < rows && kc < depth && (tri != 1 || kc <= rr) && (tri != 2 || kc >= rr);
+        const bool ok = rr < rows && kc < depth && (tri != 1 || kc <= rr) &&
+                        (tri != 2 || kc >= rr) && (tri != 3 || kc > rr);
         st.v[u][c] = ok ? __ldg(p + (int64_t)rr * sr + (int64_t)kc * sk) : 0.f;
       }
     }
@@ -152,7 +153,7 @@ __device__ __forceinline__ void k_range(int k, int a_tri, int b_tri, int m0, int
   kb = 0;
   ke = k;
   if (a_tri == 1) ke = min(ke, m0 + BM);   // kk <= i
-  if (a_tri == 2) kb = max(kb, m0);        // kk >= i
+  if (a_tri == 2 || a_tri == 3) kb = max(kb, m0);  // kk >= i (kk > i)
   if (b_tri == 1) kb = max(kb, n0);        // kk >= j
   if (b_tri == 2) ke = min(ke, n0 + BN);   // kk <= j
   kb = (kb / BK) * BK;

@@ -43,6 +43,31 @@ struct PackArgs {
   float diag_scale;        // dense -> RFP: diagonal elements are multiplied by this
 };
 
+// The tile list of the three RFP blocks of geometry g (64 x 64 tiles; the
+// triangular blocks list only their lower-triangle tiles).  Returns the
+// number of tiles; drs / dcs / diag_scale are left to the caller.
+inline int pack_blocks(const Geometry& g, PackArgs* a) {
+  const BlockGeom* bg[3] = {&g.b11, &g.b21, &g.b22};
+  const int rows[3] = {g.n1, g.n2, g.n2}, cols[3] = {g.n1, g.n1, g.n2};
+  const int pb[3] = {0, g.n1, g.n1}, qb[3] = {0, 0, g.n1};
+  int tiles = 0, cnt = 0;
+  for (int b = 0; b < 3; ++b) {
+    if (rows[b] <= 0 || cols[b] <= 0) continue;
+    PackBlock& B = a->b[cnt++];
+    B.off = bg[b]->off; B.rs = bg[b]->rs; B.cs = bg[b]->cs;
+    B.rows = rows[b]; B.cols = cols[b];
+    B.p_base = pb[b]; B.q_base = qb[b];
+    B.tri = (b != 1);
+    B.tiles_p = (rows[b] + TS - 1) / TS;
+    B.tiles_q = (cols[b] + TS - 1) / TS;
+    B.tile_begin = tiles;
+    tiles += B.tri ? B.tiles_p * (B.tiles_p + 1) / 2 : B.tiles_p * B.tiles_q;
+  }
+  a->nblocks = cnt;
+  a->total_tiles = tiles;
+  return tiles;
+}
+
 __device__ __forceinline__ void pack_tile_coords(const PackBlock& B, int lt,
                                                  int& tp, int& tq) {
   if (!B.tri) {
@@ -142,7 +167,7 @@ __global__ void __launch_bounds__(TX * TY) pack_kernel(const PackArgs args,
 
 // idx[i] = RFP offset of diagonal element i (reference
 // curfp/__init__.py:194-269 builds the same two arithmetic progressions).
-__global__ void diag_indices(Geometry g, int64_t* idx) {
+static __global__ void diag_indices(Geometry g, int64_t* idx) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < g.n) idx[i] = diag_offset(g, i);
 }

@@ -459,35 +459,41 @@ int spftrf_backward(Exec& ex, int transr, int lower, int n, const float* L,
   return 0;
 }
 
-int rfp_symm_dbl(Exec& ex, int transr, int lower, int n, const float* G, View X, View Y,
-                 int m, float alpha, float beta) {
+namespace {
+// Y := alpha (G_L + G_L^T - s D) X + beta Y with D the diagonal of G_L:
+// s = 0 counts the diagonal twice, s = 1 once (the symmetric matrix itself;
+// the transposed triangles then exclude their diagonal).  The blocks follow
+// the reference's SSYMM + 2 SGEMM split (src/curfp_ssfmm.cpp:150-306):
+//   Y1 = a (G11 sym) X1 + a G21^T X2 + b Y1,  Y2 = a G21 X1 + a (G22 sym) X2 + b Y2
+int symm_blocks(Exec& ex, int transr, int lower, int n, const float* G, View X, View Y,
+                int m, float alpha, float beta, int once) {
   Blocks g = blocks(transr, lower, n, G);
   const int n1 = g.g.n1, n2 = g.g.n2;
+  const int up = once ? 3 : 2;  // mask of the transposed triangles
   View X1 = X, X2 = sub(X, n1, 0), Y1 = Y, Y2 = sub(Y, n1, 0);
-  int rc;
-  // Y1 = a (G11_L + G11_L^T) X1 + a G21^T X2 + b Y1
-  // Y2 = a G21 X1 + a (G22_L + G22_L^T) X2 + b Y2
+  const bool zero = alpha == 0.0f;  // C := beta C, A and X not read
   GemmProb p[2];
   int cnt = 0;
   if (n1 > 0) {
-    GemmProb q = gemm_prob(g.V11, X1, Y1, n1, m, n1, alpha, beta, 0);
+    GemmProb q = gemm_prob(g.V11, X1, Y1, n1, m, zero ? 0 : n1, alpha, beta, 0);
     q.a_tri = 1;
     q.A2 = tr(g.V11);
     q.B2 = X1;
-    q.k2 = n1;
-    q.a2_tri = 2;
+    q.k2 = zero ? 0 : n1;
+    q.a2_tri = up;
     p[cnt++] = q;
   }
   if (n2 > 0) {
-    GemmProb q = gemm_prob(g.V21, X1, Y2, n2, m, n1, alpha, beta, 0);
-    if (n1 == 0) q.k = 0;
+    GemmProb q = gemm_prob(g.V21, X1, Y2, n2, m, (zero || n1 == 0) ? 0 : n1, alpha, beta, 0);
     q.A2 = g.V22;
     q.B2 = X2;
-    q.k2 = n2;
+    q.k2 = zero ? 0 : n2;
     q.a2_tri = 1;
     p[cnt++] = q;
   }
+  int rc;
   if ((rc = ex.gemm(p, cnt))) return rc;
+  if (zero) return 0;
   cnt = 0;
   if (n1 > 0 && n2 > 0) {
     GemmProb q = gemm_prob(tr(g.V21), X2, Y1, n1, m, n2, alpha, 1.0f, 0);
@@ -495,10 +501,21 @@ int rfp_symm_dbl(Exec& ex, int transr, int lower, int n, const float* G, View X,
   }
   if (n2 > 0) {
     GemmProb q = gemm_prob(tr(g.V22), X2, Y2, n2, m, n2, alpha, 1.0f, 0);
-    q.a_tri = 2;
+    q.a_tri = up;
     p[cnt++] = q;
   }
   return ex.gemm(p, cnt);
+}
+}  // namespace
+
+int rfp_symm(Exec& ex, int transr, int lower, int n, const float* A, View X, View Y, int m,
+             float alpha, float beta) {
+  return symm_blocks(ex, transr, lower, n, A, X, Y, m, alpha, beta, 1);
+}
+
+int rfp_symm_dbl(Exec& ex, int transr, int lower, int n, const float* G, View X, View Y,
+                 int m, float alpha, float beta) {
+  return symm_blocks(ex, transr, lower, n, G, X, Y, m, alpha, beta, 0);
 }
 
 }  // namespace plan

@@ -24,7 +24,8 @@ enum KClass : int {
   K_DIAG = 7,     // diagonal index / shift / small helpers
   K_SYMM64 = 8,   // FP64-accumulated RFP symmetric multiply (residuals)
   K_TRSV = 9,     // wavefront triangular solves
-  K_NCLASS = 10
+  K_NORM = 10,    // RFP norms and condition-estimator vector kernels
+  K_NCLASS = 11
 };
 
 struct ProfRec {

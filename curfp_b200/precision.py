@@ -141,7 +141,7 @@ def release_workspace() -> None:
 
 
 KERNEL_CLASSES = ["sgemm", "tc_gemm", "tc_stage", "potrf_tile", "trtri", "lauum",
-                  "pack", "diag", "symm_acc64", "trsv_wave"]
+                  "pack", "diag", "symm_acc64", "trsv_wave", "norm"]
 
 
 def profile_enable(on: bool = True) -> None:

@@ -54,6 +54,19 @@ typedef enum {
     CURFP_FILL_MODE_UPPER = 1
 } curfpFillMode_t;
 
+/* Side of curfpSsfmm — reference include/curfp.h:41-44. */
+typedef enum {
+    CURFP_SIDE_LEFT  = 0,  /* C = alpha * A * B + beta * C */
+    CURFP_SIDE_RIGHT = 1   /* C = alpha * B * A + beta * C */
+} curfpSideMode_t;
+
+/* Norm type of curfpSlansf — reference include/curfp.h:47-53. */
+typedef enum {
+    CURFP_NORM_MAX = 0,  /* max |A(i,j)|                              */
+    CURFP_NORM_ONE = 1,  /* max column sum of |A| (= infinity norm)   */
+    CURFP_NORM_FRO = 2   /* Frobenius norm                            */
+} curfpNormType_t;
+
 /* Opaque handle — reference include/curfp.h:58.  The context holds the
  * stream, the device, a device-side info word and a grow-only workspace. */
 typedef struct curfpContext *curfpHandle_t;
@@ -243,6 +256,42 @@ curfpStatus_t curfpSgpnllBackward(curfpHandle_t handle, curfpOperation_t transr,
                                   float *Xbar, int ldxbar, double *sums,
                                   curfpMath_t math);
 
+/* Symmetric matrix (RFP) times dense: side = LEFT C := alpha*A*B + beta*C
+ * with A m x m; side = RIGHT C := alpha*B*A + beta*C with A n x n.  B, C
+ * column-major m x n (ldb, ldc >= m); alpha, beta host pointers.  FP32
+ * products on the SIMT GEMM kernels.  Replaces reference include/curfp.h:
+ * 334-348 (src/curfp_ssfmm.cpp:108-306). */
+curfpStatus_t curfpSsfmm(curfpHandle_t handle, curfpOperation_t transr,
+                         curfpFillMode_t uplo, curfpSideMode_t side, int m, int n,
+                         const float *alpha, const float *arf, const float *B,
+                         int ldb, const float *beta, float *C, int ldc);
+
+/* y := alpha*A*x + beta*y, A symmetric in RFP (n x n), x and y device vectors
+ * with BLAS increments (non-zero).  Replaces reference include/curfp.h:
+ * 160-172 (src/curfp_ssfmv.cpp:134-255). */
+curfpStatus_t curfpSsfmv(curfpHandle_t handle, curfpOperation_t transr,
+                         curfpFillMode_t uplo, int n, const float *alpha,
+                         const float *arf, const float *x, int incx,
+                         const float *beta, float *y, int incy);
+
+/* *result := the requested norm of the symmetric matrix held in arf (RFP,
+ * not a factor).  Waits for the handle's stream (host result).  n = 0 gives
+ * 0.  Replaces reference include/curfp.h:219-227 (src/curfp_slansf.cu:
+ * 280-435); sums of squares and column sums are accumulated in FP64 and
+ * there is no limit of 2^31 elements on MAX / FRO. */
+curfpStatus_t curfpSlansf(curfpHandle_t handle, curfpNormType_t norm,
+                          curfpOperation_t transr, curfpFillMode_t uplo, int n,
+                          const float *arf, float *result);
+
+/* *rcond := 1 / (||A^-1||_1 * anorm) from the RFP Cholesky factor, with
+ * ||A^-1||_1 estimated by the Hager-Higham iteration (LAPACK SLACN2, at most
+ * 5 iterations, each applying A^-1 by curfpSpftrs to one vector).  *rcond =
+ * 0 when n = 0 or anorm = 0.  Replaces reference include/curfp.h:242-250
+ * (src/curfp_spfcon.cu:88-271). */
+curfpStatus_t curfpSpfcon(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, int n, const float *arf,
+                          float anorm, float *rcond);
+
 /* Release the handle's workspaces (staging planes of the split-BF16 path,
  * refinement and adjoint scratch): waits for the handle's stream, frees every
  * buffer and returns the device pool's unused memory to the driver.  The
@@ -258,7 +307,7 @@ curfpStatus_t curfpGetKernelLaunchCount(curfpHandle_t handle, long long *count);
  * (0 SIMT GEMM, 1 tensor-core contraction, 2 tensor-core operand staging,
  * 3 Cholesky tiles, 4 triangular inverses, 5 L^T L tiles, 6 strttf/stfttr,
  * 7 diagonal helpers, 8 FP64-accumulated symmetric multiply, 9 wavefront
- * triangular solves).  Enabling (or disabling) clears the records;
+ * triangular solves, 10 norms and condition-estimator vectors).  Enabling (or disabling) clears the records;
  * curfpProfileRead synchronises the stream and returns the summed device
  * milliseconds, algorithmic flops and bytes, and the launch count of one
  * class. */

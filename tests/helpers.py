@@ -77,3 +77,27 @@ class RefLib:
     def stfttr(self, tr, ul, n, arf, A, lda):
         return self.lib.curfpSstfttr(self.h, tr, ul, n, ctypes.c_void_p(arf.data_ptr()),
                                      ctypes.c_void_p(A.data_ptr()), lda)
+
+    def ssfmm(self, tr, ul, side, m, n, alpha, arf, B, ldb, beta, C, ldc):
+        a, b = ctypes.c_float(alpha), ctypes.c_float(beta)
+        return self.lib.curfpSsfmm(self.h, tr, ul, side, m, n, ctypes.byref(a),
+                                   ctypes.c_void_p(arf.data_ptr()), ctypes.c_void_p(B.data_ptr()),
+                                   ldb, ctypes.byref(b), ctypes.c_void_p(C.data_ptr()), ldc)
+
+    def ssfmv(self, tr, ul, n, alpha, arf, x, incx, beta, y, incy):
+        a, b = ctypes.c_float(alpha), ctypes.c_float(beta)
+        return self.lib.curfpSsfmv(self.h, tr, ul, n, ctypes.byref(a),
+                                   ctypes.c_void_p(arf.data_ptr()), ctypes.c_void_p(x.data_ptr()),
+                                   incx, ctypes.byref(b), ctypes.c_void_p(y.data_ptr()), incy)
+
+    def slansf(self, norm, tr, ul, n, arf):
+        out = ctypes.c_float(0.0)
+        st = self.lib.curfpSlansf(self.h, norm, tr, ul, n, ctypes.c_void_p(arf.data_ptr()),
+                                  ctypes.byref(out))
+        return st, out.value
+
+    def spfcon(self, tr, ul, n, arf, anorm):
+        out = ctypes.c_float(0.0)
+        st = self.lib.curfpSpfcon(self.h, tr, ul, n, ctypes.c_void_p(arf.data_ptr()),
+                                  ctypes.c_float(anorm), ctypes.byref(out))
+        return st, out.value

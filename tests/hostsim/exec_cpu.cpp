@@ -43,8 +43,8 @@ class CpuExec : public Exec {
         for (int i = 0; i < g.m; ++i) {
           double s = 0.0;
           auto keep = [&](int at_, int bt_, int k) {
-            return (at_ != 1 || k <= i) && (at_ != 2 || k >= i) && (bt_ != 1 || k >= j) &&
-                   (bt_ != 2 || k <= j);
+            return (at_ != 1 || k <= i) && (at_ != 2 || k >= i) && (at_ != 3 || k > i) &&
+                   (bt_ != 1 || k >= j) && (bt_ != 2 || k <= j);
           };
           for (int k = 0; k < g.k; ++k)
             if (keep(g.a_tri, g.b_tri, k)) s += (double)at(g.A, i, k) * (double)at(g.B, k, j);
@@ -252,6 +252,18 @@ int hs_rfp_trsm(int transr, int lower, int n, const float* L, int trans, float* 
                 float alpha) {
   CpuExec ex;
   return plan::rfp_trsm(ex, transr, lower, n, L, trans, View{B, 1, n}, m, alpha, 0);
+}
+
+// Same planning as curfpSsfmm (side 0 left, 1 right; B, C column-major m x n).
+int hs_ssfmm(int transr, int lower, int side, int m, int n, float alpha, const float* A,
+             const float* B, int ldb, float beta, float* C, int ldc) {
+  CpuExec ex;
+  View Bv{const_cast<float*>(B), 1, ldb}, Cv{C, 1, ldc};
+  if (side) {
+    Bv = tr(Bv);
+    Cv = tr(Cv);
+  }
+  return plan::rfp_symm(ex, transr, lower, side ? n : m, A, Bv, Cv, side ? m : n, alpha, beta);
 }
 
 int hs_geometry(int n, int transr, int lower, int64_t* out) {

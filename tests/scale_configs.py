@@ -113,6 +113,17 @@ class Ours:
     def stfttr(self, tr, ul, n, arf, D):
         assert self.lib.curfpSstfttr(self.h.ptr, tr, ul, n, vp(arf), vp(D), n) == 0
 
+    def slansf(self, norm, tr, ul, n, C):
+        out = ctypes.c_float(0.0)
+        assert self.lib.curfpSlansf(self.h.ptr, norm, tr, ul, n, vp(C), ctypes.byref(out)) == 0
+        return float(out.value)
+
+    def spfcon(self, tr, ul, n, F, anorm):
+        out = ctypes.c_float(0.0)
+        assert self.lib.curfpSpfcon(self.h.ptr, tr, ul, n, vp(F), ctypes.c_float(anorm),
+                                    ctypes.byref(out)) == 0
+        return float(out.value)
+
     def release(self):
         assert self.lib.curfpReleaseWorkspace(self.h.ptr) == 0
 
@@ -448,6 +459,7 @@ def run_c3(args):
             if iters:
                 d["refine_corrections"] = iters[-1]
             d["errors_vs_fp64"] = solve_errors(orc, B0, X)
+            d.update(conditioning(ours, tr, ul, n, C, F))
             # the stored matrix against the exact one on 512 sampled rows
             d["ssfrk_rel_err_sampled"] = ssfrk_sample_err(ours, tr, ul, n, C, orc, 512)
             d["breakdown_ms"] = breakdown(lambda: (F.copy_(C), ours.spftrf(tr, ul, n, F, math_)))
@@ -460,6 +472,18 @@ def run_c3(args):
         emit(res, args.out)
         del orc
         torch.cuda.empty_cache()
+
+
+def conditioning(ours: Ours, tr, ul, n, C, F) -> dict:
+    """1-norm condition estimate of the stored matrix: slansf('1') of C and
+    spfcon on its factor F (both timed once, host result)."""
+    t0 = time.perf_counter()
+    anorm = ours.slansf(1, tr, ul, n, C)
+    t1 = time.perf_counter()
+    rc = ours.spfcon(tr, ul, n, F, anorm)
+    t2 = time.perf_counter()
+    return {"anorm_1": anorm, "rcond_spfcon": rc, "cond1_est": (1.0 / rc) if rc else None,
+            "slansf_ms": round((t1 - t0) * 1e3, 2), "spfcon_ms": round((t2 - t1) * 1e3, 2)}
 
 
 def ssfrk_sample_err(ours: Ours, tr, ul, n, C, orc: GramOracle, nrows: int) -> float:
@@ -546,6 +570,7 @@ def run_c5(args):
         "pipeline_ms": round(ms_s + ms_f + ms_x, 1),
         "refine_corrections": iters[-1],
         "errors_vs_fp64": solve_errors(orc, B0, X),
+        **conditioning(ours, tr, ul, n, C, F),
         "ssfrk_rel_err_sampled": ssfrk_sample_err(ours, tr, ul, n, C, orc, 256),
         "breakdown_ms": breakdown(lambda: (F.copy_(C), ours.spftrf(tr, ul, n, F, 1))),
         "peak_mem_gb": round(torch.cuda.max_memory_allocated() / 1e9, 1)}

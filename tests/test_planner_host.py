@@ -98,3 +98,30 @@ def test_planner_info(orc, hostsim, tr, ul, n, bad):
     info = ctypes.c_int(-1)
     assert hostsim.hs_spftrf(tr, 1 - ul, n, fp(arf), ctypes.byref(info)) == 0
     assert info.value == bad
+
+
+@pytest.mark.parametrize("n,m", [(1, 3), (2, 1), (7, 5), (64, 3), (65, 8), (130, 1)])
+@pytest.mark.parametrize("side", [0, 1])
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+def test_planner_ssfmm(orc, hostsim, n, m, side, tr, ul):
+    """rfp_symm (ssfmm / ssfmv planning, strict-upper mask on the transposed
+    triangles) against the dense symmetric product: side 0 C = a A B + b C
+    (B n x m), side 1 C = a B A + b C (B m x n); column-major."""
+    rng = np.random.default_rng(11 * n + m + side)
+    nt = n * (n + 1) // 2
+    arf = rng.standard_normal(nt).astype(np.float32)
+    A = orc.rfp_to_dense_sym(tr, ul, n, arf.astype(np.float64))
+    rows, cols = (n, m) if side == 0 else (m, n)
+    B = np.asfortranarray(rng.standard_normal((rows, cols)).astype(np.float32))
+    C = np.asfortranarray(rng.standard_normal((rows, cols)).astype(np.float32))
+    want = 0.5 * (A @ B if side == 0 else B @ A) - 2.0 * C.astype(np.float64)
+    assert hostsim.hs_ssfmm(tr, 1 - ul, side, rows, cols, ctypes.c_float(0.5), fp(arf), fp(B),
+                            rows, ctypes.c_float(-2.0), fp(C), rows) == 0
+    np.testing.assert_allclose(C, want, rtol=1e-5, atol=1e-5)
+    # alpha = 0: C := beta C without reading A or B
+    C0 = C.copy()
+    bad = np.full(nt, np.nan, np.float32)
+    assert hostsim.hs_ssfmm(tr, 1 - ul, side, rows, cols, ctypes.c_float(0.0), fp(bad),
+                            fp(np.full_like(B, np.nan)), rows, ctypes.c_float(3.0), fp(C),
+                            rows) == 0
+    np.testing.assert_array_equal(C, 3.0 * C0)

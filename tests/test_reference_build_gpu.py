@@ -90,3 +90,64 @@ def test_info_vs_reference(curfp, ref, orc, tr, ul, n, bad):
     st, info_ref = ref.spftrf(tr, ul, n, a1)
     assert st == 0
     assert curfp.spftrf(a2, transr=TR[tr], uplo=UL[ul], check=False) == info_ref == bad
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,m", [(1, 4), (64, 3), (65, 17), (1000, 64), (1001, 1)])
+@pytest.mark.parametrize("side", [0, 1])
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+def test_ssfmm_vs_reference(curfp, ref, n, m, side, tr, ul):
+    """Same RFP matrix and operands through both libraries' curfpSsfmm:
+    agreement to FP32 summation-order spread (max-abs 2e-5 of the scale)."""
+    g = torch.Generator(device="cuda").manual_seed(n + 7 * m + side)
+    arf = torch.randn(n * (n + 1) // 2, device="cuda", generator=g)
+    rows, cols = (n, m) if side == 0 else (m, n)
+    B = torch.randn(cols, rows, device="cuda", generator=g)  # column-major rows x cols
+    C0 = torch.randn(cols, rows, device="cuda", generator=g)
+    C_ref, C_our = C0.clone(), C0.clone()
+    assert ref.ssfmm(tr, ul, side, rows, cols, 0.75, arf, B, rows, -0.5, C_ref, rows) == 0
+    curfp.ssfmm_raw(curfp._get_handle(), tr, ul, side, rows, cols, 0.75, arf, B, rows, -0.5,
+                    C_our, rows)
+    torch.cuda.synchronize()
+    scale = C_ref.abs().max().item()
+    assert (C_our - C_ref).abs().max().item() <= 2e-5 * scale * max(1.0, n ** 0.5 / 8)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 2, 65, 1000, 1001])
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+def test_ssfmv_and_norms_vs_reference(curfp, ref, n, tr, ul):
+    g = torch.Generator(device="cuda").manual_seed(n + 3)
+    arf = torch.randn(n * (n + 1) // 2, device="cuda", generator=g)
+    x = torch.randn(n, device="cuda", generator=g)
+    y0 = torch.randn(n, device="cuda", generator=g)
+    y_ref, y_our = y0.clone(), y0.clone()
+    assert ref.ssfmv(tr, ul, n, 1.5, arf, x, 1, 0.25, y_ref, 1) == 0
+    curfp.ssfmv(arf, x, y_our, alpha=1.5, beta=0.25, transr=TR[tr], uplo=UL[ul])
+    torch.cuda.synchronize()
+    scale = y_ref.abs().max().item()
+    assert (y_our - y_ref).abs().max().item() <= 2e-5 * scale * max(1.0, n ** 0.5 / 8)
+    for norm, s in ((0, "M"), (1, "1"), (2, "F")):
+        st, want = ref.slansf(norm, tr, ul, n, arf)
+        assert st == 0
+        got = curfp.slansf(arf, s, transr=TR[tr], uplo=UL[ul])
+        assert abs(got - want) <= 1e-5 * want, (s, got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 3, 64, 300, 1001])
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+def test_spfcon_vs_reference(curfp, ref, n, tr, ul):
+    """Both estimators on the same factor: the same iteration (argmax picks
+    and stopping) gives the same estimate up to FP32 solve differences."""
+    g = torch.Generator(device="cuda").manual_seed(n + 11)
+    A = torch.randn(n, max(1, n // 4), device="cuda", generator=g)
+    C = torch.empty(n * (n + 1) // 2, device="cuda")
+    curfp.ssfrk(A, C, alpha=1.0 / max(1, n // 4), transr=TR[tr], uplo=UL[ul])
+    curfp.add_to_diagonal(C, 0.05, transr=TR[tr], uplo=UL[ul])
+    anorm = curfp.slansf(C, "1", transr=TR[tr], uplo=UL[ul])
+    assert curfp.spftrf(C, transr=TR[tr], uplo=UL[ul]) == 0
+    st, want = ref.spfcon(tr, ul, n, C, anorm)
+    assert st == 0
+    got = curfp.spfcon(C, anorm, transr=TR[tr], uplo=UL[ul])
+    assert abs(got - want) <= 1e-3 * want, (got, want)
