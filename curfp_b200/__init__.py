@@ -28,6 +28,7 @@ __all__ = [
     "strttf_raw", "stfttr", "stfttr_raw", "ssfr2k", "ssfr2k_raw", "CurfpError",
     "NORM_MAX", "NORM_ONE", "NORM_FRO", "slansf", "slansf_raw", "spfcon", "spfcon_raw",
     "spftrf_rcond", "SIDE_LEFT", "SIDE_RIGHT", "ssfmm", "ssfmm_raw", "ssfmv", "ssfmv_raw",
+    "ssfr", "ssfr_raw", "ssfr2", "ssfr2_raw",
 ]
 
 # Enum values of include/curfp.h (reference curfp/_ext.cpp:869-877).
@@ -512,3 +513,55 @@ def ssfmm(arf: torch.Tensor, B: torch.Tensor, C: torch.Tensor = None, *, alpha: 
     ssfmm_raw(_get_handle(), _op(transr), _fill(uplo), _side(side), m, n, alpha, arf, B, m,
               beta, C, m)
     return C
+
+
+# ---------------------------------------------------------------------------
+# Rank-1 / rank-2 updates (reference curfp/__init__.py:966-1097)
+# ---------------------------------------------------------------------------
+
+def ssfr_raw(handle, transr: int, uplo: int, n: int, alpha: float, x: torch.Tensor,
+             incx: int, arf: torch.Tensor) -> None:
+    """arf := alpha*x*x^T + arf (BLAS increment incx)."""
+    _validate(x, "x")
+    _validate(arf, "arf")
+    a = ctypes.c_float(alpha)
+    check(_lib.load().curfpSsfr(_hp(handle), transr, uplo, n, ctypes.byref(a), _ptr(x), incx,
+                                _ptr(arf)))
+
+
+def ssfr(arf: torch.Tensor, x: torch.Tensor, *, alpha: float = 1.0, transr: str = "T",
+         uplo: str = "U", n: int = None) -> None:
+    """In-place symmetric rank-1 update arf := alpha*x*x^T + arf (RFP)."""
+    _validate(arf, "arf")
+    _validate(x, "x")
+    if n is None:
+        n = _n_from_rfp(arf.numel())
+    if x.numel() != n:
+        raise ValueError(f"x must have {n} elements, got {x.numel()}")
+    ssfr_raw(_get_handle(), _op(transr), _fill(uplo), n, alpha, x, 1, arf)
+
+
+def ssfr2_raw(handle, transr: int, uplo: int, n: int, alpha: float, x: torch.Tensor,
+              incx: int, y: torch.Tensor, incy: int, arf: torch.Tensor) -> None:
+    """arf := alpha*(x*y^T + y*x^T) + arf (BLAS increments)."""
+    _validate(x, "x")
+    _validate(y, "y")
+    _validate(arf, "arf")
+    a = ctypes.c_float(alpha)
+    check(_lib.load().curfpSsfr2(_hp(handle), transr, uplo, n, ctypes.byref(a), _ptr(x), incx,
+                                 _ptr(y), incy, _ptr(arf)))
+
+
+def ssfr2(arf: torch.Tensor, x: torch.Tensor, y: torch.Tensor, *, alpha: float = 1.0,
+          transr: str = "T", uplo: str = "U", n: int = None) -> None:
+    """In-place symmetric rank-2 update arf := alpha*(x*y^T + y*x^T) + arf."""
+    _validate(arf, "arf")
+    _validate(x, "x")
+    _validate(y, "y")
+    if n is None:
+        n = _n_from_rfp(arf.numel())
+    if x.numel() != n:
+        raise ValueError(f"x must have {n} elements, got {x.numel()}")
+    if y.numel() != n:
+        raise ValueError(f"y must have {n} elements, got {y.numel()}")
+    ssfr2_raw(_get_handle(), _op(transr), _fill(uplo), n, alpha, x, 1, y, 1, arf)

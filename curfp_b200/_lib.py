@@ -46,6 +46,8 @@ SIGNATURES = {
     "curfpSlansf": [_h, _i, _i, _i, _i, _p, ctypes.POINTER(_f)],
     "curfpSsfmm": [_h, _i, _i, _i, _i, _i, ctypes.POINTER(_f), _p, _p, _i,
                    ctypes.POINTER(_f), _p, _i],
+    "curfpSsfr": [_h, _i, _i, _i, ctypes.POINTER(_f), _p, _i, _p],
+    "curfpSsfr2": [_h, _i, _i, _i, ctypes.POINTER(_f), _p, _i, _p, _i, _p],
     "curfpSsfmv": [_h, _i, _i, _i, ctypes.POINTER(_f), _p, _p, _i, ctypes.POINTER(_f), _p, _i],
     "curfpSpfcon": [_h, _i, _i, _i, _p, _f, ctypes.POINTER(_f)],
     "curfpSpftrsNoAlloc": [_h, _i, _i, _i, _i, _p, _p, _i],

@@ -479,6 +479,43 @@ curfpStatus_t curfpSsfmv(curfpHandle_t handle, curfpOperation_t transr, curfpFil
                                        n, arf, X, Y, 1, *alpha, *beta));
 }
 
+namespace {
+// Shared body of curfpSsfr / curfpSsfr2 (y == nullptr: rank 1).
+curfpStatus_t rank_update(curfpHandle_t h, curfpOperation_t transr, curfpFillMode_t uplo, int n,
+                          const float* alpha, const float* x, int incx, const float* y,
+                          int incy, float* arf) {
+  if (!h) return CURFP_STATUS_NOT_INITIALIZED;
+  if (n < 0 || !alpha) return CURFP_STATUS_INVALID_VALUE;
+  if (n == 0 || *alpha == 0.0f) return CURFP_STATUS_SUCCESS;
+  if (incx == 0 || (y && incy == 0) || !x || !arf) return CURFP_STATUS_INVALID_VALUE;
+  Geometry g = rfp::geometry(n, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER);
+  rfp::kpack::PackArgs a{};
+  const int tiles = rfp::kpack::pack_blocks(g, &a);
+  const float* xb = x + (incx < 0 ? -(int64_t)(n - 1) * incx : 0);
+  const float* yb = y ? y + (incy < 0 ? -(int64_t)(n - 1) * incy : 0) : nullptr;
+  const double nt = (double)n * (n + 1) / 2;
+  rfp::ProfScope ps(h->prof, h->stream, rfp::K_PACK, (y ? 4.0 : 2.0) * nt, 8.0 * nt);
+  rfp::kpack::rank_update<<<tiles, dim3(rfp::kpack::TX, rfp::kpack::TY), 0, h->stream>>>(
+      a, arf, xb, incx, yb, incy, *alpha, y ? 1 : 0);
+  ++h->launches;
+  return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
+}
+}  // namespace
+
+// src/curfp_ssfr.cpp:99-173: C := alpha x x^T + C (alpha == 0: no-op).
+curfpStatus_t curfpSsfr(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                        int n, const float* alpha, const float* x, int incx, float* arf) {
+  return rank_update(handle, transr, uplo, n, alpha, x, incx, nullptr, 0, arf);
+}
+
+// src/curfp_ssfr2.cpp:94-190: C := alpha (x y^T + y x^T) + C (alpha == 0: no-op).
+curfpStatus_t curfpSsfr2(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                         int n, const float* alpha, const float* x, int incx, const float* y,
+                         int incy, float* arf) {
+  if (!y && handle && n > 0 && alpha && *alpha != 0.0f) return CURFP_STATUS_INVALID_VALUE;
+  return rank_update(handle, transr, uplo, n, alpha, x, incx, y ? y : x, incy, arf);
+}
+
 // ---------------------------------------------------------------------------
 // Adjoints (differentiation form)
 // ---------------------------------------------------------------------------
@@ -596,33 +633,50 @@ curfpStatus_t curfpSpftrsRefine(curfpHandle_t handle, curfpOperation_t transr,
   rfp::kref::copy_block<<<grid, 256, 0, st>>>(B0, n, B, ldb, n, nrhs);
   ++handle->launches;
   CudaExec ex(handle);
-  int rc = rfp::plan::spftrs(ex, tr, lower, n, nrhs, factor, B, ldb);
+  // The solves take split-BF16 tensor-core updates where large enough: the
+  // corrections need only FP32-level accuracy, the FP64 residual carries the
+  // refinement.
+  const int kMath = CURFP_MATH_SPLIT_BF16;
+  int rc = rfp::plan::spftrs(ex, tr, lower, n, nrhs, factor, B, ldb, kMath);
   if (rc) return status_of(rc);
   Geometry g = rfp::geometry(n, tr, lower);
   float prev = INFINITY;
+  auto absmax_of = [&](const float* M, int64_t ld, float* out) -> bool {
+    if (cudaMemsetAsync(nrm, 0, sizeof(unsigned), st) != cudaSuccess) return false;
+    rfp::kref::absmax<<<grid, 256, 0, st>>>(M, ld, n, nrhs, nrm);
+    ++handle->launches;
+    unsigned bits = 0;
+    if (!ok_launch() ||
+        cudaMemcpyAsync(&bits, nrm, sizeof(unsigned), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      return false;
+    memcpy(out, &bits, sizeof(float));
+    return true;
+  };
   for (int it = 0; it < max_iter; ++it) {
     // R := B0 - A X in FP64
     rfp::kref::copy_block<<<grid, 256, 0, st>>>(R, n, B0, n, n, nrhs);
     if ((rc = symm_launch(handle, g, Aorig, B, ldb, R, n, nrhs, -1.0f, 1.0f)))
       return status_of(rc);
-    cudaMemsetAsync(nrm, 0, sizeof(unsigned), st);
-    rfp::kref::absmax<<<grid, 256, 0, st>>>(R, n, n, nrhs, nrm);
-    handle->launches += 2;
-    if (!ok_launch()) return CURFP_STATUS_EXECUTION_FAILED;
-    unsigned bits = 0;
-    if (cudaMemcpyAsync(&bits, nrm, sizeof(unsigned), cudaMemcpyDeviceToHost, st) !=
-            cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      return CURFP_STATUS_EXECUTION_FAILED;
+    ++handle->launches;
     float r;
-    memcpy(&r, &bits, sizeof(r));
+    if (!absmax_of(R, n, &r)) return CURFP_STATUS_EXECUTION_FAILED;
     if (!(r < 0.5f * prev) || r == 0.0f) break;  // converged or stalled
     prev = r;
-    if ((rc = rfp::plan::spftrs(ex, tr, lower, n, nrhs, factor, R, n))) return status_of(rc);
+    if ((rc = rfp::plan::spftrs(ex, tr, lower, n, nrhs, factor, R, n, kMath)))
+      return status_of(rc);
     rfp::kref::add_inplace<<<grid, 256, 0, st>>>(B, ldb, R, n, n, nrhs);
     ++handle->launches;
     if (!ok_launch()) return CURFP_STATUS_EXECUTION_FAILED;
     if (iters) *iters = it + 1;
+    // A correction below 4 ulp of the solution: another residual would not
+    // change the FP32 result.
+    float d, x;
+    if (it + 1 < max_iter) {
+      if (!absmax_of(R, n, &d) || !absmax_of(B, ldb, &x)) return CURFP_STATUS_EXECUTION_FAILED;
+      if (d <= 0x1p-22f * x) break;
+    }
   }
   return CURFP_STATUS_SUCCESS;
 }

@@ -58,6 +58,7 @@ constexpr int kInvStride = 2 * kTrsmLeaf * kTrsmLeaf;
 constexpr int kTriTile = 64;     // trtri / lauum tiles
 constexpr int kTrmmLeaf = 64;    // TRMM leaves (masked in-place multiply)
 constexpr int kTrsvMaxRhs = 512; // wavefront solve for at most this many RHS
+constexpr int kTrsvMaxRhsTc = 64;  // ... when the updates may use the tensor cores
 constexpr int kWaveLeaf = 512;   // recursive TRSM hands blocks <= this to the wavefront solve
 constexpr int kWaveLeafWide = 512;  // ... when there are more than 4 * kTrsvMaxRhs RHS
 constexpr int kNotSupported = -1;
@@ -146,7 +147,7 @@ int ssfr2k(Exec& ex, int transr, int lower, int trans, int n, int k,
            float beta, float* C);
 int spftrf(Exec& ex, int transr, int lower, int n, float* A, int math = 0);
 int spftrs(Exec& ex, int transr, int lower, int n, int nrhs, const float* A,
-           float* B, int ldb);
+           float* B, int ldb, int math = 0);
 int spftri(Exec& ex, int transr, int lower, int n, float* A);
 // In place: the RFP factor L := L^-1 (the first half of spftri).
 int rfp_trtri(Exec& ex, int transr, int lower, int n, float* A, int math = 0);

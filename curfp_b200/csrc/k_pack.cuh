@@ -165,6 +165,51 @@ __global__ void __launch_bounds__(TX * TY) pack_kernel(const PackArgs args,
   }
 }
 
+// BLAS-2 rank updates over the stored elements (tiles of pack_blocks, warp
+// along the block's contiguous dimension, read-modify-write once):
+//   two = 0:  a(p,q) += (alpha x_q) x_p                      (ssfr, SSYR form)
+//   two = 1:  a(p,q) += x_p (alpha y_q) + y_p (alpha x_q)    (ssfr2, SSYR2 form)
+// x and y element i at x[i * incx] (the caller shifts the base for negative
+// increments).
+static __global__ void __launch_bounds__(TX * TY)
+    rank_update(const PackArgs args, float* arf, const float* __restrict__ x, int64_t incx,
+                const float* __restrict__ y, int64_t incy, float alpha, int two) {
+  __shared__ float xp[TS], xq[TS], yp[TS], yq[TS];
+  int t = blockIdx.x, bi = 0;
+  while (bi + 1 < args.nblocks && t >= args.b[bi + 1].tile_begin) ++bi;
+  const PackBlock& B = args.b[bi];
+  int tp, tq;
+  pack_tile_coords(B, t - B.tile_begin, tp, tq);
+  const int p0 = tp * TS, q0 = tq * TS;
+  const int prow = B.rows - p0, qcol = B.cols - q0;
+  const int64_t P0 = (int64_t)B.p_base + p0, Q0 = (int64_t)B.q_base + q0;
+  const int tx = threadIdx.x, ty = threadIdx.y, lin = ty * TX + tx;
+  if (lin < TS) {
+    xp[lin] = lin < prow ? x[(P0 + lin) * incx] : 0.f;
+    xq[lin] = lin < qcol ? alpha * x[(Q0 + lin) * incx] : 0.f;
+    if (two) {
+      yp[lin] = lin < prow ? y[(P0 + lin) * incy] : 0.f;
+      yq[lin] = lin < qcol ? alpha * y[(Q0 + lin) * incy] : 0.f;
+    }
+  }
+  __syncthreads();
+  float* base = arf + B.off + (int64_t)p0 * B.rs + (int64_t)q0 * B.cs;
+  const bool qc = (B.cs == 1 || B.cs == -1);
+  const int64_t sl = qc ? B.cs : B.rs, sw = qc ? B.rs : B.cs;
+#pragma unroll
+  for (int r = 0; r < TS / TY; ++r) {
+#pragma unroll
+    for (int h = 0; h < TS / TX; ++h) {
+      const int l = tx + TX * h, w = ty + TY * r;
+      const int lp = qc ? w : l, lq = qc ? l : w;
+      if (lp < prow && lq < qcol && (!B.tri || p0 + lp >= q0 + lq)) {
+        float* e = base + (int64_t)l * sl + (int64_t)w * sw;
+        *e = two ? fmaf(yp[lp], xq[lq], fmaf(xp[lp], yq[lq], *e)) : fmaf(xp[lp], xq[lq], *e);
+      }
+    }
+  }
+}
+
 // idx[i] = RFP offset of diagonal element i (reference
 // curfp/__init__.py:194-269 builds the same two arithmetic progressions).
 static __global__ void diag_indices(Geometry g, int64_t* idx) {

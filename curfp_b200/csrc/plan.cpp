@@ -71,7 +71,9 @@ int trsm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math) {
   if (!W) return 2;
   int rc = ex.trtri_blocks(L, n, kTrsmLeaf, W);
   if (rc) return rc;
-  if (m <= kTrsvMaxRhs) {
+  // One wavefront launch for few right-hand sides; with tensor-core updates
+  // available the recursive solve wins above kTrsvMaxRhsTc of them.
+  if (m <= (math ? kTrsvMaxRhsTc : kTrsvMaxRhs)) {
     rc = ex.trsm_wave(L, n, B, m, alpha, W);
     if (rc != kNotSupported) return rc;
   }
@@ -237,7 +239,7 @@ int spftrf(Exec& ex, int transr, int lower, int n, float* A, int math) {
 }
 
 int spftrs(Exec& ex, int transr, int lower, int n, int nrhs, const float* A,
-           float* B, int ldb) {
+           float* B, int ldb, int math) {
   Geometry g = geometry(n, transr, lower);
   float* Af = const_cast<float*>(A);
   View V11 = block_view(Af, g.b11), V21 = block_view(Af, g.b21),
@@ -246,19 +248,19 @@ int spftrs(Exec& ex, int transr, int lower, int n, int nrhs, const float* A,
   View B2 = sub(B1, g.n1, 0);
   int rc;
   // Forward: L Y = B.
-  if ((rc = trsm_lln(ex, V11, g.n1, B1, nrhs, 1.0f))) return rc;
+  if ((rc = trsm_lln(ex, V11, g.n1, B1, nrhs, 1.0f, math))) return rc;
   if (g.n1 > 0 && g.n2 > 0) {
-    GemmProb p = gemm_prob(V21, B1, B2, g.n2, nrhs, g.n1, -1.0f, 1.0f, 0);
+    GemmProb p = gemm_prob(V21, B1, B2, g.n2, nrhs, g.n1, -1.0f, 1.0f, math);
     if ((rc = ex.gemm(&p, 1))) return rc;
   }
-  if ((rc = trsm_lln(ex, V22, g.n2, B2, nrhs, 1.0f))) return rc;
+  if ((rc = trsm_lln(ex, V22, g.n2, B2, nrhs, 1.0f, math))) return rc;
   // Backward: L^T X = Y.
-  if ((rc = trsm(ex, 1, 1, 1, V22, B2, g.n2, nrhs, 1.0f))) return rc;
+  if ((rc = trsm(ex, 1, 1, 1, V22, B2, g.n2, nrhs, 1.0f, math))) return rc;
   if (g.n1 > 0 && g.n2 > 0) {
-    GemmProb p = gemm_prob(tr(V21), B2, B1, g.n1, nrhs, g.n2, -1.0f, 1.0f, 0);
+    GemmProb p = gemm_prob(tr(V21), B2, B1, g.n1, nrhs, g.n2, -1.0f, 1.0f, math);
     if ((rc = ex.gemm(&p, 1))) return rc;
   }
-  return trsm(ex, 1, 1, 1, V11, B1, g.n1, nrhs, 1.0f);
+  return trsm(ex, 1, 1, 1, V11, B1, g.n1, nrhs, 1.0f, math);
 }
 
 int rfp_trtri(Exec& ex, int transr, int lower, int n, float* A, int math) {

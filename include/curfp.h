@@ -174,10 +174,12 @@ curfpStatus_t curfpSpftrfEx(curfpHandle_t handle, curfpOperation_t transr,
 /* Solve A*X = B with iterative refinement: X0 = spftrs(factor, B), then
  * repeatedly R = B - A*X with the products of the ORIGINAL matrix Aorig (RFP,
  * same transr/uplo) summed in FP64, D = spftrs(factor, R), X += D, for at most
- * max_iter corrections, stopping when max|R| no longer halves.  B (n x nrhs,
- * column-major, ldb >= n) is overwritten with X; *iters (host, may be NULL)
- * receives the number of corrections applied.  Synchronises the stream once
- * per iteration (the stopping test). */
+ * max_iter corrections, stopping when max|R| no longer halves or when a
+ * correction is below 4 ulp of max|X|.  The solves use split-BF16 tensor-core
+ * updates where they are large enough (the FP64 residual carries the
+ * accuracy).  B (n x nrhs, column-major, ldb >= n) is overwritten with X;
+ * *iters (host, may be NULL) receives the number of corrections applied.
+ * Synchronises the stream for each stopping test. */
 curfpStatus_t curfpSpftrsRefine(curfpHandle_t handle, curfpOperation_t transr,
                                 curfpFillMode_t uplo, int n, int nrhs,
                                 const float *Aorig, const float *factor,
@@ -273,6 +275,20 @@ curfpStatus_t curfpSsfmv(curfpHandle_t handle, curfpOperation_t transr,
                          curfpFillMode_t uplo, int n, const float *alpha,
                          const float *arf, const float *x, int incx,
                          const float *beta, float *y, int incy);
+
+/* Rank-1 update C := alpha*x*x^T + C of the RFP matrix (alpha host pointer,
+ * x device vector with BLAS increment; alpha = 0 is a no-op).  Replaces
+ * reference include/curfp.h:261-270 (src/curfp_ssfr.cpp:99-173). */
+curfpStatus_t curfpSsfr(curfpHandle_t handle, curfpOperation_t transr,
+                        curfpFillMode_t uplo, int n, const float *alpha,
+                        const float *x, int incx, float *arf);
+
+/* Rank-2 update C := alpha*(x*y^T + y*x^T) + C.  Replaces reference
+ * include/curfp.h:281-292 (src/curfp_ssfr2.cpp:94-190). */
+curfpStatus_t curfpSsfr2(curfpHandle_t handle, curfpOperation_t transr,
+                         curfpFillMode_t uplo, int n, const float *alpha,
+                         const float *x, int incx, const float *y, int incy,
+                         float *arf);
 
 /* *result := the requested norm of the symmetric matrix held in arf (RFP,
  * not a factor).  Waits for the handle's stream (host result).  n = 0 gives

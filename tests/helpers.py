@@ -101,3 +101,15 @@ class RefLib:
         st = self.lib.curfpSpfcon(self.h, tr, ul, n, ctypes.c_void_p(arf.data_ptr()),
                                   ctypes.c_float(anorm), ctypes.byref(out))
         return st, out.value
+
+    def ssfr(self, tr, ul, n, alpha, x, incx, arf):
+        a = ctypes.c_float(alpha)
+        return self.lib.curfpSsfr(self.h, tr, ul, n, ctypes.byref(a), ctypes.c_void_p(x.data_ptr()),
+                                  incx, ctypes.c_void_p(arf.data_ptr()))
+
+    def ssfr2(self, tr, ul, n, alpha, x, incx, y, incy, arf):
+        a = ctypes.c_float(alpha)
+        return self.lib.curfpSsfr2(self.h, tr, ul, n, ctypes.byref(a),
+                                   ctypes.c_void_p(x.data_ptr()), incx,
+                                   ctypes.c_void_p(y.data_ptr()), incy,
+                                   ctypes.c_void_p(arf.data_ptr()))

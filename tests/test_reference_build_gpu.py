@@ -151,3 +151,22 @@ def test_spfcon_vs_reference(curfp, ref, n, tr, ul):
     assert st == 0
     got = curfp.spfcon(C, anorm, transr=TR[tr], uplo=UL[ul])
     assert abs(got - want) <= 1e-3 * want, (got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 2, 65, 1000, 1001])
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+def test_ssfr_ssfr2_vs_reference(curfp, ref, n, tr, ul):
+    g = torch.Generator(device="cuda").manual_seed(n + 17)
+    arf = torch.randn(n * (n + 1) // 2, device="cuda", generator=g)
+    x = torch.randn(n, device="cuda", generator=g)
+    y = torch.randn(n, device="cuda", generator=g)
+    a_ref, a_our = arf.clone(), arf.clone()
+    assert ref.ssfr(tr, ul, n, 0.75, x, 1, a_ref) == 0
+    curfp.ssfr(a_our, x, alpha=0.75, transr=TR[tr], uplo=UL[ul])
+    torch.cuda.synchronize()
+    assert (a_our - a_ref).abs().max().item() <= 1e-6 * a_ref.abs().max().item()
+    assert ref.ssfr2(tr, ul, n, -0.5, x, 1, y, 1, a_ref) == 0
+    curfp.ssfr2(a_our, x, y, alpha=-0.5, transr=TR[tr], uplo=UL[ul])
+    torch.cuda.synchronize()
+    assert (a_our - a_ref).abs().max().item() <= 2e-6 * a_ref.abs().max().item()

@@ -1,6 +1,6 @@
-"""ssfmm / ssfmv on the GPU, all 8 variants and both sides, against FP64
-products of the dense symmetric matrix (oracle expansion of the RFP array):
-max-abs error within 2e-6 of the product's scale times sqrt(n)/8 (FP32
+"""ssfmm / ssfmv / ssfr / ssfr2 on the GPU, all 8 variants (both sides for ssfmm),
+against FP64 products of the dense symmetric matrix (oracle expansion of the RFP
+array): max-abs error within 2e-6 of the scale times sqrt(n)/8 (FP32
 summation).  Also: BLAS increments (negative, strided), alpha = 0 reads
 neither A nor B, beta = 0 does not read C, argument errors."""
 import numpy as np
@@ -100,3 +100,36 @@ def test_symm_argument_errors(curfp):
         curfp.ssfmv_raw(h, 1, 1, 4, 1.0, A, B, 0, 0.0, B, 1)  # incx = 0
     with pytest.raises(ValueError):
         curfp.ssfmm(A, torch.zeros(3, 4, device="cuda"))  # side L: A is 4 x 4, B has 3 rows
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 2, 3, 64, 65, 1000, 4097])
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+@pytest.mark.parametrize("incx,incy", [(1, 1), (2, -3)])
+def test_ssfr_ssfr2_vs_fp64(curfp, orc, n, tr, ul, incx, incy):
+    """Rank-1 / rank-2 updates of every stored element against FP64: one
+    rounding of two FMAs per element (<= 2 ulp of the operand scale)."""
+    rng = np.random.default_rng(n + incy)
+    nt = n * (n + 1) // 2
+    arf = rng.standard_normal(nt).astype(np.float32)
+    xs = rng.standard_normal(n * abs(incx)).astype(np.float32)
+    ys = rng.standard_normal(n * abs(incy)).astype(np.float32)
+    ix = np.arange(n) * incx if incx > 0 else (n - 1 - np.arange(n)) * -incx
+    iy = np.arange(n) * incy if incy > 0 else (n - 1 - np.arange(n)) * -incy
+    x, y = xs[ix].astype(np.float64), ys[iy].astype(np.float64)
+    A = orc.rfp_to_dense_sym(tr, ul, n, arf.astype(np.float64))
+    h = curfp._get_handle()
+    a1 = dev(arf)
+    curfp.ssfr_raw(h, tr, ul, n, 0.75, dev(xs), incx, a1)
+    got = orc.rfp_to_dense_sym(tr, ul, n, host(a1).astype(np.float64))
+    want = A + 0.75 * np.outer(x, x)
+    assert np.abs(got - want).max() <= 4e-7 * max(1.0, np.abs(want).max())
+    a2 = dev(arf)
+    curfp.ssfr2_raw(h, tr, ul, n, -0.5, dev(xs), incx, dev(ys), incy, a2)
+    got = orc.rfp_to_dense_sym(tr, ul, n, host(a2).astype(np.float64))
+    want = A - 0.5 * (np.outer(x, y) + np.outer(y, x))
+    assert np.abs(got - want).max() <= 6e-7 * max(1.0, np.abs(want).max())
+    # alpha = 0: no-op, x not read
+    a3 = dev(arf)
+    curfp.ssfr_raw(h, tr, ul, n, 0.0, torch.full((n,), float("nan"), device="cuda"), 1, a3)
+    np.testing.assert_array_equal(host(a3), arf)
