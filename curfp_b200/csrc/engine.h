@@ -17,10 +17,11 @@ namespace rfp {
 
 // C(m x n) := alpha * (A(m x k) B(k x n) + A2(m x k2) B2(k2 x n)) + beta * C
 // beta == 0 means C is not read.  k2 == 0 disables the second product.
-struct GemmProb {
-  View A, B, A2, B2, C;
+template <typename T>
+struct GemmProbT {
+  ViewT<T> A, B, A2, B2, C;
   int m, n, k, k2;
-  float alpha, beta;
+  T alpha, beta;
   int c_lower;  // write only C(i,j) with i >= j (tiles above the diagonal skipped)
   // Triangular operands: 0 = full, 1 = lower (incl. diagonal), 2 = upper
   // (incl. diagonal), 3 = strictly upper (A operands only); elements outside
@@ -32,8 +33,9 @@ struct GemmProb {
   int inplace;  // C aliases B: the executor must read all of B's column block
                 // before writing it (the planner guarantees m <= inplace_rows())
   int math;     // 0 = FP32 FMA, 1 = split-BF16 tensor cores (engine may ignore
-                // for small problems)
+                // for small problems and for FP64)
 };
+using GemmProb = GemmProbT<float>;
 
 constexpr int kMaxBatch = 4;
 
@@ -41,12 +43,22 @@ constexpr int kMaxBatch = 4;
 // same matrix X (rows x k): C := alpha * X[a_row0:+m, :] X[b_row0:+n, :]^T
 // + beta * C.  SYRK updates of the RFP blocks and the three blocks of ssfrk
 // are of this form, so the operand is staged (split) once for all of them.
-struct SharedTask {
+template <typename T>
+struct SharedTaskT {
   int a_row0, b_row0, m, n;
-  View C;
-  float alpha, beta;
+  ViewT<T> C;
+  T alpha, beta;
   int c_lower;  // 1: write only i >= j; 2 (executor-internal): only i <= j
 };
+using SharedTask = SharedTaskT<float>;
+
+// Non-deduced scalar parameter: the element type comes from the executor.
+template <typename T>
+struct Id {
+  using type = T;
+};
+template <typename T>
+using Scalar = typename Id<T>::type;
 
 // Block sizes of the recursive algorithms.
 constexpr int kPotrfTile = 128;  // diagonal Cholesky tiles
@@ -63,47 +75,48 @@ constexpr int kWaveLeaf = 512;   // recursive TRSM hands blocks <= this to the w
 constexpr int kWaveLeafWide = 512;  // ... when there are more than 4 * kTrsvMaxRhs RHS
 constexpr int kNotSupported = -1;
 
-class Exec {
+template <typename T>
+class ExecT {
  public:
-  virtual ~Exec() {}
+  virtual ~ExecT() {}
   // Independent problems, executed as one launch where possible.
-  virtual int gemm(const GemmProb* p, int count) = 0;
+  virtual int gemm(const GemmProbT<T>* p, int count) = 0;
   // In-place Cholesky of the lower triangle of L (n <= kPotrfTile).  On the
   // first non-positive (or NaN) pivot at local column j the device info word
   // becomes min(info, info_base + j + 1) and the tile stops.
-  virtual int potrf_tile(View L, int n, int info_base) = 0;
+  virtual int potrf_tile(ViewT<T> L, int n, int info_base) = 0;
   // Inverses of the diagonal nb x nb blocks of lower L (n x n): block b is
   // written to W + b*nb*nb, column-major with ld nb, zeros above the diagonal.
   // (W: nblk records of kInvStride floats, see kInvStride)
-  virtual int trtri_blocks(View L, int n, int nb, float* W) = 0;
+  virtual int trtri_blocks(ViewT<T> L, int n, int nb, T* W) = 0;
   // In-place inverse of lower L (n <= kTriTile).
-  virtual int trtri_tile(View L, int n) = 0;
+  virtual int trtri_tile(ViewT<T> L, int n) = 0;
   // In-place L := L^T L (lower triangle; n <= kTriTile).
-  virtual int lauum_tile(View L, int n) = 0;
-  // Scratch of at least nfloats, valid until the next workspace() call.
-  virtual float* workspace(size_t nfloats) = 0;
+  virtual int lauum_tile(ViewT<T> L, int n) = 0;
+  // Scratch of at least count elements, valid until the next workspace() call.
+  virtual T* workspace(size_t count) = 0;
   // Largest m of an in-place GEMM.
   virtual int inplace_rows() const = 0;
   // One-launch triangular solve L X = alpha B for few right-hand sides, with
   // W holding the inverted 64 x 64 diagonal blocks (trtri_blocks).  Returns
   // kNotSupported when the executor has no such path (the planner then uses
   // the recursive blocked solve).
-  virtual int trsm_wave(View L, int n, View B, int m, float alpha, const float* W) {
+  virtual int trsm_wave(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const T* W) {
     (void)L; (void)n; (void)B; (void)m; (void)alpha; (void)W;
     return kNotSupported;
   }
   // D(j,i) := D(i,j) for i > j (n x n view): the stored lower triangle is
   // mirrored into the upper one.
-  virtual int mirror_lower(View D, int n) = 0;
+  virtual int mirror_lower(ViewT<T> D, int n) = 0;
   // Contractions sharing one operand matrix.  The default lowers them to
   // gemm(); the CUDA executor stages X once for the tensor-core path.
-  virtual int gemm_shared(View X, int rows, int k, const SharedTask* t, int count,
+  virtual int gemm_shared(ViewT<T> X, int rows, int k, const SharedTaskT<T>* t, int count,
                           int math) {
     (void)rows;
-    GemmProb p[kMaxBatch];
+    GemmProbT<T> p[kMaxBatch];
     if (count > kMaxBatch) return 3;
     for (int i = 0; i < count; ++i) {
-      GemmProb& g = p[i];
+      GemmProbT<T>& g = p[i];
       g.A = sub(X, t[i].a_row0, 0);
       g.B = tr(sub(X, t[i].b_row0, 0));
       g.A2 = g.A; g.B2 = g.B;
@@ -117,60 +130,79 @@ class Exec {
     return gemm(p, count);
   }
 };
+using Exec = ExecT<float>;
 
 namespace plan {
 
 // L X = alpha B (L n x n lower, non-unit; B n x m), X overwrites B.
-int trsm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math = 0);
+template <typename T>
+int trsm_lln(ExecT<T>& ex, ViewT<T> L, int n, ViewT<T> B, int m, Scalar<T> alpha, int math = 0);
 // op(T) X = alpha B (left) or X op(T) = alpha B (right); B is rows x cols.
-int trsm(Exec& ex, int left, int lower, int trans, View T, View B, int rows,
-         int cols, float alpha, int math = 0);
+template <typename T>
+int trsm(ExecT<T>& ex, int left, int lower, int trans, ViewT<T> Tm, ViewT<T> B, int rows,
+         int cols, Scalar<T> alpha, int math = 0);
 // B := alpha L B (L lower n x n, B n x m).
-int trmm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math = 0);
+template <typename T>
+int trmm_lln(ExecT<T>& ex, ViewT<T> L, int n, ViewT<T> B, int m, Scalar<T> alpha, int math = 0);
 // B := alpha op(T) B (left) or alpha B op(T) (right).
-int trmm(Exec& ex, int left, int lower, int trans, View T, View B, int rows,
-         int cols, float alpha, int math = 0);
+template <typename T>
+int trmm(ExecT<T>& ex, int left, int lower, int trans, ViewT<T> Tm, ViewT<T> B, int rows,
+         int cols, Scalar<T> alpha, int math = 0);
 // In-place lower Cholesky; info_base is added to local failure columns.
-int potrf_lower(Exec& ex, View A, int n, int info_base, int math = 0);
+template <typename T>
+int potrf_lower(ExecT<T>& ex, ViewT<T> A, int n, int info_base, int math = 0);
 // In-place inverse of a lower triangular matrix.
-int trtri_lower(Exec& ex, View L, int n, int math = 0);
+template <typename T>
+int trtri_lower(ExecT<T>& ex, ViewT<T> L, int n, int math = 0);
 // In-place L := L^T L (lower part).
-int lauum_lower(Exec& ex, View L, int n, int math = 0);
+template <typename T>
+int lauum_lower(ExecT<T>& ex, ViewT<T> L, int n, int math = 0);
 
 // RFP routines (logical level, all 8 variants through rfp::geometry).
 // transr: 0 = N, 1 = T; lower: 1 = L, 0 = U; trans: 0 = N, 1 = T.
-int ssfrk(Exec& ex, int transr, int lower, int trans, int n, int k,
-          float alpha, const float* A, int lda, float beta, float* C,
+template <typename T>
+int ssfrk(ExecT<T>& ex, int transr, int lower, int trans, int n, int k,
+          Scalar<T> alpha, const T* A, int lda, Scalar<T> beta, T* C,
           int math = 0);
-int ssfr2k(Exec& ex, int transr, int lower, int trans, int n, int k,
-           float alpha, const float* A, int lda, const float* B, int ldb,
-           float beta, float* C);
-int spftrf(Exec& ex, int transr, int lower, int n, float* A, int math = 0);
-int spftrs(Exec& ex, int transr, int lower, int n, int nrhs, const float* A,
-           float* B, int ldb, int math = 0);
-int spftri(Exec& ex, int transr, int lower, int n, float* A);
+template <typename T>
+int ssfr2k(ExecT<T>& ex, int transr, int lower, int trans, int n, int k,
+           Scalar<T> alpha, const T* A, int lda, const T* B, int ldb,
+           Scalar<T> beta, T* C);
+template <typename T>
+int spftrf(ExecT<T>& ex, int transr, int lower, int n, T* A, int math = 0);
+template <typename T>
+int spftrs(ExecT<T>& ex, int transr, int lower, int n, int nrhs, const T* A,
+           T* B, int ldb, int math = 0);
+template <typename T>
+int spftri(ExecT<T>& ex, int transr, int lower, int n, T* A);
 // In place: the RFP factor L := L^-1 (the first half of spftri).
-int rfp_trtri(Exec& ex, int transr, int lower, int n, float* A, int math = 0);
+template <typename T>
+int rfp_trtri(ExecT<T>& ex, int transr, int lower, int n, T* A, int math = 0);
 
 // Building blocks of the adjoints, on the logical lower factor L held in an
 // RFP array (all 8 variants):
 // L X = alpha B (trans = 0) or L^T X = alpha B (trans = 1), B dense n x m.
-int rfp_trsm(Exec& ex, int transr, int lower, int n, const float* L, int trans, View B,
-             int m, float alpha, int math = 0);
+template <typename T>
+int rfp_trsm(ExecT<T>& ex, int transr, int lower, int n, const T* L, int trans, ViewT<T> B,
+             int m, Scalar<T> alpha, int math = 0);
 // B := L^T B (B dense n x m).
-int rfp_trmm_t(Exec& ex, int transr, int lower, int n, const float* L, View B, int m);
+template <typename T>
+int rfp_trmm_t(ExecT<T>& ex, int transr, int lower, int n, const T* L, ViewT<T> B, int m);
 // D(i,j) := (L^T Lbar)(i,j) for i >= j (D dense n x n view; upper part
 // untouched); L and Lbar in RFP with the same variant.
-int rfp_ltl(Exec& ex, int transr, int lower, int n, const float* L, const float* Lbar,
-            View D);
+template <typename T>
+int rfp_ltl(ExecT<T>& ex, int transr, int lower, int n, const T* L, const T* Lbar,
+            ViewT<T> D);
 // Lower triangle of the logical matrix C (RFP): C := alpha (A1 B1 + A2 B2)
 // + beta C with A1, A2 n x k and B1, B2 k x n dense views.
-int rfp_gemm_lower2(Exec& ex, int transr, int lower, int n, float* C, View A1, View B1,
-                    View A2, View B2, int k, float alpha, float beta);
+template <typename T>
+int rfp_gemm_lower2(ExecT<T>& ex, int transr, int lower, int n, T* C, ViewT<T> A1, ViewT<T> B1,
+                    ViewT<T> A2, ViewT<T> B2, int k, Scalar<T> alpha, Scalar<T> beta);
 // L^T X = B for the lower triangle of X only (diagonal included): reads the
 // lower triangle of B and overwrites it with that of X; above the diagonal B
 // may hold anything and is left undefined.  n^3/3 flops instead of n^3.
-int trsm_lt_lowerout(Exec& ex, View L, int n, View B, int math = 0);
+template <typename T>
+int trsm_lt_lowerout(ExecT<T>& ex, ViewT<T> L, int n, ViewT<T> B, int math = 0);
 // Adjoint of the Cholesky factorization.  Given the factor L and the cotangent
 // Lbar of its stored lower triangle (both RFP, same variant), leaves in the
 // view S (n x n, dense, anything may alias nothing) the lower triangle of
@@ -178,17 +210,20 @@ int trsm_lt_lowerout(Exec& ex, View L, int n, View B, int math = 0);
 // L^T Lbar.  The cotangent of the stored triangle of A is then S(p,q) for
 // p > q and S(p,p)/2 on the diagonal.  D is an n x n column-major scratch;
 // S is returned as a view into D.
-int spftrf_backward(Exec& ex, int transr, int lower, int n, const float* L,
-                    const float* Lbar, float* D, int64_t ldd, View* S, int math = 0);
+template <typename T>
+int spftrf_backward(ExecT<T>& ex, int transr, int lower, int n, const T* L,
+                    const T* Lbar, T* D, int64_t ldd, ViewT<T>* S, int math = 0);
 // Y := alpha A X + beta Y for the symmetric matrix A held in the RFP array
 // (any variant); X, Y dense n x m views.  alpha == 0 reads neither A nor X.
-int rfp_symm(Exec& ex, int transr, int lower, int n, const float* A, View X, View Y, int m,
-             float alpha, float beta);
+template <typename T>
+int rfp_symm(ExecT<T>& ex, int transr, int lower, int n, const T* A, ViewT<T> X, ViewT<T> Y, int m,
+             Scalar<T> alpha, Scalar<T> beta);
 // Y := alpha (G_L + G_L^T) X + beta Y where G_L is the stored lower triangle
 // (diagonal included, so the diagonal counts twice) of the RFP array G; X, Y
 // dense n x m views.
-int rfp_symm_dbl(Exec& ex, int transr, int lower, int n, const float* G, View X, View Y,
-                 int m, float alpha, float beta);
+template <typename T>
+int rfp_symm_dbl(ExecT<T>& ex, int transr, int lower, int n, const T* G, ViewT<T> X, ViewT<T> Y,
+                 int m, Scalar<T> alpha, Scalar<T> beta);
 
 }  // namespace plan
 }  // namespace rfp

@@ -11,7 +11,8 @@
 // The first two are one grid-stride pass; the column sums walk 64 x 64 tiles
 // of the three RFP blocks (the tile list of the packing kernels) with the
 // warp along the stored block's contiguous dimension, reduce inside the tile
-// and add one FP64 partial per tile row and column to global memory.
+// and add one exact fixed-point partial per tile row and column to global
+// memory, so every result is independent of scheduling (bitwise repeatable).
 #pragma once
 #include <cstdint>
 
@@ -24,22 +25,23 @@ namespace knorm {
 constexpr int kThreads = 256;
 
 // Device results of one norm / estimator step (read back with one copy).
+// Every reduction is deterministic: fixed-order combines inside a CTA,
+// per-CTA partials summed in a fixed order, exact integer (fixed-point)
+// atomics across CTAs, and order-independent max.
 struct Stats {
   double sum;          // sum a^2 (norms) or sum |x| (estimator)
   double diag;         // sum of squared diagonal elements
   unsigned long long key;  // max |a| bits (norms); (|x| bits << 32) | ~index (argmax)
-  unsigned long long colmax;  // max column sum (FP64 bits, non-negative)
+  unsigned long long colmax;  // max column sum (fixed point, see colsum)
   int mismatch;        // estimator: count of sign(x_i) != isgn_i
   int pad;
   float xj;            // estimator: |x[j]| for the caller's previous index j
   float pad2;
 };
 
+constexpr int kMaxParts = 148 * 8;  // grid cap of the flat passes (per-CTA partials)
+
 __device__ __forceinline__ double warp_sum(double v) {
-  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-__device__ __forceinline__ float warp_sumf(float v) {
   for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
@@ -51,10 +53,10 @@ __device__ __forceinline__ unsigned long long warp_max(unsigned long long v) {
   return v;
 }
 
-// Block-wide sum (double) and max (u64) of per-thread values; thread 0 adds
-// them to the global accumulators.
-__device__ __forceinline__ void block_commit(double s, unsigned long long m, double* gsum,
-                                             unsigned long long* gmax) {
+// Block-wide sum (fixed order) and max of per-thread values; thread 0
+// stores the sum to *part (if given) and max-combines into *gmax.
+__device__ __forceinline__ double block_reduce(double s, unsigned long long m, double* part,
+                                               unsigned long long* gmax) {
   __shared__ double ss[kThreads / 32];
   __shared__ unsigned long long sm[kThreads / 32];
   s = warp_sum(s);
@@ -62,22 +64,24 @@ __device__ __forceinline__ void block_commit(double s, unsigned long long m, dou
   const int w = threadIdx.x / 32, l = threadIdx.x % 32;
   if (l == 0) { ss[w] = s; sm[w] = m; }
   __syncthreads();
+  double t = 0;
   if (threadIdx.x == 0) {
-    double t = 0;
     unsigned long long x = 0;
     for (int i = 0; i < kThreads / 32; ++i) { t += ss[i]; x = sm[i] > x ? sm[i] : x; }
-    if (gsum) atomicAdd(gsum, t);
+    if (part) *part = t;
     if (gmax) atomicMax(gmax, x);
   }
+  return t;
 }
 
 __device__ __forceinline__ unsigned abs_bits(float v) {
   return __float_as_uint(v) & 0x7fffffffu;  // NaN keeps the largest patterns
 }
 
-// sum a^2 and max |a| over the flat array (count elements).
+// sum a^2 (per-CTA partial into part[blockIdx.x]) and max |a| over the flat
+// array (count elements).  Launch with at most kMaxParts CTAs.
 __global__ void __launch_bounds__(kThreads) flat_stats(const float* __restrict__ a, int64_t count,
-                                                       Stats* st) {
+                                                       double* part, Stats* st) {
   double s = 0.0;
   unsigned m = 0;
   const int64_t tid = (int64_t)blockIdx.x * kThreads + threadIdx.x;
@@ -101,31 +105,55 @@ __global__ void __launch_bounds__(kThreads) flat_stats(const float* __restrict__
     s += (double)v * v;
     m = max(m, abs_bits(v));
   }
-  block_commit(s, (unsigned long long)m, &st->sum, &st->key);
+  block_reduce(s, (unsigned long long)m, part + blockIdx.x, &st->key);
 }
 
-// sum of squared diagonal elements.
+// st->sum := part[0] + ... + part[np - 1] in a fixed order (one CTA).
+__global__ void __launch_bounds__(kThreads) sum_parts(const double* __restrict__ part, int np,
+                                                      Stats* st) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < np; i += kThreads) s += part[i];
+  const double t = block_reduce(s, 0ull, nullptr, nullptr);
+  if (threadIdx.x == 0) st->sum = t;
+}
+
+// sum of squared diagonal elements (one CTA, fixed order).
 __global__ void __launch_bounds__(kThreads) diag_sumsq(Geometry g, const float* __restrict__ a,
                                                        Stats* st) {
   double s = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < g.n;
-       i += (int64_t)gridDim.x * kThreads) {
+  for (int64_t i = threadIdx.x; i < g.n; i += kThreads) {
     const float v = a[diag_offset(g, i)];
     s += (double)v * v;
   }
-  block_commit(s, 0ull, &st->diag, nullptr);
+  const double t = block_reduce(s, 0ull, nullptr, nullptr);
+  if (threadIdx.x == 0) st->diag = t;
+}
+
+// Fixed-point exponent of the column sums: every column sum is at most
+// n max|a| < 2^(e_max), so sums scaled by 2^(62 - e_max) fit in 63 bits.
+__device__ __forceinline__ int colsum_shift(const Stats* st, int n) {
+  const float amax = __uint_as_float((unsigned)st->key);
+  if (!(amax > 0.f) || !(amax <= 3.0e38f)) return 0;  // zero, inf or NaN: handled by the caller
+  int e;
+  frexp((double)amax * (double)n, &e);  // amax * n < 2^e
+  return 62 - e;
 }
 
 // Column sums of |A| over the tiles of the RFP blocks (block 32 x 8, one
-// 64 x 64 tile per CTA).  col (n doubles) must start at zero.
+// 64 x 64 tile per CTA) as 64-bit fixed-point integers (scale 2^shift from
+// colsum_shift; the max pass of flat_stats runs first).  Inside a tile every
+// partial is combined in a fixed order; across tiles the integer atomics are
+// exact, so the result does not depend on scheduling.  col (n words) must
+// start at zero.
 __global__ void __launch_bounds__(kpack::TX * kpack::TY) colsum(const kpack::PackArgs args,
                                                                 const float* __restrict__ arf,
-                                                                double* col) {
+                                                                int n, const Stats* st,
+                                                                unsigned long long* col) {
   using namespace kpack;
-  __shared__ float cacc[TS], racc[TS];  // per tile column (q) / row (p)
+  __shared__ double lpart[TY][TS];  // lane-indexed partials of each thread row
+  __shared__ double wpart[TS];      // warp-indexed partials (one owner each)
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int lin = ty * TX + tx;
-  if (lin < TS) { cacc[lin] = 0.f; racc[lin] = 0.f; }
   int t = blockIdx.x, bi = 0;
   while (bi + 1 < args.nblocks && t >= args.b[bi + 1].tile_begin) ++bi;
   const PackBlock& B = args.b[bi];
@@ -138,12 +166,11 @@ __global__ void __launch_bounds__(kpack::TX * kpack::TY) colsum(const kpack::Pac
   // warp along the contiguous dimension: lane index L, warp index W
   const bool qc = (B.cs == 1 || B.cs == -1);
   const int64_t sl = qc ? B.cs : B.rs, sw = qc ? B.rs : B.cs;
-  __syncthreads();
-  float accL[TS / TX] = {0.f, 0.f};
+  double accL[TS / TX] = {0.0, 0.0};
 #pragma unroll
   for (int r = 0; r < TS / TY; ++r) {
     const int w = ty + TY * r;
-    float accW = 0.f;
+    double accW = 0.0;
 #pragma unroll
     for (int h = 0; h < TS / TX; ++h) {
       const int l = tx + TX * h;
@@ -156,33 +183,41 @@ __global__ void __launch_bounds__(kpack::TX * kpack::TY) colsum(const kpack::Pac
       if (qc) { accL[h] += v; accW += vr; }
       else    { accL[h] += vr; accW += v; }
     }
-    accW = warp_sumf(accW);
-    if (tx == 0 && accW != 0.f) atomicAdd(qc ? &racc[w] : &cacc[w], accW);
+    accW = warp_sum(accW);
+    if (tx == 0) wpart[w] = accW;
   }
 #pragma unroll
-  for (int h = 0; h < TS / TX; ++h) {
-    const int l = tx + TX * h;
-    if (accL[h] != 0.f) atomicAdd(qc ? &cacc[l] : &racc[l], accL[h]);
-  }
+  for (int h = 0; h < TS / TX; ++h) lpart[ty][tx + TX * h] = accL[h];
   __syncthreads();
-  if (lin < TS) {
-    if (lin < qcol && cacc[lin] != 0.f) atomicAdd(col + Q0 + lin, (double)cacc[lin]);
-  } else if (lin < 2 * TS) {
-    const int i = lin - TS;
-    if (i < prow && racc[i] != 0.f) atomicAdd(col + P0 + i, (double)racc[i]);
+  const int shift = colsum_shift(st, n);
+  if (lin < 2 * TS) {
+    const int i = lin % TS;
+    const bool lane_side = lin < TS;  // lane-indexed (L) or warp-indexed (W) partial
+    double v;
+    if (lane_side) {
+      v = 0.0;
+#pragma unroll
+      for (int y = 0; y < TY; ++y) v += lpart[y][i];
+    } else {
+      v = wpart[i];
+    }
+    // lane index is q when the warp runs along q, else p
+    const bool is_col = lane_side == qc;
+    const int lim = is_col ? qcol : prow;
+    const int64_t g = (is_col ? Q0 : P0) + i;
+    if (i < lim && v != 0.0)
+      atomicAdd(col + g, (unsigned long long)llrint(ldexp(v, shift)));
   }
 }
 
-// max of n non-negative doubles into st->colmax.
-__global__ void __launch_bounds__(kThreads) max_of(const double* __restrict__ v, int n,
-                                                   Stats* st) {
+// Largest column sum (fixed point) into st->colmax.
+__global__ void __launch_bounds__(kThreads) max_of(const unsigned long long* __restrict__ v,
+                                                   int n, Stats* st) {
   unsigned long long m = 0;
   for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * kThreads) {
-    const unsigned long long b = (unsigned long long)__double_as_longlong(v[i]);
-    m = b > m ? b : m;
-  }
-  block_commit(0.0, m, nullptr, &st->colmax);
+       i += (int64_t)gridDim.x * kThreads)
+    m = v[i] > m ? v[i] : m;
+  block_reduce(0.0, m, nullptr, &st->colmax);
 }
 
 // ---------------------------------------------------------------------------
@@ -220,26 +255,27 @@ __global__ void altsgn(float* x, int n) {
 }
 
 // sum |x| (FP64), first index of max |x|, the number of i with
-// sign(x_i) != isgn_i (isgn may be null) and |x[j]| for the given j.
+// sign(x_i) != isgn_i (zeros match; isgn may be null) and |x[j]| for the
+// given j.  One CTA, fixed-order sums.
 __global__ void __launch_bounds__(kThreads) vstats(const float* __restrict__ x,
                                                    const float* __restrict__ isgn, int n, int j,
                                                    Stats* st) {
   double s = 0.0;
   unsigned long long key = 0;
   int mis = 0;
-  for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * kThreads) {
+  for (int64_t i = threadIdx.x; i < n; i += kThreads) {
     const float v = x[i];
     s += fabs((double)v);
     const unsigned long long k = ((unsigned long long)abs_bits(v) << 32) |
                                  (unsigned long long)(0xffffffffu - (unsigned)i);
     key = k > key ? k : key;
-    if (isgn) mis += ((v >= 0.f ? 1.f : -1.f) != isgn[i]);
+    if (isgn) mis += (v != 0.f && (v > 0.f ? 1.f : -1.f) != isgn[i]);
     if (i == j) st->xj = fabsf(v);
   }
   for (int o = 16; o; o >>= 1) mis += __shfl_xor_sync(0xffffffffu, mis, o);
   if ((threadIdx.x & 31) == 0 && mis) atomicAdd(&st->mismatch, mis);
-  block_commit(s, key, &st->sum, &st->key);
+  const double t = block_reduce(s, key, nullptr, &st->key);
+  if (threadIdx.x == 0) st->sum = t;
 }
 
 }  // namespace knorm

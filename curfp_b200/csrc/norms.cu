@@ -37,12 +37,6 @@ inline bool read_stats(curfpHandle_t h, const Stats* d, Stats* out) {
   return cudaStreamSynchronize(h->stream) == cudaSuccess;
 }
 
-inline double u64_as_double(unsigned long long b) {
-  double d;
-  std::memcpy(&d, &b, sizeof d);
-  return d;
-}
-
 }  // namespace
 
 extern "C" {
@@ -63,45 +57,56 @@ curfpStatus_t curfpSlansf(curfpHandle_t handle, curfpNormType_t norm, curfpOpera
   const int tr = transr == CURFP_OP_T, lower = uplo == CURFP_FILL_MODE_LOWER;
   const rfp::Geometry g = rfp::geometry(n, tr, lower);
   const int64_t nt = (int64_t)n * (n + 1) / 2;
+  using namespace rfp::knorm;
+  // scratch: per-CTA partials (kMaxParts doubles), then the column sums
   void* tail = nullptr;
-  Stats* st = scratch(handle, norm == CURFP_NORM_ONE ? (size_t)n * sizeof(double) : 0, &tail);
+  const size_t parts = (size_t)kMaxParts * sizeof(double);
+  Stats* st = scratch(handle, parts + (norm == CURFP_NORM_ONE ? (size_t)n * 8 : 0), &tail);
   if (!st) return CURFP_STATUS_ALLOC_FAILED;
+  double* part = static_cast<double*>(tail);
   cudaStream_t s = handle->stream;
   if (cudaMemsetAsync(st, 0, sizeof(Stats), s) != cudaSuccess)
     return CURFP_STATUS_EXECUTION_FAILED;
-  using namespace rfp::knorm;
-  if (norm == CURFP_NORM_ONE) {
-    double* col = static_cast<double*>(tail);
-    if (cudaMemsetAsync(col, 0, (size_t)n * sizeof(double), s) != cudaSuccess)
+  const int fb = blocks_for((nt + 3) / 4, kMaxParts);
+  {
+    rfp::ProfScope ps(handle->prof, s, rfp::K_NORM, 0, 4.0 * (double)nt);
+    flat_stats<<<fb, kThreads, 0, s>>>(arf, nt, part, st);  // max |a| (all norms), sum a^2
+    ++handle->launches;
+  }
+  if (norm == CURFP_NORM_FRO) {
+    sum_parts<<<1, kThreads, 0, s>>>(part, fb, st);
+    diag_sumsq<<<1, kThreads, 0, s>>>(g, arf, st);
+    handle->launches += 2;
+  } else if (norm == CURFP_NORM_ONE) {
+    auto* col = reinterpret_cast<unsigned long long*>(static_cast<char*>(tail) + parts);
+    if (cudaMemsetAsync(col, 0, (size_t)n * 8, s) != cudaSuccess)
       return CURFP_STATUS_EXECUTION_FAILED;
     rfp::kpack::PackArgs a{};
     const int tiles = rfp::kpack::pack_blocks(g, &a);
     rfp::ProfScope ps(handle->prof, s, rfp::K_NORM, 0, 4.0 * (double)nt + 16.0 * n);
-    colsum<<<tiles, dim3(rfp::kpack::TX, rfp::kpack::TY), 0, s>>>(a, arf, col);
+    colsum<<<tiles, dim3(rfp::kpack::TX, rfp::kpack::TY), 0, s>>>(a, arf, n, st, col);
     max_of<<<blocks_for(n, kGridCap), kThreads, 0, s>>>(col, n, st);
     handle->launches += 2;
-  } else {
-    rfp::ProfScope ps(handle->prof, s, rfp::K_NORM, 0, 4.0 * (double)nt);
-    flat_stats<<<blocks_for((nt + 3) / 4, kGridCap), kThreads, 0, s>>>(arf, nt, st);
-    ++handle->launches;
-    if (norm == CURFP_NORM_FRO) {
-      diag_sumsq<<<blocks_for(n, kGridCap), kThreads, 0, s>>>(g, arf, st);
-      ++handle->launches;
-    }
   }
   if (cudaGetLastError() != cudaSuccess) return CURFP_STATUS_EXECUTION_FAILED;
   Stats hs;
   if (!read_stats(handle, st, &hs)) return CURFP_STATUS_EXECUTION_FAILED;
+  const unsigned mb = (unsigned)hs.key;
+  float amax;
+  std::memcpy(&amax, &mb, sizeof amax);
   if (norm == CURFP_NORM_MAX) {
-    const unsigned b = (unsigned)hs.key;
-    float v;
-    std::memcpy(&v, &b, sizeof v);
-    *result = v;
+    *result = amax;
   } else if (norm == CURFP_NORM_FRO) {
     const double f2 = 2.0 * hs.sum - hs.diag;
     *result = f2 > 0.0 ? (float)std::sqrt(f2) : 0.0f;
+    if (!(amax <= 3.0e38f)) *result = amax;  // inf or NaN element
+  } else if (!(amax > 0.0f) || !(amax <= 3.0e38f)) {
+    *result = amax;  // zero matrix (0), inf or NaN element
   } else {
-    *result = (float)u64_as_double(hs.colmax);
+    // the fixed-point scale of colsum_shift
+    int e;
+    std::frexp((double)amax * (double)n, &e);
+    *result = (float)std::ldexp((double)hs.colmax, -(62 - e));
   }
   return CURFP_STATUS_SUCCESS;
 }
@@ -143,7 +148,7 @@ curfpStatus_t curfpSpfcon(curfpHandle_t handle, curfpOperation_t transr, curfpFi
   auto stats = [&](const float* sg, int j) -> bool {
     if (cudaMemsetAsync(st, 0, sizeof(Stats), s) != cudaSuccess) return false;
     rfp::ProfScope ps(handle->prof, s, rfp::K_NORM, 0, 8.0 * n);
-    vstats<<<blocks_for(n, kGridCap), kThreads, 0, s>>>(x, sg, n, j, st);
+    vstats<<<1, kThreads, 0, s>>>(x, sg, n, j, st);
     ++handle->launches;
     return cudaGetLastError() == cudaSuccess && read_stats(handle, st, &hs);
   };
