@@ -70,7 +70,8 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     if LIB.exists() and not force and LIB.stat().st_mtime >= max(o.stat().st_mtime for o in objs):
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", str(tmp)] + [str(o) for o in objs] + ["-lcuda"]
+    cmd = ([nvcc()] + ARCH + ["-shared", "-o", str(tmp)] + [str(o) for o in objs] +
+           ["-lcuda", "-Xlinker", "--no-undefined"])  # an unresolved symbol fails the build
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

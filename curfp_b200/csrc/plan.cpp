@@ -22,9 +22,10 @@ inline int split(int n, int blk) {
   return n1;
 }
 
-inline GemmProb gemm_prob(View A, View B, View C, int m, int n, int k,
-                          float alpha, float beta, int math) {
-  GemmProb p{};
+template <typename T>
+inline GemmProbT<T> gemm_prob(ViewT<T> A, ViewT<T> B, ViewT<T> C, int m, int n, int k,
+                              Scalar<T> alpha, Scalar<T> beta, int math) {
+  GemmProbT<T> p{};
   p.A = A; p.B = B; p.C = C;
   p.A2 = A; p.B2 = B;
   p.m = m; p.n = n; p.k = k; p.k2 = 0;
@@ -35,13 +36,14 @@ inline GemmProb gemm_prob(View A, View B, View C, int m, int n, int k,
   return p;
 }
 
-int trsm_rec(Exec& ex, View L, int n, View B, int m, float alpha,
-             const float* W, int blk0, int math) {
+template <typename T>
+int trsm_rec(ExecT<T>& ex, ViewT<T> L, int n, ViewT<T> B, int m, Scalar<T> alpha,
+             const T* W, int blk0, int math) {
   if (n <= 0 || m <= 0) return 0;
-  const float* Wb = W + (int64_t)blk0 * kInvStride;
+  const T* Wb = W + (int64_t)blk0 * kInvStride;
   if (n <= kTrsmLeaf) {
-    View Wv{const_cast<float*>(Wb), 1, kTrsmLeaf};
-    GemmProb p = gemm_prob(Wv, B, B, n, m, n, alpha, 0.0f, 0);
+    ViewT<T> Wv{const_cast<T*>(Wb), 1, kTrsmLeaf};
+    GemmProbT<T> p = gemm_prob(Wv, B, B, n, m, n, alpha, 0.0f, 0);
     p.inplace = 1;
     return ex.gemm(&p, 1);
   }
@@ -55,7 +57,7 @@ int trsm_rec(Exec& ex, View L, int n, View B, int m, float alpha,
   int n1 = split(n, kTrsmLeaf), n2 = n - n1;
   int rc = trsm_rec(ex, L, n1, B, m, alpha, W, blk0, math);
   if (rc) return rc;
-  GemmProb p = gemm_prob(sub(L, n1, 0), B, sub(B, n1, 0), n2, m, n1, -1.0f,
+  GemmProbT<T> p = gemm_prob(sub(L, n1, 0), B, sub(B, n1, 0), n2, m, n1, -1.0f,
                          alpha, math);
   if ((rc = ex.gemm(&p, 1))) return rc;
   return trsm_rec(ex, sub(L, n1, n1), n2, sub(B, n1, 0), m, 1.0f, W,
@@ -64,10 +66,11 @@ int trsm_rec(Exec& ex, View L, int n, View B, int m, float alpha,
 
 }  // namespace
 
-int trsm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math) {
+template <typename T>
+int trsm_lln(ExecT<T>& ex, ViewT<T> L, int n, ViewT<T> B, int m, Scalar<T> alpha, int math) {
   if (n <= 0 || m <= 0) return 0;
   int nblk = (n + kTrsmLeaf - 1) / kTrsmLeaf;
-  float* W = ex.workspace((size_t)nblk * kInvStride);
+  T* W = ex.workspace((size_t)nblk * kInvStride);
   if (!W) return 2;
   int rc = ex.trtri_blocks(L, n, kTrsmLeaf, W);
   if (rc) return rc;
@@ -80,25 +83,27 @@ int trsm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math) {
   return trsm_rec(ex, L, n, B, m, alpha, W, 0, math);
 }
 
-int trsm(Exec& ex, int left, int lower, int trans, View T, View B, int rows,
-         int cols, float alpha, int math) {
+template <typename T>
+int trsm(ExecT<T>& ex, int left, int lower, int trans, ViewT<T> Tm, ViewT<T> B, int rows,
+         int cols, Scalar<T> alpha, int math) {
   if (!left) {  // X op(T) = B  <=>  op(T)^T X^T = B^T
     B = tr(B);
     int t = rows; rows = cols; cols = t;
     trans = !trans;
   }
-  View E = trans ? tr(T) : T;
+  ViewT<T> E = trans ? tr(Tm) : Tm;
   int e_lower = lower ^ trans;
   if (e_lower) return trsm_lln(ex, E, rows, B, cols, alpha, math);
   return trsm_lln(ex, rev(E, rows, rows), rows, rev_rows(B, rows), cols,
                   alpha, math);
 }
 
-int trmm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math) {
+template <typename T>
+int trmm_lln(ExecT<T>& ex, ViewT<T> L, int n, ViewT<T> B, int m, Scalar<T> alpha, int math) {
   if (n <= 0 || m <= 0) return 0;
   int leaf = kTrmmLeaf < ex.inplace_rows() ? kTrmmLeaf : ex.inplace_rows();
   if (n <= leaf) {
-    GemmProb p = gemm_prob(L, B, B, n, m, n, alpha, 0.0f, 0);
+    GemmProbT<T> p = gemm_prob(L, B, B, n, m, n, alpha, 0.0f, 0);
     p.a_tri = 1;
     p.inplace = 1;
     return ex.gemm(&p, 1);
@@ -106,62 +111,66 @@ int trmm_lln(Exec& ex, View L, int n, View B, int m, float alpha, int math) {
   int n1 = split(n, leaf), n2 = n - n1;
   int rc = trmm_lln(ex, sub(L, n1, n1), n2, sub(B, n1, 0), m, alpha, math);
   if (rc) return rc;
-  GemmProb p = gemm_prob(sub(L, n1, 0), B, sub(B, n1, 0), n2, m, n1, alpha,
+  GemmProbT<T> p = gemm_prob(sub(L, n1, 0), B, sub(B, n1, 0), n2, m, n1, alpha,
                          1.0f, math);
   if ((rc = ex.gemm(&p, 1))) return rc;
   return trmm_lln(ex, L, n1, B, m, alpha, math);
 }
 
-int trmm(Exec& ex, int left, int lower, int trans, View T, View B, int rows,
-         int cols, float alpha, int math) {
+template <typename T>
+int trmm(ExecT<T>& ex, int left, int lower, int trans, ViewT<T> Tm, ViewT<T> B, int rows,
+         int cols, Scalar<T> alpha, int math) {
   if (!left) {  // B op(T)  <=>  (op(T)^T B^T)^T
     B = tr(B);
     int t = rows; rows = cols; cols = t;
     trans = !trans;
   }
-  View E = trans ? tr(T) : T;
+  ViewT<T> E = trans ? tr(Tm) : Tm;
   int e_lower = lower ^ trans;
   if (e_lower) return trmm_lln(ex, E, rows, B, cols, alpha, math);
   return trmm_lln(ex, rev(E, rows, rows), rows, rev_rows(B, rows), cols,
                   alpha, math);
 }
 
-int potrf_lower(Exec& ex, View A, int n, int info_base, int math) {
+template <typename T>
+int potrf_lower(ExecT<T>& ex, ViewT<T> A, int n, int info_base, int math) {
   if (n <= 0) return 0;
   if (n <= kPotrfTile) return ex.potrf_tile(A, n, info_base);
   int n1 = split(n, kPotrfTile), n2 = n - n1;
   int rc = potrf_lower(ex, A, n1, info_base, math);
   if (rc) return rc;
-  View A21 = sub(A, n1, 0);
+  ViewT<T> A21 = sub(A, n1, 0);
   // A21 := A21 L11^{-T}   <=>   L11 A21^T = A21^T
   if ((rc = trsm_lln(ex, A, n1, tr(A21), n2, 1.0f, math))) return rc;
   // A22 := A22 - A21 A21^T (lower)
-  SharedTask t{0, 0, n2, n2, sub(A, n1, n1), -1.0f, 1.0f, 1};
+  SharedTaskT<T> t{0, 0, n2, n2, sub(A, n1, n1), -1.0f, 1.0f, 1};
   if ((rc = ex.gemm_shared(A21, n2, n1, &t, 1, math))) return rc;
   return potrf_lower(ex, sub(A, n1, n1), n2, info_base + n1, math);
 }
 
-int trtri_lower(Exec& ex, View L, int n, int math) {
+template <typename T>
+int trtri_lower(ExecT<T>& ex, ViewT<T> L, int n, int math) {
   if (n <= 0) return 0;
   if (n <= kTriTile) return ex.trtri_tile(L, n);
   int n1 = split(n, kTriTile), n2 = n - n1;
   int rc = trtri_lower(ex, L, n1, math);
   if (rc) return rc;
   if ((rc = trtri_lower(ex, sub(L, n1, n1), n2, math))) return rc;
-  View L21 = sub(L, n1, 0);
+  ViewT<T> L21 = sub(L, n1, 0);
   // L21 := -inv(L22) L21 inv(L11)
   if ((rc = trmm(ex, 0, 1, 0, L, L21, n2, n1, 1.0f, math))) return rc;
   return trmm(ex, 1, 1, 0, sub(L, n1, n1), L21, n2, n1, -1.0f, math);
 }
 
-int lauum_lower(Exec& ex, View L, int n, int math) {
+template <typename T>
+int lauum_lower(ExecT<T>& ex, ViewT<T> L, int n, int math) {
   if (n <= 0) return 0;
   if (n <= kTriTile) return ex.lauum_tile(L, n);
   int n1 = split(n, kTriTile), n2 = n - n1;
-  View L21 = sub(L, n1, 0);
+  ViewT<T> L21 = sub(L, n1, 0);
   int rc = lauum_lower(ex, L, n1, math);
   if (rc) return rc;
-  GemmProb p = gemm_prob(tr(L21), L21, L, n1, n1, n2, 1.0f, 1.0f, math);
+  GemmProbT<T> p = gemm_prob(tr(L21), L21, L, n1, n1, n2, 1.0f, 1.0f, math);
   p.c_lower = 1;
   if ((rc = ex.gemm(&p, 1))) return rc;
   if ((rc = trmm(ex, 1, 1, 1, sub(L, n1, n1), L21, n2, n1, 1.0f, math)))
@@ -173,46 +182,48 @@ int lauum_lower(Exec& ex, View L, int n, int math) {
 // RFP routines
 // ---------------------------------------------------------------------------
 
-int ssfrk(Exec& ex, int transr, int lower, int trans, int n, int k,
-          float alpha, const float* A, int lda, float beta, float* C,
+template <typename T>
+int ssfrk(ExecT<T>& ex, int transr, int lower, int trans, int n, int k,
+          Scalar<T> alpha, const T* A, int lda, Scalar<T> beta, T* C,
           int math) {
   Geometry g = geometry(n, transr, lower);
   // op(A) is n x k.  trans = N: A is n x k column-major; trans = T: A is
   // k x n column-major and op(A) = A^T.
-  View opA = trans ? View{const_cast<float*>(A), lda, 1}
-                   : View{const_cast<float*>(A), 1, lda};
+  ViewT<T> opA = trans ? ViewT<T>{const_cast<T*>(A), lda, 1}
+                   : ViewT<T>{const_cast<T*>(A), 1, lda};
   if (alpha == 0.0f) k = 0;  // C := beta*C; A is not read
-  View C11 = block_view(C, g.b11), C21 = block_view(C, g.b21),
+  ViewT<T> C11 = block_view(C, g.b11), C21 = block_view(C, g.b21),
        C22 = block_view(C, g.b22);
-  SharedTask t[3];
+  SharedTaskT<T> t[3];
   int cnt = 0;
-  if (g.n1 > 0) t[cnt++] = SharedTask{0, 0, g.n1, g.n1, C11, alpha, beta, 1};
+  if (g.n1 > 0) t[cnt++] = SharedTaskT<T>{0, 0, g.n1, g.n1, C11, alpha, beta, 1};
   if (g.n1 > 0 && g.n2 > 0)
-    t[cnt++] = SharedTask{g.n1, 0, g.n2, g.n1, C21, alpha, beta, 0};
-  if (g.n2 > 0) t[cnt++] = SharedTask{g.n1, g.n1, g.n2, g.n2, C22, alpha, beta, 1};
+    t[cnt++] = SharedTaskT<T>{g.n1, 0, g.n2, g.n1, C21, alpha, beta, 0};
+  if (g.n2 > 0) t[cnt++] = SharedTaskT<T>{g.n1, g.n1, g.n2, g.n2, C22, alpha, beta, 1};
   return ex.gemm_shared(opA, n, k, t, cnt, math);
 }
 
-int ssfr2k(Exec& ex, int transr, int lower, int trans, int n, int k,
-           float alpha, const float* A, int lda, const float* B, int ldb,
-           float beta, float* C) {
+template <typename T>
+int ssfr2k(ExecT<T>& ex, int transr, int lower, int trans, int n, int k,
+           Scalar<T> alpha, const T* A, int lda, const T* B, int ldb,
+           Scalar<T> beta, T* C) {
   Geometry g = geometry(n, transr, lower);
-  View opA = trans ? View{const_cast<float*>(A), lda, 1}
-                   : View{const_cast<float*>(A), 1, lda};
-  View opB = trans ? View{const_cast<float*>(B), ldb, 1}
-                   : View{const_cast<float*>(B), 1, ldb};
+  ViewT<T> opA = trans ? ViewT<T>{const_cast<T*>(A), lda, 1}
+                   : ViewT<T>{const_cast<T*>(A), 1, lda};
+  ViewT<T> opB = trans ? ViewT<T>{const_cast<T*>(B), ldb, 1}
+                   : ViewT<T>{const_cast<T*>(B), 1, ldb};
   if (alpha == 0.0f) k = 0;
-  View Ab[2] = {opA, sub(opA, g.n1, 0)};
-  View Bb[2] = {opB, sub(opB, g.n1, 0)};
-  View Cb[3] = {block_view(C, g.b11), block_view(C, g.b21),
+  ViewT<T> Ab[2] = {opA, sub(opA, g.n1, 0)};
+  ViewT<T> Bb[2] = {opB, sub(opB, g.n1, 0)};
+  ViewT<T> Cb[3] = {block_view(C, g.b11), block_view(C, g.b21),
                 block_view(C, g.b22)};
   const int bi[3] = {0, 1, 1}, bj[3] = {0, 0, 1};
   const int dm[3] = {g.n1, g.n2, g.n2}, dn[3] = {g.n1, g.n1, g.n2};
-  GemmProb p[3];
+  GemmProbT<T> p[3];
   int cnt = 0;
   for (int b = 0; b < 3; ++b) {
     if (dm[b] <= 0 || dn[b] <= 0) continue;
-    GemmProb q = gemm_prob(Ab[bi[b]], tr(Bb[bj[b]]), Cb[b], dm[b], dn[b], k,
+    GemmProbT<T> q = gemm_prob(Ab[bi[b]], tr(Bb[bj[b]]), Cb[b], dm[b], dn[b], k,
                            alpha, beta, 0);
     q.A2 = Bb[bi[b]];
     q.B2 = tr(Ab[bj[b]]);
@@ -223,49 +234,52 @@ int ssfr2k(Exec& ex, int transr, int lower, int trans, int n, int k,
   return ex.gemm(p, cnt);
 }
 
-int spftrf(Exec& ex, int transr, int lower, int n, float* A, int math) {
+template <typename T>
+int spftrf(ExecT<T>& ex, int transr, int lower, int n, T* A, int math) {
   Geometry g = geometry(n, transr, lower);
-  View V11 = block_view(A, g.b11), V21 = block_view(A, g.b21),
+  ViewT<T> V11 = block_view(A, g.b11), V21 = block_view(A, g.b21),
        V22 = block_view(A, g.b22);
   int rc = potrf_lower(ex, V11, g.n1, 0, math);
   if (rc) return rc;
   if (g.n2 == 0) return 0;
   if (g.n1 > 0) {
     if ((rc = trsm_lln(ex, V11, g.n1, tr(V21), g.n2, 1.0f, math))) return rc;
-    SharedTask t{0, 0, g.n2, g.n2, V22, -1.0f, 1.0f, 1};
+    SharedTaskT<T> t{0, 0, g.n2, g.n2, V22, -1.0f, 1.0f, 1};
     if ((rc = ex.gemm_shared(V21, g.n2, g.n1, &t, 1, math))) return rc;
   }
   return potrf_lower(ex, V22, g.n2, g.n1, math);
 }
 
-int spftrs(Exec& ex, int transr, int lower, int n, int nrhs, const float* A,
-           float* B, int ldb, int math) {
+template <typename T>
+int spftrs(ExecT<T>& ex, int transr, int lower, int n, int nrhs, const T* A,
+           T* B, int ldb, int math) {
   Geometry g = geometry(n, transr, lower);
-  float* Af = const_cast<float*>(A);
-  View V11 = block_view(Af, g.b11), V21 = block_view(Af, g.b21),
+  T* Af = const_cast<T*>(A);
+  ViewT<T> V11 = block_view(Af, g.b11), V21 = block_view(Af, g.b21),
        V22 = block_view(Af, g.b22);
-  View B1{B, 1, ldb};
-  View B2 = sub(B1, g.n1, 0);
+  ViewT<T> B1{B, 1, ldb};
+  ViewT<T> B2 = sub(B1, g.n1, 0);
   int rc;
   // Forward: L Y = B.
   if ((rc = trsm_lln(ex, V11, g.n1, B1, nrhs, 1.0f, math))) return rc;
   if (g.n1 > 0 && g.n2 > 0) {
-    GemmProb p = gemm_prob(V21, B1, B2, g.n2, nrhs, g.n1, -1.0f, 1.0f, math);
+    GemmProbT<T> p = gemm_prob(V21, B1, B2, g.n2, nrhs, g.n1, -1.0f, 1.0f, math);
     if ((rc = ex.gemm(&p, 1))) return rc;
   }
   if ((rc = trsm_lln(ex, V22, g.n2, B2, nrhs, 1.0f, math))) return rc;
   // Backward: L^T X = Y.
   if ((rc = trsm(ex, 1, 1, 1, V22, B2, g.n2, nrhs, 1.0f, math))) return rc;
   if (g.n1 > 0 && g.n2 > 0) {
-    GemmProb p = gemm_prob(tr(V21), B2, B1, g.n1, nrhs, g.n2, -1.0f, 1.0f, math);
+    GemmProbT<T> p = gemm_prob(tr(V21), B2, B1, g.n1, nrhs, g.n2, -1.0f, 1.0f, math);
     if ((rc = ex.gemm(&p, 1))) return rc;
   }
   return trsm(ex, 1, 1, 1, V11, B1, g.n1, nrhs, 1.0f, math);
 }
 
-int rfp_trtri(Exec& ex, int transr, int lower, int n, float* A, int math) {
+template <typename T>
+int rfp_trtri(ExecT<T>& ex, int transr, int lower, int n, T* A, int math) {
   Geometry g = geometry(n, transr, lower);
-  View V11 = block_view(A, g.b11), V21 = block_view(A, g.b21),
+  ViewT<T> V11 = block_view(A, g.b11), V21 = block_view(A, g.b21),
        V22 = block_view(A, g.b22);
   int rc;
   // inv(L) = [M11 0; -M22 L21 M11  M22]
@@ -278,9 +292,10 @@ int rfp_trtri(Exec& ex, int transr, int lower, int n, float* A, int math) {
   return 0;
 }
 
-int spftri(Exec& ex, int transr, int lower, int n, float* A) {
+template <typename T>
+int spftri(ExecT<T>& ex, int transr, int lower, int n, T* A) {
   Geometry g = geometry(n, transr, lower);
-  View V11 = block_view(A, g.b11), V21 = block_view(A, g.b21),
+  ViewT<T> V11 = block_view(A, g.b11), V21 = block_view(A, g.b21),
        V22 = block_view(A, g.b22);
   int rc;
   if ((rc = rfp_trtri(ex, transr, lower, n, A, 0))) return rc;
@@ -288,7 +303,7 @@ int spftri(Exec& ex, int transr, int lower, int n, float* A) {
   //                  (22) = M22^T M22
   if ((rc = lauum_lower(ex, V11, g.n1))) return rc;
   if (g.n1 > 0 && g.n2 > 0) {
-    GemmProb p = gemm_prob(tr(V21), V21, V11, g.n1, g.n1, g.n2, 1.0f, 1.0f, 0);
+    GemmProbT<T> p = gemm_prob(tr(V21), V21, V11, g.n1, g.n1, g.n2, 1.0f, 1.0f, 0);
     p.c_lower = 1;
     if ((rc = ex.gemm(&p, 1))) return rc;
     if ((rc = trmm(ex, 1, 1, 1, V22, V21, g.n2, g.n1, 1.0f))) return rc;
@@ -301,14 +316,16 @@ int spftri(Exec& ex, int transr, int lower, int n, float* A) {
 // ---------------------------------------------------------------------------
 
 namespace {
+template <typename T>
 struct Blocks {
   Geometry g;
-  View V11, V21, V22;
+  ViewT<T> V11, V21, V22;
 };
-inline Blocks blocks(int transr, int lower, int n, const float* A) {
-  Blocks b;
+template <typename T>
+inline Blocks<T> blocks(int transr, int lower, int n, const T* A) {
+  Blocks<T> b;
   b.g = geometry(n, transr, lower);
-  float* p = const_cast<float*>(A);
+  T* p = const_cast<T*>(A);
   b.V11 = block_view(p, b.g.b11);
   b.V21 = block_view(p, b.g.b21);
   b.V22 = block_view(p, b.g.b22);
@@ -316,53 +333,56 @@ inline Blocks blocks(int transr, int lower, int n, const float* A) {
 }
 }  // namespace
 
-int rfp_trsm(Exec& ex, int transr, int lower, int n, const float* L, int trans, View B,
-             int m, float alpha, int math) {
-  Blocks b = blocks(transr, lower, n, L);
+template <typename T>
+int rfp_trsm(ExecT<T>& ex, int transr, int lower, int n, const T* L, int trans, ViewT<T> B,
+             int m, Scalar<T> alpha, int math) {
+  Blocks<T> b = blocks(transr, lower, n, L);
   const int n1 = b.g.n1, n2 = b.g.n2;
-  View B1 = B, B2 = sub(B, n1, 0);
+  ViewT<T> B1 = B, B2 = sub(B, n1, 0);
   int rc;
   if (!trans) {
     if ((rc = trsm_lln(ex, b.V11, n1, B1, m, alpha, math))) return rc;
     if (n1 > 0 && n2 > 0) {
-      GemmProb p = gemm_prob(b.V21, B1, B2, n2, m, n1, -1.0f, alpha, math);
+      GemmProbT<T> p = gemm_prob(b.V21, B1, B2, n2, m, n1, -1.0f, alpha, math);
       if ((rc = ex.gemm(&p, 1))) return rc;
     }
     return trsm_lln(ex, b.V22, n2, B2, m, n1 > 0 ? 1.0f : alpha, math);
   }
   if ((rc = trsm(ex, 1, 1, 1, b.V22, B2, n2, m, alpha, math))) return rc;
   if (n1 > 0 && n2 > 0) {
-    GemmProb p = gemm_prob(tr(b.V21), B2, B1, n1, m, n2, -1.0f, alpha, math);
+    GemmProbT<T> p = gemm_prob(tr(b.V21), B2, B1, n1, m, n2, -1.0f, alpha, math);
     if ((rc = ex.gemm(&p, 1))) return rc;
   }
   return trsm(ex, 1, 1, 1, b.V11, B1, n1, m, n2 > 0 ? 1.0f : alpha, math);
 }
 
-int rfp_trmm_t(Exec& ex, int transr, int lower, int n, const float* L, View B, int m) {
-  Blocks b = blocks(transr, lower, n, L);
+template <typename T>
+int rfp_trmm_t(ExecT<T>& ex, int transr, int lower, int n, const T* L, ViewT<T> B, int m) {
+  Blocks<T> b = blocks(transr, lower, n, L);
   const int n1 = b.g.n1, n2 = b.g.n2;
-  View B1 = B, B2 = sub(B, n1, 0);
+  ViewT<T> B1 = B, B2 = sub(B, n1, 0);
   int rc;
   // (L^T B)_1 = L11^T B1 + L21^T B2 ; (L^T B)_2 = L22^T B2
   if ((rc = trmm(ex, 1, 1, 1, b.V11, B1, n1, m, 1.0f))) return rc;
   if (n1 > 0 && n2 > 0) {
-    GemmProb p = gemm_prob(tr(b.V21), B2, B1, n1, m, n2, 1.0f, 1.0f, 0);
+    GemmProbT<T> p = gemm_prob(tr(b.V21), B2, B1, n1, m, n2, 1.0f, 1.0f, 0);
     if ((rc = ex.gemm(&p, 1))) return rc;
   }
   return trmm(ex, 1, 1, 1, b.V22, B2, n2, m, 1.0f);
 }
 
-int rfp_ltl(Exec& ex, int transr, int lower, int n, const float* L, const float* Lbar,
-            View D) {
-  Blocks a = blocks(transr, lower, n, L), c = blocks(transr, lower, n, Lbar);
+template <typename T>
+int rfp_ltl(ExecT<T>& ex, int transr, int lower, int n, const T* L, const T* Lbar,
+            ViewT<T> D) {
+  Blocks<T> a = blocks(transr, lower, n, L), c = blocks(transr, lower, n, Lbar);
   const int n1 = a.g.n1, n2 = a.g.n2;
-  GemmProb p[3];
+  GemmProbT<T> p[3];
   int cnt = 0;
   // (L^T Lbar) lower blocks:
   //   11: tril(L11^T Lbar11) + L21^T Lbar21     21: L22^T Lbar21
   //   22: tril(L22^T Lbar22)
   if (n1 > 0) {
-    GemmProb q = gemm_prob(tr(a.V11), c.V11, D, n1, n1, n1, 1.0f, 0.0f, 0);
+    GemmProbT<T> q = gemm_prob(tr(a.V11), c.V11, D, n1, n1, n1, 1.0f, 0.0f, 0);
     q.a_tri = 2;  // L11^T is upper
     q.b_tri = 1;  // Lbar11 is lower
     if (n2 > 0) {
@@ -374,12 +394,12 @@ int rfp_ltl(Exec& ex, int transr, int lower, int n, const float* L, const float*
     p[cnt++] = q;
   }
   if (n1 > 0 && n2 > 0) {
-    GemmProb q = gemm_prob(tr(a.V22), c.V21, sub(D, n1, 0), n2, n1, n2, 1.0f, 0.0f, 0);
+    GemmProbT<T> q = gemm_prob(tr(a.V22), c.V21, sub(D, n1, 0), n2, n1, n2, 1.0f, 0.0f, 0);
     q.a_tri = 2;
     p[cnt++] = q;
   }
   if (n2 > 0) {
-    GemmProb q = gemm_prob(tr(a.V22), c.V22, sub(D, n1, n1), n2, n2, n2, 1.0f, 0.0f, 0);
+    GemmProbT<T> q = gemm_prob(tr(a.V22), c.V22, sub(D, n1, n1), n2, n2, n2, 1.0f, 0.0f, 0);
     q.a_tri = 2;
     q.b_tri = 1;
     q.c_lower = 1;
@@ -388,18 +408,19 @@ int rfp_ltl(Exec& ex, int transr, int lower, int n, const float* L, const float*
   return ex.gemm(p, cnt);
 }
 
-int rfp_gemm_lower2(Exec& ex, int transr, int lower, int n, float* C, View A1, View B1,
-                    View A2, View B2, int k, float alpha, float beta) {
-  Blocks c = blocks(transr, lower, n, C);
+template <typename T>
+int rfp_gemm_lower2(ExecT<T>& ex, int transr, int lower, int n, T* C, ViewT<T> A1, ViewT<T> B1,
+                    ViewT<T> A2, ViewT<T> B2, int k, Scalar<T> alpha, Scalar<T> beta) {
+  Blocks<T> c = blocks(transr, lower, n, C);
   const int n1 = c.g.n1, n2 = c.g.n2;
-  View Cb[3] = {c.V11, c.V21, c.V22};
+  ViewT<T> Cb[3] = {c.V11, c.V21, c.V22};
   const int r0[3] = {0, n1, n1}, c0[3] = {0, 0, n1};
   const int dm[3] = {n1, n2, n2}, dn[3] = {n1, n1, n2};
-  GemmProb p[3];
+  GemmProbT<T> p[3];
   int cnt = 0;
   for (int b = 0; b < 3; ++b) {
     if (dm[b] <= 0 || dn[b] <= 0) continue;
-    GemmProb q = gemm_prob(sub(A1, r0[b], 0), sub(B1, 0, c0[b]), Cb[b], dm[b], dn[b], k,
+    GemmProbT<T> q = gemm_prob(sub(A1, r0[b], 0), sub(B1, 0, c0[b]), Cb[b], dm[b], dn[b], k,
                            alpha, beta, 0);
     q.A2 = sub(A2, r0[b], 0);
     q.B2 = sub(B2, 0, c0[b]);
@@ -410,18 +431,19 @@ int rfp_gemm_lower2(Exec& ex, int transr, int lower, int n, float* C, View A1, V
   return ex.gemm(p, cnt);
 }
 
-int trsm_lt_lowerout(Exec& ex, View L, int n, View B, int math) {
+template <typename T>
+int trsm_lt_lowerout(ExecT<T>& ex, ViewT<T> L, int n, ViewT<T> B, int math) {
   if (n <= 0) return 0;
   if (n <= kWaveLeaf) return trsm(ex, 1, 1, 1, L, B, n, n, 1.0f, math);
   // L = [L11 0; L21 L22]:  L22^T X22 = B22 (lower part), L22^T X21 = B21,
   // L11^T X11 = B11 - L21^T X21 (lower part).
   const int n1 = split(n, kTriTile), n2 = n - n1;
-  View L11 = L, L21 = sub(L, n1, 0), L22 = sub(L, n1, n1);
-  View B11 = B, B21 = sub(B, n1, 0), B22 = sub(B, n1, n1);
+  ViewT<T> L11 = L, L21 = sub(L, n1, 0), L22 = sub(L, n1, n1);
+  ViewT<T> B11 = B, B21 = sub(B, n1, 0), B22 = sub(B, n1, n1);
   int rc;
   if ((rc = trsm_lt_lowerout(ex, L22, n2, B22, math))) return rc;
   if ((rc = trsm(ex, 1, 1, 1, L22, B21, n2, n1, 1.0f, math))) return rc;
-  GemmProb p = gemm_prob(tr(L21), B21, B11, n1, n1, n2, -1.0f, 1.0f, math);
+  GemmProbT<T> p = gemm_prob(tr(L21), B21, B11, n1, n1, n2, -1.0f, 1.0f, math);
   p.c_lower = 1;
   if ((rc = ex.gemm(&p, 1))) return rc;
   return trsm_lt_lowerout(ex, L11, n1, B11, math);
@@ -429,16 +451,17 @@ int trsm_lt_lowerout(Exec& ex, View L, int n, View B, int math) {
 
 namespace {
 // trsm_lt_lowerout with L the logical factor of an RFP array.
-int rfp_trsm_lowerout(Exec& ex, int transr, int lower, int n, const float* L, View B,
+template <typename T>
+int rfp_trsm_lowerout(ExecT<T>& ex, int transr, int lower, int n, const T* L, ViewT<T> B,
                       int math) {
-  Blocks b = blocks(transr, lower, n, L);
+  Blocks<T> b = blocks(transr, lower, n, L);
   const int n1 = b.g.n1, n2 = b.g.n2;
-  View B11 = B, B21 = sub(B, n1, 0), B22 = sub(B, n1, n1);
+  ViewT<T> B11 = B, B21 = sub(B, n1, 0), B22 = sub(B, n1, n1);
   int rc;
   if ((rc = trsm_lt_lowerout(ex, b.V22, n2, B22, math))) return rc;
   if (n1 > 0 && n2 > 0) {
     if ((rc = trsm(ex, 1, 1, 1, b.V22, B21, n2, n1, 1.0f, math))) return rc;
-    GemmProb p = gemm_prob(tr(b.V21), B21, B11, n1, n1, n2, -1.0f, 1.0f, math);
+    GemmProbT<T> p = gemm_prob(tr(b.V21), B21, B11, n1, n1, n2, -1.0f, 1.0f, math);
     p.c_lower = 1;
     if ((rc = ex.gemm(&p, 1))) return rc;
   }
@@ -446,16 +469,17 @@ int rfp_trsm_lowerout(Exec& ex, int transr, int lower, int n, const float* L, Vi
 }
 }  // namespace
 
-int spftrf_backward(Exec& ex, int transr, int lower, int n, const float* L,
-                    const float* Lbar, float* D, int64_t ldd, View* S, int math) {
-  View Dv{D, 1, ldd};
+template <typename T>
+int spftrf_backward(ExecT<T>& ex, int transr, int lower, int n, const T* L,
+                    const T* Lbar, T* D, int64_t ldd, ViewT<T>* S, int math) {
+  ViewT<T> Dv{D, 1, ldd};
   int rc;
   // lower(Q) = lower(L^T Lbar); Q symmetric
   if ((rc = rfp_ltl(ex, transr, lower, n, L, Lbar, Dv))) return rc;
   if ((rc = ex.mirror_lower(Dv, n))) return rc;
   // Z = L^-T Q, then S = L^-T Z^T (= Z L^-1, symmetric): lower part only
   if ((rc = rfp_trsm(ex, transr, lower, n, L, 1, Dv, n, 1.0f, math))) return rc;
-  View St = tr(Dv);
+  ViewT<T> St = tr(Dv);
   if ((rc = rfp_trsm_lowerout(ex, transr, lower, n, L, St, math))) return rc;
   *S = St;
   return 0;
@@ -467,17 +491,18 @@ namespace {
 // the transposed triangles then exclude their diagonal).  The blocks follow
 // the reference's SSYMM + 2 SGEMM split (src/curfp_ssfmm.cpp:150-306):
 //   Y1 = a (G11 sym) X1 + a G21^T X2 + b Y1,  Y2 = a G21 X1 + a (G22 sym) X2 + b Y2
-int symm_blocks(Exec& ex, int transr, int lower, int n, const float* G, View X, View Y,
-                int m, float alpha, float beta, int once) {
-  Blocks g = blocks(transr, lower, n, G);
+template <typename T>
+int symm_blocks(ExecT<T>& ex, int transr, int lower, int n, const T* G, ViewT<T> X, ViewT<T> Y,
+                int m, Scalar<T> alpha, Scalar<T> beta, int once) {
+  Blocks<T> g = blocks(transr, lower, n, G);
   const int n1 = g.g.n1, n2 = g.g.n2;
   const int up = once ? 3 : 2;  // mask of the transposed triangles
-  View X1 = X, X2 = sub(X, n1, 0), Y1 = Y, Y2 = sub(Y, n1, 0);
+  ViewT<T> X1 = X, X2 = sub(X, n1, 0), Y1 = Y, Y2 = sub(Y, n1, 0);
   const bool zero = alpha == 0.0f;  // C := beta C, A and X not read
-  GemmProb p[2];
+  GemmProbT<T> p[2];
   int cnt = 0;
   if (n1 > 0) {
-    GemmProb q = gemm_prob(g.V11, X1, Y1, n1, m, zero ? 0 : n1, alpha, beta, 0);
+    GemmProbT<T> q = gemm_prob(g.V11, X1, Y1, n1, m, zero ? 0 : n1, alpha, beta, 0);
     q.a_tri = 1;
     q.A2 = tr(g.V11);
     q.B2 = X1;
@@ -486,7 +511,7 @@ int symm_blocks(Exec& ex, int transr, int lower, int n, const float* G, View X, 
     p[cnt++] = q;
   }
   if (n2 > 0) {
-    GemmProb q = gemm_prob(g.V21, X1, Y2, n2, m, (zero || n1 == 0) ? 0 : n1, alpha, beta, 0);
+    GemmProbT<T> q = gemm_prob(g.V21, X1, Y2, n2, m, (zero || n1 == 0) ? 0 : n1, alpha, beta, 0);
     q.A2 = g.V22;
     q.B2 = X2;
     q.k2 = zero ? 0 : n2;
@@ -498,11 +523,11 @@ int symm_blocks(Exec& ex, int transr, int lower, int n, const float* G, View X, 
   if (zero) return 0;
   cnt = 0;
   if (n1 > 0 && n2 > 0) {
-    GemmProb q = gemm_prob(tr(g.V21), X2, Y1, n1, m, n2, alpha, 1.0f, 0);
+    GemmProbT<T> q = gemm_prob(tr(g.V21), X2, Y1, n1, m, n2, alpha, 1.0f, 0);
     p[cnt++] = q;
   }
   if (n2 > 0) {
-    GemmProb q = gemm_prob(tr(g.V22), X2, Y2, n2, m, n2, alpha, 1.0f, 0);
+    GemmProbT<T> q = gemm_prob(tr(g.V22), X2, Y2, n2, m, n2, alpha, 1.0f, 0);
     q.a_tri = up;
     p[cnt++] = q;
   }
@@ -510,15 +535,53 @@ int symm_blocks(Exec& ex, int transr, int lower, int n, const float* G, View X, 
 }
 }  // namespace
 
-int rfp_symm(Exec& ex, int transr, int lower, int n, const float* A, View X, View Y, int m,
-             float alpha, float beta) {
+template <typename T>
+int rfp_symm(ExecT<T>& ex, int transr, int lower, int n, const T* A, ViewT<T> X, ViewT<T> Y, int m,
+             Scalar<T> alpha, Scalar<T> beta) {
   return symm_blocks(ex, transr, lower, n, A, X, Y, m, alpha, beta, 1);
 }
 
-int rfp_symm_dbl(Exec& ex, int transr, int lower, int n, const float* G, View X, View Y,
-                 int m, float alpha, float beta) {
+template <typename T>
+int rfp_symm_dbl(ExecT<T>& ex, int transr, int lower, int n, const T* G, ViewT<T> X, ViewT<T> Y,
+                 int m, Scalar<T> alpha, Scalar<T> beta) {
   return symm_blocks(ex, transr, lower, n, G, X, Y, m, alpha, beta, 0);
 }
+
+// The planner is instantiated for the FP32 routines and their FP64 twins.
+#define RFP_PLAN_INSTANTIATE(T)                                                              \
+  template int trsm_lln<T>(ExecT<T>&, ViewT<T>, int, ViewT<T>, int, Scalar<T>, int);          \
+  template int trsm<T>(ExecT<T>&, int, int, int, ViewT<T>, ViewT<T>, int, int, Scalar<T>,     \
+                       int);                                                                 \
+  template int trmm_lln<T>(ExecT<T>&, ViewT<T>, int, ViewT<T>, int, Scalar<T>, int);          \
+  template int trmm<T>(ExecT<T>&, int, int, int, ViewT<T>, ViewT<T>, int, int, Scalar<T>,     \
+                       int);                                                                 \
+  template int potrf_lower<T>(ExecT<T>&, ViewT<T>, int, int, int);                            \
+  template int trtri_lower<T>(ExecT<T>&, ViewT<T>, int, int);                                 \
+  template int lauum_lower<T>(ExecT<T>&, ViewT<T>, int, int);                                 \
+  template int ssfrk<T>(ExecT<T>&, int, int, int, int, int, Scalar<T>, const T*, int,         \
+                        Scalar<T>, T*, int);                                                 \
+  template int ssfr2k<T>(ExecT<T>&, int, int, int, int, int, Scalar<T>, const T*, int,        \
+                         const T*, int, Scalar<T>, T*);                                      \
+  template int spftrf<T>(ExecT<T>&, int, int, int, T*, int);                                  \
+  template int spftrs<T>(ExecT<T>&, int, int, int, int, const T*, T*, int, int);              \
+  template int spftri<T>(ExecT<T>&, int, int, int, T*);                                       \
+  template int rfp_trtri<T>(ExecT<T>&, int, int, int, T*, int);                               \
+  template int rfp_trsm<T>(ExecT<T>&, int, int, int, const T*, int, ViewT<T>, int, Scalar<T>, \
+                           int);                                                             \
+  template int rfp_trmm_t<T>(ExecT<T>&, int, int, int, const T*, ViewT<T>, int);              \
+  template int rfp_ltl<T>(ExecT<T>&, int, int, int, const T*, const T*, ViewT<T>);            \
+  template int rfp_gemm_lower2<T>(ExecT<T>&, int, int, int, T*, ViewT<T>, ViewT<T>, ViewT<T>, \
+                                  ViewT<T>, int, Scalar<T>, Scalar<T>);                      \
+  template int trsm_lt_lowerout<T>(ExecT<T>&, ViewT<T>, int, ViewT<T>, int);                  \
+  template int spftrf_backward<T>(ExecT<T>&, int, int, int, const T*, const T*, T*, int64_t,  \
+                                  ViewT<T>*, int);                                           \
+  template int rfp_symm<T>(ExecT<T>&, int, int, int, const T*, ViewT<T>, ViewT<T>, int,       \
+                           Scalar<T>, Scalar<T>);                                            \
+  template int rfp_symm_dbl<T>(ExecT<T>&, int, int, int, const T*, ViewT<T>, ViewT<T>, int,   \
+                               Scalar<T>, Scalar<T>);
+
+RFP_PLAN_INSTANTIATE(float)
+RFP_PLAN_INSTANTIATE(double)
 
 }  // namespace plan
 }  // namespace rfp
