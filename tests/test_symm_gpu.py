@@ -47,7 +47,7 @@ def test_ssfmm_vs_fp64(curfp, orc, n, m, side, tr, ul):
 @pytest.mark.parametrize("tr,ul", VARIANTS)
 @pytest.mark.parametrize("incx,incy", [(1, 1), (2, 3), (-1, 1), (3, -2)])
 def test_ssfmv_vs_fp64(curfp, orc, n, tr, ul, incx, incy):
-    rng = np.random.default_rng(n + 5 * incx + incy)
+    rng = np.random.default_rng(n + 5 * abs(incx) + abs(incy) + 100)
     nt = n * (n + 1) // 2
     arf = rng.standard_normal(nt).astype(np.float32)
     A = orc.rfp_to_dense_sym(tr, ul, n, arf.astype(np.float64))
