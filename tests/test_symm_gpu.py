@@ -109,7 +109,7 @@ def test_symm_argument_errors(curfp):
 def test_ssfr_ssfr2_vs_fp64(curfp, orc, n, tr, ul, incx, incy):
     """Rank-1 / rank-2 updates of every stored element against FP64: one
     rounding of two FMAs per element (<= 2 ulp of the operand scale)."""
-    rng = np.random.default_rng(n + incy)
+    rng = np.random.default_rng(n + abs(incy) + 7)
     nt = n * (n + 1) // 2
     arf = rng.standard_normal(nt).astype(np.float32)
     xs = rng.standard_normal(n * abs(incx)).astype(np.float32)
