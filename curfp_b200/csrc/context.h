@@ -38,26 +38,31 @@ struct curfpContext {
 
 namespace rfp {
 
-class CudaExec : public Exec {
+// The CUDA executor for FP32 (SIMT and split-BF16 tensor-core contractions)
+// and FP64 (SIMT DFMA) element types.
+template <typename T>
+class CudaExecT : public ExecT<T> {
  public:
-  explicit CudaExec(curfpContext* ctx, const int* abort_flag = nullptr)
+  explicit CudaExecT(curfpContext* ctx, const int* abort_flag = nullptr)
       : ctx_(ctx), abort_(abort_flag) {}
-  int gemm(const GemmProb* p, int count) override;
-  int potrf_tile(View L, int n, int info_base) override;
-  int trtri_blocks(View L, int n, int nb, float* W) override;
-  int trtri_tile(View L, int n) override;
-  int lauum_tile(View L, int n) override;
-  float* workspace(size_t nfloats) override;
+  int gemm(const GemmProbT<T>* p, int count) override;
+  int potrf_tile(ViewT<T> L, int n, int info_base) override;
+  int trtri_blocks(ViewT<T> L, int n, int nb, T* W) override;
+  int trtri_tile(ViewT<T> L, int n) override;
+  int lauum_tile(ViewT<T> L, int n) override;
+  T* workspace(size_t count) override;
   int inplace_rows() const override { return 64; }
-  int gemm_shared(View X, int rows, int k, const SharedTask* t, int count,
+  int gemm_shared(ViewT<T> X, int rows, int k, const SharedTaskT<T>* t, int count,
                   int math) override;
-  int trsm_wave(View L, int n, View B, int m, float alpha, const float* W) override;
-  int mirror_lower(View D, int n) override;
+  int trsm_wave(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const T* W) override;
+  int mirror_lower(ViewT<T> D, int n) override;
 
  protected:
   curfpContext* ctx_;
   const int* abort_;
 };
+using CudaExec = CudaExecT<float>;
+using CudaExecD = CudaExecT<double>;
 
 // Grow a stream-ordered buffer to at least `bytes`; returns nullptr on failure.
 void* grow_buffer(curfpContext* ctx, void** buf, size_t* cur, size_t bytes);

@@ -35,24 +35,24 @@ void* grow_buffer(curfpContext* ctx, void** buf, size_t* cur, size_t bytes) {
   return p;
 }
 
-float* CudaExec::workspace(size_t nfloats) {
-  return static_cast<float*>(
-      grow_buffer(ctx_, &ctx_->ws, &ctx_->ws_bytes, nfloats * sizeof(float)));
+template <typename T>
+T* CudaExecT<T>::workspace(size_t count) {
+  return static_cast<T*>(grow_buffer(ctx_, &ctx_->ws, &ctx_->ws_bytes, count * sizeof(T)));
 }
 
 namespace {
 
-template <int BM, int BN>
-int launch_gemm(const GemmProb* p, int count, const int* abort_flag,
+template <typename T, int BM, int BN>
+int launch_gemm(const GemmProbT<T>* p, int count, const int* abort_flag,
                 curfpContext* ctx) {
   cudaStream_t st = ctx->stream;
   double flops = 0;
-  kgemm::Batch b{};
+  kgemm::Batch<T> b{};
   int tiles = 0, cnt = 0;
   for (int i = 0; i < count; ++i) {
-    const GemmProb& g = p[i];
+    const GemmProbT<T>& g = p[i];
     if (g.m <= 0 || g.n <= 0) continue;
-    kgemm::Prob& q = b.p[cnt];
+    kgemm::Prob<T>& q = b.p[cnt];
     q.A = g.A.p; q.a_rs = g.A.rs; q.a_cs = g.A.cs;
     q.B = g.B.p; q.b_rs = g.B.rs; q.b_cs = g.B.cs;
     q.A2 = g.A2.p; q.a2_rs = g.A2.rs; q.a2_cs = g.A2.cs;
@@ -77,7 +77,7 @@ int launch_gemm(const GemmProb* p, int count, const int* abort_flag,
   b.total_tiles = tiles;
   b.abort_flag = abort_flag;
   ProfScope ps(ctx->prof, st, K_SGEMM, flops, 0);
-  kgemm::sgemm_batch<BM, BN><<<tiles, kgemm::kThreads, 0, st>>>(b);
+  kgemm::sgemm_batch<T, BM, BN><<<tiles, kgemm::kThreads, 0, st>>>(b);
   ++ctx->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
@@ -98,8 +98,15 @@ static void orient(View& A, int& arows, View& B, int& brows, SharedTask& t) {
   t.c_lower = t.c_lower ? 2 : 0;  // 2 = upper mask after transposition
 }
 
-int CudaExec::gemm_shared(View X, int rows, int k, const SharedTask* t, int count,
-                          int math) {
+template <>
+int CudaExecT<double>::gemm_shared(ViewT<double> X, int rows, int k,
+                                   const SharedTaskT<double>* t, int count, int math) {
+  return ExecT<double>::gemm_shared(X, rows, k, t, count, math);  // SIMT FP64 only
+}
+
+template <>
+int CudaExecT<float>::gemm_shared(View X, int rows, int k, const SharedTask* t, int count,
+                                  int math) {
   bool tc = math != 0 && count <= kMaxBatch;
   for (int i = 0; tc && i < count; ++i)
     tc = tc_worthwhile(t[i].m, t[i].n, k);
@@ -114,7 +121,15 @@ int CudaExec::gemm_shared(View X, int rows, int k, const SharedTask* t, int coun
   return tc_contract(ctx_, abort_, X, rows, View{nullptr, 0, 0}, rows, k, tt, count);
 }
 
-int CudaExec::gemm(const GemmProb* p, int count) {
+template <>
+int CudaExecT<double>::gemm(const GemmProbT<double>* p, int count) {
+  if (count <= 0) return 0;
+  if (count > kMaxBatch) return 3;
+  return launch_gemm<double, 64, 64>(p, count, abort_, ctx_);  // 16 accumulators per thread
+}
+
+template <>
+int CudaExecT<float>::gemm(const GemmProb* p, int count) {
   if (count <= 0) return 0;
   if (count > kMaxBatch) return 3;
   if (count == 1 && p[0].math && !p[0].inplace && !p[0].a_tri && !p[0].b_tri && p[0].k2 == 0 &&
@@ -135,82 +150,103 @@ int CudaExec::gemm(const GemmProb* p, int count) {
     if (p[i].inplace && p[i].m > maxm) maxm = p[i].m;
   }
   if (t128 >= 2 * 148 && maxm == 0)
-    return launch_gemm<128, 128>(p, count, abort_, ctx_);
-  return launch_gemm<64, 64>(p, count, abort_, ctx_);
+    return launch_gemm<float, 128, 128>(p, count, abort_, ctx_);
+  return launch_gemm<float, 64, 64>(p, count, abort_, ctx_);
 }
 
-int CudaExec::mirror_lower(View D, int n) {
+namespace {
+// Opt a kernel into more than 48 KB of dynamic shared memory (once per
+// instantiation).
+template <typename K>
+bool smem_attr(K kernel, int bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) ==
+         cudaSuccess;
+}
+}  // namespace
+
+template <typename T>
+int CudaExecT<T>::mirror_lower(ViewT<T> D, int n) {
   if (n <= 1) return 0;
   const int t = (n + ktile::MTS - 1) / ktile::MTS;
-  ProfScope ps(ctx_->prof, ctx_->stream, K_PACK, 0, 4.0 * n * (double)(n - 1));
-  ktile::mirror_lower<<<t * (t + 1) / 2, dim3(ktile::MTS, ktile::MTY), 0, ctx_->stream>>>(D, n);
+  ProfScope ps(ctx_->prof, ctx_->stream, K_PACK, 0, (double)sizeof(T) * n * (double)(n - 1));
+  ktile::mirror_lower<T>
+      <<<t * (t + 1) / 2, dim3(ktile::MTS, ktile::MTY), 0, ctx_->stream>>>(D, n);
   ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
-int CudaExec::potrf_tile(View L, int n, int info_base) {
+template <typename T>
+int CudaExecT<T>::potrf_tile(ViewT<T> L, int n, int info_base) {
   if (n <= 0) return 0;
   ProfScope ps(ctx_->prof, ctx_->stream, K_POTRF, (double)n * n * n / 3.0, 0);
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(ktile::potrf_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             ktile::POTRF_SMEM) != cudaSuccess)
-      return 4;
-    attr = true;
-  }
-  ktile::potrf_tile<<<1, 256, ktile::POTRF_SMEM, ctx_->stream>>>(L, n, info_base, ctx_->d_info);
+  constexpr int smem = ktile::potrf_smem<T>();
+  static const bool attr = smem_attr(ktile::potrf_tile<T>, smem);
+  if (!attr) return 4;
+  ktile::potrf_tile<T><<<1, 256, smem, ctx_->stream>>>(L, n, info_base, ctx_->d_info);
   ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
-int CudaExec::trtri_blocks(View L, int n, int nb, float* W) {
+template <typename T>
+int CudaExecT<T>::trtri_blocks(ViewT<T> L, int n, int nb, T* W) {
   if (n <= 0) return 0;
   if (nb != ktile::T) return 3;
   int nblk = (n + nb - 1) / nb;
   ProfScope ps(ctx_->prof, ctx_->stream, K_TRTRI, (double)n * nb * nb / 3.0, 0);
-  ktile::trtri_blocks<<<nblk, ktile::TRTRI_THREADS, 0, ctx_->stream>>>(L, n, W, abort_);
+  constexpr int smem = ktile::trtri_smem<T>();
+  static const bool attr = smem_attr(ktile::trtri_blocks<T>, smem);
+  if (!attr) return 4;
+  ktile::trtri_blocks<T>
+      <<<nblk, ktile::TRTRI_THREADS, smem, ctx_->stream>>>(L, n, W, abort_);
   ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
-int CudaExec::trtri_tile(View L, int n) {
+template <typename T>
+int CudaExecT<T>::trtri_tile(ViewT<T> L, int n) {
   if (n <= 0) return 0;
   if (n > ktile::T) return 3;
   ProfScope ps(ctx_->prof, ctx_->stream, K_TRTRI, (double)n * n * n / 3.0, 0);
-  ktile::trtri_blocks<<<1, ktile::TRTRI_THREADS, 0, ctx_->stream>>>(L, n, nullptr, abort_);
+  constexpr int smem = ktile::trtri_smem<T>();
+  static const bool attr = smem_attr(ktile::trtri_blocks<T>, smem);
+  if (!attr) return 4;
+  ktile::trtri_blocks<T>
+      <<<1, ktile::TRTRI_THREADS, smem, ctx_->stream>>>(L, n, nullptr, abort_);
   ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
-int CudaExec::lauum_tile(View L, int n) {
+template <typename T>
+int CudaExecT<T>::lauum_tile(ViewT<T> L, int n) {
   if (n <= 0) return 0;
   if (n > ktile::T) return 3;
   ProfScope ps(ctx_->prof, ctx_->stream, K_LAUUM, (double)n * n * n / 3.0, 0);
-  ktile::lauum_tile<<<1, 256, 0, ctx_->stream>>>(L, n);
+  ktile::lauum_tile<T><<<1, 256, 0, ctx_->stream>>>(L, n);
   ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
-int CudaExec::trsm_wave(View L, int n, View B, int m, float alpha, const float* W) {
+template <typename T>
+int CudaExecT<T>::trsm_wave(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const T* W) {
   if (n <= 0 || m <= 0) return 0;
   const int nblk = (n + ktrsv::NB - 1) / ktrsv::NB, nchunk = (m + ktrsv::NB - 1) / ktrsv::NB;
   const size_t words = 1 + (size_t)nblk * nchunk;
   int* sync = static_cast<int*>(grow_buffer(ctx_, &ctx_->tsv, &ctx_->tsv_bytes, words * 4));
   if (!sync) return 2;
   if (cudaMemsetAsync(sync, 0, words * 4, ctx_->stream) != cudaSuccess) return 4;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(ktrsv::trsm_wave, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             ktrsv::SMEM) != cudaSuccess)
-      return 4;
-    attr = true;
-  }
-  ProfScope ps(ctx_->prof, ctx_->stream, K_TRSV, (double)n * n * m, (double)n * n * 2.0);
-  ktrsv::trsm_wave<<<nblk * nchunk, 256, ktrsv::SMEM, ctx_->stream>>>(L, n, B, m, alpha, W, sync,
-                                                                     ctx_->d_info + 1, abort_);
+  constexpr int smem = ktrsv::smem_bytes<T>();
+  static const bool attr = smem_attr(ktrsv::trsm_wave<T>, smem);
+  if (!attr) return 4;
+  ProfScope ps(ctx_->prof, ctx_->stream, K_TRSV, (double)n * n * m,
+               (double)n * n * sizeof(T) / 2.0);
+  ktrsv::trsm_wave<T><<<nblk * nchunk, 256, smem, ctx_->stream>>>(L, n, B, m, alpha, W, sync,
+                                                                 ctx_->d_info + 1, abort_);
   ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
+
+template class CudaExecT<float>;
+template class CudaExecT<double>;
 
 int launch_trsm_wave_fixed(curfpContext* ctx, const int* abort_flag, View L, int n, View B,
                            int m, float alpha, const float* W, int* sync, size_t sync_words) {
@@ -219,12 +255,12 @@ int launch_trsm_wave_fixed(curfpContext* ctx, const int* abort_flag, View L, int
   const size_t words = 1 + (size_t)nblk * nchunk;
   if (words > sync_words) return 3;
   if (cudaMemsetAsync(sync, 0, words * 4, ctx->stream) != cudaSuccess) return 4;
-  if (cudaFuncSetAttribute(ktrsv::trsm_wave, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(ktrsv::trsm_wave<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            ktrsv::SMEM) != cudaSuccess)
     return 4;
   ProfScope ps(ctx->prof, ctx->stream, K_TRSV, (double)n * n * m, (double)n * n * 2.0);
-  ktrsv::trsm_wave<<<nblk * nchunk, 256, ktrsv::SMEM, ctx->stream>>>(L, n, B, m, alpha, W, sync,
-                                                                    ctx->d_info + 1, abort_flag);
+  ktrsv::trsm_wave<float><<<nblk * nchunk, 256, ktrsv::SMEM, ctx->stream>>>(
+      L, n, B, m, alpha, W, sync, ctx->d_info + 1, abort_flag);
   ++ctx->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }

@@ -30,22 +30,24 @@ namespace kgemm {
 
 constexpr int kThreads = 256;
 
+template <typename T>
 struct Prob {
-  const float* A; int64_t a_rs, a_cs;
-  const float* B; int64_t b_rs, b_cs;
-  const float* A2; int64_t a2_rs, a2_cs;
-  const float* B2; int64_t b2_rs, b2_cs;
-  float* C; int64_t c_rs, c_cs;
+  const T* A; int64_t a_rs, a_cs;
+  const T* B; int64_t b_rs, b_cs;
+  const T* A2; int64_t a2_rs, a2_cs;
+  const T* B2; int64_t b2_rs, b2_cs;
+  T* C; int64_t c_rs, c_cs;
   int m, n, k, k2;
-  float alpha, beta;
+  T alpha, beta;
   int c_lower;
   int a_tri, b_tri, a2_tri, b2_tri;  // 0 full, 1 lower, 2 upper (incl. diagonal)
   int tiles_m, tiles_n;
   int tile_begin;
 };
 
+template <typename T>
 struct Batch {
-  Prob p[kMaxBatch];
+  Prob<T> p[kMaxBatch];
   int count;
   int total_tiles;
   const int* abort_flag;  // if non-null and *abort_flag != INT_MAX: no-op
@@ -53,7 +55,8 @@ struct Batch {
 
 // Map a linear tile index of a problem to (ti, tj), in the L2-friendly
 // orders of k_order.cuh (c_lower problems: lower tile triangle).
-__device__ __forceinline__ void tile_coords(const Prob& P, int lt, int& ti,
+template <typename T>
+__device__ __forceinline__ void tile_coords(const Prob<T>& P, int lt, int& ti,
                                             int& tj) {
   if (!P.c_lower) order::grouped_tile(P.tiles_m, P.tiles_n, lt, ti, tj);
   else order::tri_band_tile(P.tiles_m, lt, ti, tj);
@@ -74,9 +77,10 @@ __device__ __forceinline__ int swz(int r, int kk) {
 // One operand of one product is seen as rows r (m of A or n of B) by kk:
 // element (r, kk) at p[r*sr + kk*sk]; tri in the (r, kk) convention: 1 keeps
 // kk <= r, 2 keeps kk >= r, 3 keeps kk > r.  Flags: bit 0 = kk is the unit-stride dimension
-// (else r), bit 1 = float4 loads allowed (unit stride +1, 16-byte aligned
-// base, other stride a multiple of 4).
-__device__ __forceinline__ int operand_flags(const float* p, int64_t sr, int64_t sk) {
+// (else r), bit 1 = vector loads of 4-element groups allowed (unit stride +1,
+// 16-byte aligned base, other stride a multiple of 4).
+template <typename T>
+__device__ __forceinline__ int operand_flags(const T* p, int64_t sr, int64_t sk) {
   const bool kcont = (sk == 1 || sk == -1) && !(sr == 1 || sr == -1);
   const int64_t unit = kcont ? sk : sr, other = kcont ? sr : sk;
   const bool vec = unit == 1 && (other & 3) == 0 && ((reinterpret_cast<uintptr_t>(p) & 15) == 0);
@@ -85,24 +89,51 @@ __device__ __forceinline__ int operand_flags(const float* p, int64_t sr, int64_t
 
 // Register staging of one R x BK tile: NG groups of 4 elements along the
 // operand's unit-stride dimension, G per thread.
-template <int R, int BK>
+template <typename T, int R, int BK>
 struct Stage {
   static constexpr int NG = R * BK / 4;
   static constexpr int G = (NG + kThreads - 1) / kThreads;
-  float v[G][4];
+  T v[G][4];
 };
 
-template <int R, int BK>
-__device__ __forceinline__ void stage_load(Stage<R, BK>& st, const float* p, int64_t sr, int64_t sk,
+// Four consecutive elements as 16-byte accesses (one float4 / two double2).
+__device__ __forceinline__ void ld4(const float* p, float (&v)[4]) {
+  const float4 x = __ldg(reinterpret_cast<const float4*>(p));
+  v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&v)[4]) {
+  const double2 x = __ldg(reinterpret_cast<const double2*>(p));
+  const double2 y = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
+}
+__device__ __forceinline__ void lds4(const float* p, float* v) {
+  const float4 x = *reinterpret_cast<const float4*>(p);
+  v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+}
+__device__ __forceinline__ void lds4(const double* p, double* v) {
+  const double2 x = reinterpret_cast<const double2*>(p)[0];
+  const double2 y = reinterpret_cast<const double2*>(p)[1];
+  v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
+}
+__device__ __forceinline__ void sts4(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void sts4(double* p, const double (&v)[4]) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
+template <typename T, int R, int BK>
+__device__ __forceinline__ void stage_load(Stage<T, R, BK>& st, const T* p, int64_t sr, int64_t sk,
                                            int rows, int depth, int tri, int flags, int r0,
                                            int k0) {
   const int tid = threadIdx.x;
   const bool kcont = flags & 1;
   constexpr int KG = BK / 4;  // groups per row along k
 #pragma unroll
-  for (int u = 0; u < Stage<R, BK>::G; ++u) {
+  for (int u = 0; u < Stage<T, R, BK>::G; ++u) {
     const int e = tid + kThreads * u;
-    if (Stage<R, BK>::NG % kThreads != 0 && e >= Stage<R, BK>::NG) break;
+    if (Stage<T, R, BK>::NG % kThreads != 0 && e >= Stage<T, R, BK>::NG) break;
     int r, kk;  // first element of the group
     if (kcont) { r = e / KG; kk = (e % KG) << 2; }
     else       { r = (e % (R / 4)) << 2; kk = e / (R / 4); }
@@ -110,37 +141,34 @@ __device__ __forceinline__ void stage_load(Stage<R, BK>& st, const float* p, int
     const int lim_r = rows - gr, lim_k = depth - gk;
     const bool full = tri == 0 && (kcont ? (lim_r > 0 && lim_k >= 4) : (lim_k > 0 && lim_r >= 4));
     if ((flags & 2) && full) {
-      const float4 x =
-          __ldg(reinterpret_cast<const float4*>(p + (int64_t)gr * sr + (int64_t)gk * sk));
-      st.v[u][0] = x.x; st.v[u][1] = x.y; st.v[u][2] = x.z; st.v[u][3] = x.w;
+      ld4(p + (int64_t)gr * sr + (int64_t)gk * sk, st.v[u]);
     } else {
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         const int rr = gr + (kcont ? 0 : c), kc = gk + (kcont ? c : 0);
         const bool ok = rr < rows && kc < depth && (tri != 1 || kc <= rr) &&
                         (tri != 2 || kc >= rr) && (tri != 3 || kc > rr);
-        st.v[u][c] = ok ? __ldg(p + (int64_t)rr * sr + (int64_t)kc * sk) : 0.f;
+        st.v[u][c] = ok ? __ldg(p + (int64_t)rr * sr + (int64_t)kc * sk) : T(0);
       }
     }
   }
 }
 
-template <int R, int BK>
-__device__ __forceinline__ void stage_store(const Stage<R, BK>& st, float (*s)[R], bool kcont) {
+template <typename T, int R, int BK>
+__device__ __forceinline__ void stage_store(const Stage<T, R, BK>& st, T (*s)[R], bool kcont) {
   const int tid = threadIdx.x;
   constexpr int KG = BK / 4;
 #pragma unroll
-  for (int u = 0; u < Stage<R, BK>::G; ++u) {
+  for (int u = 0; u < Stage<T, R, BK>::G; ++u) {
     const int e = tid + kThreads * u;
-    if (Stage<R, BK>::NG % kThreads != 0 && e >= Stage<R, BK>::NG) break;
+    if (Stage<T, R, BK>::NG % kThreads != 0 && e >= Stage<T, R, BK>::NG) break;
     if (kcont) {
       const int r = e / KG, kk = (e % KG) << 2;
 #pragma unroll
       for (int c = 0; c < 4; ++c) s[kk + c][swz<BK>(r, kk + c)] = st.v[u][c];
     } else {
       const int r = (e % (R / 4)) << 2, kk = e / (R / 4);
-      *reinterpret_cast<float4*>(&s[kk][swz<BK>(r, kk)]) =
-          make_float4(st.v[u][0], st.v[u][1], st.v[u][2], st.v[u][3]);
+      sts4(&s[kk][swz<BK>(r, kk)], st.v[u]);
     }
   }
 }
@@ -160,22 +188,22 @@ __device__ __forceinline__ void k_range(int k, int a_tri, int b_tri, int m0, int
   if (ke < kb) ke = kb;
 }
 
-template <int BM, int BN>
-__global__ void __launch_bounds__(kThreads, 2) sgemm_batch(const Batch batch) {
+template <typename T, int BM, int BN>
+__global__ void __launch_bounds__(kThreads, 2) sgemm_batch(const Batch<T> batch) {
   if (batch.abort_flag && *batch.abort_flag != INT_MAX) return;
   constexpr int TM = BM / 16, TN = BN / 16;
   constexpr int GM = TM / 4, GN = TN / 4;
   // depth 8 for the 128 x 128 tile keeps the register staging within the
   // 128-register budget of two CTAs per SM
   constexpr int BK = BM >= 128 ? 8 : 16;
-  __shared__ __align__(16) float sa[2][BK][BM];
-  __shared__ __align__(16) float sb[2][BK][BN];
+  __shared__ __align__(16) T sa[2][BK][BM];
+  __shared__ __align__(16) T sb[2][BK][BN];
 
   // Locate the problem and tile.
   int t = blockIdx.x, pi = 0;
 #pragma unroll 1
   while (pi + 1 < batch.count && t >= batch.p[pi + 1].tile_begin) ++pi;
-  const Prob& P = batch.p[pi];
+  const Prob<T>& P = batch.p[pi];
   int ti, tj;
   tile_coords(P, t - P.tile_begin, ti, tj);
   const int m0 = ti * BM, n0 = tj * BN;
@@ -183,11 +211,11 @@ __global__ void __launch_bounds__(kThreads, 2) sgemm_batch(const Batch batch) {
   const int tid = threadIdx.x;
   const int tr = tid / 16, tc = tid % 16;
 
-  float acc[TM][TN];
+  T acc[TM][TN];
 #pragma unroll
   for (int i = 0; i < TM; ++i)
 #pragma unroll
-    for (int j = 0; j < TN; ++j) acc[i][j] = 0.f;
+    for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
 
   // B's mask codes map to the (r = j, kk) convention: lower B keeps kk >= j
   // (code 2 there), upper keeps kk <= j (code 1).
@@ -202,24 +230,26 @@ __global__ void __launch_bounds__(kThreads, 2) sgemm_batch(const Batch batch) {
   const int kt2 = (ke2 - kb2 + BK - 1) / BK;
   const int ktiles = kt1 + kt2;
 
-  Stage<BM, BK> ra;
-  Stage<BN, BK> rb;
+  Stage<T, BM, BK> ra;
+  Stage<T, BN, BK> rb;
   auto load = [&](int kt) {
     if (kt < kt1) {
       const int k0 = kb1 + kt * BK;
-      stage_load<BM, BK>(ra, P.A, P.a_rs, P.a_cs, P.m, P.k, P.a_tri, fl & 3, m0, k0);
-      stage_load<BN, BK>(rb, P.B, P.b_cs, P.b_rs, P.n, P.k, bcode(P.b_tri), (fl >> 2) & 3, n0, k0);
+      stage_load<T, BM, BK>(ra, P.A, P.a_rs, P.a_cs, P.m, P.k, P.a_tri, fl & 3, m0, k0);
+      stage_load<T, BN, BK>(rb, P.B, P.b_cs, P.b_rs, P.n, P.k, bcode(P.b_tri), (fl >> 2) & 3, n0,
+                            k0);
     } else {
       const int k0 = kb2 + (kt - kt1) * BK;
-      stage_load<BM, BK>(ra, P.A2, P.a2_rs, P.a2_cs, P.m, P.k2, P.a2_tri, (fl >> 4) & 3, m0, k0);
-      stage_load<BN, BK>(rb, P.B2, P.b2_cs, P.b2_rs, P.n, P.k2, bcode(P.b2_tri), (fl >> 6) & 3, n0,
-                     k0);
+      stage_load<T, BM, BK>(ra, P.A2, P.a2_rs, P.a2_cs, P.m, P.k2, P.a2_tri, (fl >> 4) & 3, m0,
+                            k0);
+      stage_load<T, BN, BK>(rb, P.B2, P.b2_cs, P.b2_rs, P.n, P.k2, bcode(P.b2_tri), (fl >> 6) & 3,
+                            n0, k0);
     }
   };
   auto store = [&](int kt, int buf) {
     const int f = kt >= kt1 ? fl >> 4 : fl;
-    stage_store<BM, BK>(ra, sa[buf], f & 1);
-    stage_store<BN, BK>(rb, sb[buf], (f >> 2) & 1);
+    stage_store<T, BM, BK>(ra, sa[buf], f & 1);
+    stage_store<T, BN, BK>(rb, sb[buf], (f >> 2) & 1);
   };
 
   if (ktiles > 0) {
@@ -234,32 +264,24 @@ __global__ void __launch_bounds__(kThreads, 2) sgemm_batch(const Batch batch) {
     if (more) load(kt + 1);  // global loads in flight during the FMAs
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
-      float a[TM], b[TN];
+      T a[TM], b[TN];
 #pragma unroll
-      for (int g = 0; g < GM; ++g) {
-        const float4 v = *reinterpret_cast<const float4*>(
-            &sa[buf][kk][swz<BK>(g * (BM / GM) + tr * 4, kk)]);
-        a[g * 4 + 0] = v.x; a[g * 4 + 1] = v.y;
-        a[g * 4 + 2] = v.z; a[g * 4 + 3] = v.w;
-      }
+      for (int g = 0; g < GM; ++g)
+        lds4(&sa[buf][kk][swz<BK>(g * (BM / GM) + tr * 4, kk)], a + g * 4);
 #pragma unroll
-      for (int g = 0; g < GN; ++g) {
-        const float4 v = *reinterpret_cast<const float4*>(
-            &sb[buf][kk][swz<BK>(g * (BN / GN) + tc * 4, kk)]);
-        b[g * 4 + 0] = v.x; b[g * 4 + 1] = v.y;
-        b[g * 4 + 2] = v.z; b[g * 4 + 3] = v.w;
-      }
+      for (int g = 0; g < GN; ++g)
+        lds4(&sb[buf][kk][swz<BK>(g * (BN / GN) + tc * 4, kk)], b + g * 4);
 #pragma unroll
       for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
     if (more) store(kt + 1, buf ^ 1);
     __syncthreads();
   }
 
   // Epilogue.
-  const float alpha = P.alpha, beta = P.beta;
+  const T alpha = P.alpha, beta = P.beta;
 #pragma unroll
   for (int i = 0; i < TM; ++i) {
     const int gi = m0 + (i / 4) * (BM / GM) + tr * 4 + (i % 4);
@@ -269,9 +291,9 @@ __global__ void __launch_bounds__(kThreads, 2) sgemm_batch(const Batch batch) {
       const int gj = n0 + (j / 4) * (BN / GN) + tc * 4 + (j % 4);
       if (gj >= P.n) continue;
       if (P.c_lower && gj > gi) continue;
-      float* c = P.C + (int64_t)gi * P.c_rs + (int64_t)gj * P.c_cs;
-      float v = alpha * acc[i][j];
-      if (beta != 0.f) v = fmaf(beta, *c, v);
+      T* c = P.C + (int64_t)gi * P.c_rs + (int64_t)gj * P.c_cs;
+      T v = alpha * acc[i][j];
+      if (beta != T(0)) v = fma(beta, *c, v);
       *c = v;
     }
   }

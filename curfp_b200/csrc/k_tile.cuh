@@ -14,12 +14,12 @@ namespace ktile {
 // Copy the lower triangle of an n x n view tile into shared memory s[i][j]
 // (zeros above the diagonal).  The warp runs along the view's contiguous
 // dimension and each thread keeps 8 loads in flight.  n <= 32 * RW.
-template <int LDS>
-__device__ __forceinline__ void load_lower(View L, int n, float* s) {
+template <int LDS, typename E>
+__device__ __forceinline__ void load_lower(ViewT<E> L, int n, E* s) {
   const bool rcont = (L.cs == 1 || L.cs == -1);
   const int lane = threadIdx.x % 32, warp = threadIdx.x / 32, nw = blockDim.x / 32;
   for (int base = warp; base < n; base += 8 * nw) {
-    float v[8][4];
+    E v[8][4];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int a = base + u * nw;  // row (rcont) or column (!rcont)
@@ -27,7 +27,7 @@ __device__ __forceinline__ void load_lower(View L, int n, float* s) {
       for (int q = 0; q < 4; ++q) {
         const int b = lane + 32 * q;
         const int i = rcont ? a : b, j = rcont ? b : a;
-        v[u][q] = (a < n && b < n && i >= j) ? L.p[(int64_t)i * L.rs + (int64_t)j * L.cs] : 0.f;
+        v[u][q] = (a < n && b < n && i >= j) ? L.p[(int64_t)i * L.rs + (int64_t)j * L.cs] : E(0);
       }
     }
 #pragma unroll
@@ -44,8 +44,8 @@ __device__ __forceinline__ void load_lower(View L, int n, float* s) {
 }
 
 // Store the lower triangle of s back to the view (same thread mapping).
-template <int LDS>
-__device__ __forceinline__ void store_lower(View L, int n, const float* s) {
+template <int LDS, typename E>
+__device__ __forceinline__ void store_lower(ViewT<E> L, int n, const E* s) {
   const bool rcont = (L.cs == 1 || L.cs == -1);
   const int lane = threadIdx.x % 32, warp = threadIdx.x / 32, nw = blockDim.x / 32;
   for (int a = warp; a < n; a += nw) {
@@ -75,14 +75,29 @@ static_assert(T == kTrsmLeaf && T == kTriTile, "tile kernels assume one tile siz
 // back and the kernel returns (LAPACK xPOTRF semantics).
 constexpr int PT = 128;          // potrf tile (== kPotrfTile)
 constexpr int PLD = PT + 1;
-constexpr int POTRF_SMEM = PT * PLD * 4 + 64 * 4;
+template <typename E>
+constexpr int potrf_smem() { return (PT * PLD + 64) * (int)sizeof(E); }
+constexpr int POTRF_SMEM = potrf_smem<float>();
 static_assert(PT == kPotrfTile, "potrf tile size");
 
-__global__ void __launch_bounds__(256) potrf_tile(View L, int n, int info_base, int* info) {
+// 1/sqrt(d): the hardware estimate refined by one Newton-Raphson step for
+// y = x^-1/2 (y <- y (3 - d y^2) / 2).
+__device__ __forceinline__ float rsqrt_nr(float d) {
+  const float r = rsqrtf(d);
+  return r * fmaf(-0.5f * d * r, r, 1.5f);
+}
+__device__ __forceinline__ double rsqrt_nr(double d) {
+  const double r = rsqrt(d);
+  return r * fma(-0.5 * d * r, r, 1.5);
+}
+
+template <typename E>
+__global__ void __launch_bounds__(256) potrf_tile(ViewT<E> L, int n, int info_base, int* info) {
   if (info && *info != INT_MAX) return;
-  extern __shared__ float dyn[];
-  float (*s)[PLD] = reinterpret_cast<float (*)[PLD]>(dyn);
-  float* rdiag = dyn + PT * PLD;       // 32 reciprocals of the current diagonal block
+  extern __shared__ __align__(16) unsigned char dyn_raw[];
+  E* dyn = reinterpret_cast<E*>(dyn_raw);
+  E (*s)[PLD] = reinterpret_cast<E (*)[PLD]>(dyn);
+  E* rdiag = dyn + PT * PLD;           // 32 reciprocals of the current diagonal block
   __shared__ int fail_sh;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   load_lower<PLD>(L, n, dyn);
@@ -92,28 +107,25 @@ __global__ void __launch_bounds__(256) potrf_tile(View L, int n, int info_base, 
     const int w = min(32, n - c0);
     // (1) diagonal block in registers
     if (warp == 0) {
-      float a[32];
+      E a[32];
 #pragma unroll
-      for (int k = 0; k < 32; ++k) a[k] = (lane < w && k < w) ? s[c0 + lane][c0 + k] : 0.f;
+      for (int k = 0; k < 32; ++k) a[k] = (lane < w && k < w) ? s[c0 + lane][c0 + k] : E(0);
       int fail = 0;
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
         if (j < w && !fail) {
-          const float d = __shfl_sync(0xffffffffu, a[j], j);
-          if (!(d > 0.f)) {
+          const E d = __shfl_sync(0xffffffffu, a[j], j);
+          if (!(d > E(0))) {
             fail = c0 + j + 1;
           } else {
-            // 1/sqrt(d) from rsqrtf refined by one Newton-Raphson step for
-            // y = x^-1/2 (y <- y (3 - d y^2) / 2); the column is scaled by
-            // multiplication, branch-free across the warp.
-            float r = rsqrtf(d);
-            r = r * fmaf(-0.5f * d * r, r, 1.5f);
+            // the column is scaled by multiplication, branch-free across the warp
+            const E r = rsqrt_nr(d);
             a[j] = (lane == j) ? d * r : (lane > j ? a[j] * r : a[j]);
             if (lane == j) rdiag[j] = r;
 #pragma unroll
             for (int k = j + 1; k < 32; ++k) {
-              const float lkj = __shfl_sync(0xffffffffu, a[j], k);
-              if (lane >= k) a[k] = fmaf(-a[j], lkj, a[k]);
+              const E lkj = __shfl_sync(0xffffffffu, a[j], k);
+              if (lane >= k) a[k] = fma(-a[j], lkj, a[k]);
             }
           }
         }
@@ -130,16 +142,16 @@ __global__ void __launch_bounds__(256) potrf_tile(View L, int n, int info_base, 
     const int r1 = c0 + w;
     // (2) rows below: X L_blk^T = A_r
     for (int r = r1 + tid; r < n; r += 256) {
-      float x[32];
+      E x[32];
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
         if (j < w) {
-          float v = s[r][c0 + j];
+          E v = s[r][c0 + j];
 #pragma unroll
-          for (int k = 0; k < j; ++k) v = fmaf(-x[k], s[c0 + j][c0 + k], v);
+          for (int k = 0; k < j; ++k) v = fma(-x[k], s[c0 + j][c0 + k], v);
           x[j] = v * rdiag[j];
         } else {
-          x[j] = 0.f;
+          x[j] = E(0);
         }
       }
 #pragma unroll
@@ -156,24 +168,24 @@ __global__ void __launch_bounds__(256) potrf_tile(View L, int n, int info_base, 
       while (bi * (bi + 1) / 2 > e) --bi;
       const int bj = e - bi * (bi + 1) / 2;
       const int ri = r1 + 4 * bi, cj = r1 + 4 * bj;
-      float acc[4][4];
+      E acc[4][4];
 #pragma unroll
       for (int p = 0; p < 4; ++p)
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-          acc[p][q] = (ri + p < n && cj + q < n) ? s[ri + p][cj + q] : 0.f;
+          acc[p][q] = (ri + p < n && cj + q < n) ? s[ri + p][cj + q] : E(0);
 #pragma unroll 4
       for (int k = 0; k < w; ++k) {
-        float a4[4], b4[4];
+        E a4[4], b4[4];
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
-          a4[p] = (ri + p < n) ? s[ri + p][c0 + k] : 0.f;
-          b4[p] = (cj + p < n) ? s[cj + p][c0 + k] : 0.f;
+          a4[p] = (ri + p < n) ? s[ri + p][c0 + k] : E(0);
+          b4[p] = (cj + p < n) ? s[cj + p][c0 + k] : E(0);
         }
 #pragma unroll
         for (int p = 0; p < 4; ++p)
 #pragma unroll
-          for (int q = 0; q < 4; ++q) acc[p][q] = fmaf(-a4[p], b4[q], acc[p][q]);
+          for (int q = 0; q < 4; ++q) acc[p][q] = fma(-a4[p], b4[q], acc[p][q]);
       }
 #pragma unroll
       for (int p = 0; p < 4; ++p)
@@ -200,21 +212,25 @@ __global__ void __launch_bounds__(256) potrf_tile(View L, int n, int info_base, 
 // finish a block row with one product after its predecessor is published.
 // W == nullptr: the inverse replaces the lower triangle in place.
 constexpr int TRTRI_THREADS = 256;
+template <typename E>
+constexpr int trtri_smem() { return 2 * T * LD * (int)sizeof(E); }
 
-__global__ void __launch_bounds__(TRTRI_THREADS) trtri_blocks(View L, int n, float* W,
+template <typename E>
+__global__ void __launch_bounds__(TRTRI_THREADS) trtri_blocks(ViewT<E> L, int n, E* W,
                                                               const int* abort_flag) {
   if (abort_flag && *abort_flag != INT_MAX) return;
-  __shared__ float s[T][LD];  // L_bb, later the block left of it
-  __shared__ float x[T][LD];  // the inverse (upper-right quarter: scratch)
+  extern __shared__ __align__(16) unsigned char trtri_raw[];
+  E (*s)[LD] = reinterpret_cast<E (*)[LD]>(trtri_raw);  // L_bb, later the block left of it
+  E (*x)[LD] = s + T;  // the inverse (upper-right quarter: scratch)
   const int b = blockIdx.x, r0 = b * T;
   const int sz = min(T, n - r0);
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  const View Lb = sub(L, r0, r0);
+  const ViewT<E> Lb = sub(L, r0, r0);
   // both buffers start at zero: the quarter products read whole 32 x 32
   // quarters, also rows beyond a partial last block
   for (int e = tid; e < T * LD; e += TRTRI_THREADS) {
-    (&x[0][0])[e] = 0.f;
-    (&s[0][0])[e] = 0.f;
+    (&x[0][0])[e] = E(0);
+    (&s[0][0])[e] = E(0);
   }
   __syncthreads();
   load_lower<LD>(Lb, sz, &s[0][0]);
@@ -222,22 +238,22 @@ __global__ void __launch_bounds__(TRTRI_THREADS) trtri_blocks(View L, int n, flo
   if (warp < 2) {
     const int q0 = warp * 32, w = min(32, sz - q0);
     if (w > 0) {
-      float a[32], xr[32];
+      E a[32], xr[32];
 #pragma unroll
       for (int k = 0; k < 32; ++k) {
-        a[k] = (lane < w && k <= lane) ? s[q0 + lane][q0 + k] : 0.f;
-        xr[k] = (k == lane && lane < w) ? 1.f : 0.f;
+        a[k] = (lane < w && k <= lane) ? s[q0 + lane][q0 + k] : E(0);
+        xr[k] = (k == lane && lane < w) ? E(1) : E(0);
       }
-      const float rl = lane < w ? 1.0f / s[q0 + lane][q0 + lane] : 0.f;
+      const E rl = lane < w ? E(1) / s[q0 + lane][q0 + lane] : E(0);
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
         if (j < w) {
-          const float sc = lane == j ? rl : 1.f;
+          const E sc = lane == j ? rl : E(1);
 #pragma unroll
           for (int k = 0; k <= j; ++k) {
             xr[k] *= sc;
-            const float v = __shfl_sync(0xffffffffu, xr[k], j);
-            if (lane > j) xr[k] = fmaf(-a[j], v, xr[k]);
+            const E v = __shfl_sync(0xffffffffu, xr[k], j);
+            if (lane > j) xr[k] = fma(-a[j], v, xr[k]);
           }
         }
       }
@@ -251,11 +267,11 @@ __global__ void __launch_bounds__(TRTRI_THREADS) trtri_blocks(View L, int n, flo
     // diagonal, so the sums may run over all k)
     for (int e = tid; e < 1024; e += TRTRI_THREADS) {
       const int i = e >> 5, j = e & 31;
-      float a0 = 0.f, a1 = 0.f;
+      E a0 = E(0), a1 = E(0);
 #pragma unroll
       for (int k = 0; k < 32; k += 2) {
-        a0 = fmaf(s[32 + i][k], x[k][j], a0);
-        a1 = fmaf(s[32 + i][k + 1], x[k + 1][j], a1);
+        a0 = fma(s[32 + i][k], x[k][j], a0);
+        a1 = fma(s[32 + i][k + 1], x[k + 1][j], a1);
       }
       x[i][32 + j] = a0 + a1;
     }
@@ -263,42 +279,42 @@ __global__ void __launch_bounds__(TRTRI_THREADS) trtri_blocks(View L, int n, flo
     // lower-left = -inv(D1) T
     for (int e = tid; e < 1024; e += TRTRI_THREADS) {
       const int i = e >> 5, j = e & 31;
-      float a0 = 0.f, a1 = 0.f;
+      E a0 = E(0), a1 = E(0);
 #pragma unroll
       for (int k = 0; k < 32; k += 2) {
-        a0 = fmaf(x[32 + i][32 + k], x[k][32 + j], a0);
-        a1 = fmaf(x[32 + i][33 + k], x[k + 1][32 + j], a1);
+        a0 = fma(x[32 + i][32 + k], x[k][32 + j], a0);
+        a1 = fma(x[32 + i][33 + k], x[k + 1][32 + j], a1);
       }
       x[32 + i][j] = -(a0 + a1);
     }
     __syncthreads();
-    for (int e = tid; e < 1024; e += TRTRI_THREADS) x[e >> 5][32 + (e & 31)] = 0.f;
+    for (int e = tid; e < 1024; e += TRTRI_THREADS) x[e >> 5][32 + (e & 31)] = E(0);
     __syncthreads();
   }
   if (!W) {
     store_lower<LD>(Lb, sz, &x[0][0]);
     return;
   }
-  float* Wb = W + (int64_t)b * kInvStride;
+  E* Wb = W + (int64_t)b * kInvStride;
   for (int e = tid; e < T * T; e += TRTRI_THREADS) Wb[e] = x[e & 63][e >> 6];
   if (b == 0) return;
   // M_b = W_b L_{b,b-1}: the 64 x 64 block left of the diagonal block (rows
   // beyond sz are zero), 4 x 4 outputs per thread.
-  const View Lp = sub(L, r0, r0 - T);
+  const ViewT<E> Lp = sub(L, r0, r0 - T);
   for (int e = tid; e < T * T; e += TRTRI_THREADS) {
     const int i = e >> 6, c = e & 63;
-    s[i][c] = i < sz ? Lp.p[(int64_t)i * Lp.rs + (int64_t)c * Lp.cs] : 0.f;
+    s[i][c] = i < sz ? Lp.p[(int64_t)i * Lp.rs + (int64_t)c * Lp.cs] : E(0);
   }
   __syncthreads();
   const int ri = (tid >> 4) * 4, ci = (tid & 15) * 4;
-  float acc[4][4];
+  E acc[4][4];
 #pragma unroll
   for (int p = 0; p < 4; ++p)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) acc[p][q] = 0.f;
+    for (int q = 0; q < 4; ++q) acc[p][q] = E(0);
 #pragma unroll 4
   for (int k = 0; k < T; ++k) {
-    float x4[4], s4[4];
+    E x4[4], s4[4];
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
       x4[p] = x[ri + p][k];
@@ -307,9 +323,9 @@ __global__ void __launch_bounds__(TRTRI_THREADS) trtri_blocks(View L, int n, flo
 #pragma unroll
     for (int p = 0; p < 4; ++p)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) acc[p][q] = fmaf(x4[p], s4[q], acc[p][q]);
+      for (int q = 0; q < 4; ++q) acc[p][q] = fma(x4[p], s4[q], acc[p][q]);
   }
-  float* Mb = Wb + T * T;
+  E* Mb = Wb + T * T;
 #pragma unroll
   for (int p = 0; p < 4; ++p)
 #pragma unroll
@@ -318,19 +334,20 @@ __global__ void __launch_bounds__(TRTRI_THREADS) trtri_blocks(View L, int n, flo
 
 // In-place L := L^T L (lower part) for an n x n tile, n <= 64.
 // (L^T L)(i,j) = sum_{k >= i} L(k,i) L(k,j) for i >= j.
-__global__ void __launch_bounds__(256) lauum_tile(View L, int n) {
-  __shared__ float s[T][LD];
+template <typename E>
+__global__ void __launch_bounds__(256) lauum_tile(ViewT<E> L, int n) {
+  __shared__ E s[T][LD];
   const int tid = threadIdx.x;
   load_lower<LD>(L, n, &s[0][0]);
   __syncthreads();
-  float out[16];
+  E out[16];
   const int j = tid % T, i0 = tid / T;
 #pragma unroll
   for (int r = 0; r < 16; ++r) {
     const int i = i0 + 4 * r;
-    float acc = 0.f;
+    E acc = E(0);
     if (i < n && j < n && i >= j)
-      for (int k = i; k < n; ++k) acc = fmaf(s[k][i], s[k][j], acc);
+      for (int k = i; k < n; ++k) acc = fma(s[k][i], s[k][j], acc);
     out[r] = acc;
   }
   __syncthreads();
@@ -347,8 +364,9 @@ constexpr int MTS = 32, MTY = 8;  // mirror tile edge, thread rows
 // D(q,p) := D(p,q) for p > q on an n x n view: one 32 x 32 tile of the lower
 // tile triangle per CTA, read along the view's contiguous dimension and
 // written transposed through shared memory, so both sides coalesce.
-__global__ void __launch_bounds__(MTS * MTY) mirror_lower(View D, int n) {
-  __shared__ float tile[MTS][MTS + 1];
+template <typename E>
+__global__ void __launch_bounds__(MTS * MTY) mirror_lower(ViewT<E> D, int n) {
+  __shared__ E tile[MTS][MTS + 1];
   const int lt = blockIdx.x;
   int tp = (int)((sqrt(8.0 * (double)lt + 1.0) - 1.0) * 0.5);
   while ((tp + 1) * (tp + 2) / 2 <= lt) ++tp;

@@ -33,10 +33,12 @@ namespace ktrsv {
 
 constexpr int NB = 64;
 constexpr int LDL = NB + 1;  // L / W / M tiles: scalar reads down a row, conflict-free both ways
-constexpr int LDX = NB + 4;  // X / T tiles: float4 reads along a row
+constexpr int LDX = NB + 4;  // X / T tiles: 16-byte reads along a row
 constexpr uint64_t WAIT_NS = 2000000000ull;
 // Ls[2], Ws (L tiles; W_j; M_j reuses Ls[0]) and Xs[2], Ts (X tiles; B_jc / T)
-constexpr int SMEM = (3 * NB * LDL + 3 * NB * LDX) * 4;
+template <typename T>
+constexpr int smem_bytes() { return (3 * NB * LDL + 3 * NB * LDX) * (int)sizeof(T); }
+constexpr int SMEM = smem_bytes<float>();
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -51,10 +53,16 @@ __device__ __forceinline__ uint64_t gtimer() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-__device__ __forceinline__ void cp4(float* smem, const float* g, bool pred) {
+// One element by cp.async (4 or 8 bytes), zero-filled when !pred.
+__device__ __forceinline__ void cp1(float* smem, const float* g, bool pred) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(g),
                "r"(pred ? 4 : 0));
+}
+__device__ __forceinline__ void cp1(double* smem, const double* g, bool pred) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(g),
+               "r"(pred ? 8 : 0));
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
@@ -64,29 +72,31 @@ __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;
 // contiguous dimension.  (cp.async of 4 bytes caches in L1, which is not
 // coherent with other CTAs' stores: only data that no CTA of this launch
 // writes goes this way.)
-template <int LD>
-__device__ __forceinline__ void load_tile(float* s, View v, int rows, int cols) {
+template <int LD, typename T>
+__device__ __forceinline__ void load_tile(T* s, ViewT<T> v, int rows, int cols) {
   const bool rowcont = (v.cs == 1 || v.cs == -1) && !(v.rs == 1 || v.rs == -1);
 #pragma unroll 4
   for (int u = 0; u < 16; ++u) {
     const int e = threadIdx.x + 256 * u;
     const int a = rowcont ? e / NB : e % NB, b = rowcont ? e % NB : e / NB;
     const bool ok = a < rows && b < cols;
-    cp4(s + a * LD + b, ok ? v.p + (int64_t)a * v.rs + (int64_t)b * v.cs : v.p, ok);
+    cp1(s + a * LD + b, ok ? v.p + (int64_t)a * v.rs + (int64_t)b * v.cs : v.p, ok);
   }
 }
 // Tile of B / X (written by CTAs of this launch): L2-only loads into
 // registers (ld.global.cg), stored to shared memory by store_regs.
-__device__ __forceinline__ void load_regs(float (&r)[16], View v, int rows, int cols) {
+template <typename T>
+__device__ __forceinline__ void load_regs(T (&r)[16], ViewT<T> v, int rows, int cols) {
   const bool rowcont = (v.cs == 1 || v.cs == -1) && !(v.rs == 1 || v.rs == -1);
 #pragma unroll
   for (int u = 0; u < 16; ++u) {
     const int e = threadIdx.x + 256 * u;
     const int a = rowcont ? e / NB : e % NB, b = rowcont ? e % NB : e / NB;
-    r[u] = (a < rows && b < cols) ? __ldcg(v.p + (int64_t)a * v.rs + (int64_t)b * v.cs) : 0.f;
+    r[u] = (a < rows && b < cols) ? __ldcg(v.p + (int64_t)a * v.rs + (int64_t)b * v.cs) : T(0);
   }
 }
-__device__ __forceinline__ void store_regs(float* s, const float (&r)[16], View v) {
+template <typename T>
+__device__ __forceinline__ void store_regs(T* s, const T (&r)[16], ViewT<T> v) {
   const bool rowcont = (v.cs == 1 || v.cs == -1) && !(v.rs == 1 || v.rs == -1);
 #pragma unroll
   for (int u = 0; u < 16; ++u) {
@@ -96,30 +106,40 @@ __device__ __forceinline__ void store_regs(float* s, const float (&r)[16], View 
   }
 }
 // 64 x 64 column-major workspace tile -> s[a][b] (row stride LDL).
-__device__ __forceinline__ void load_ws(float* s, const float* w) {
+template <typename T>
+__device__ __forceinline__ void load_ws(T* s, const T* w) {
 #pragma unroll 4
   for (int u = 0; u < 16; ++u) {
     const int e = threadIdx.x + 256 * u;
-    cp4(s + (e % NB) * LDL + e / NB, w + e, true);
+    cp1(s + (e % NB) * LDL + e / NB, w + e, true);
   }
+}
+// Four consecutive shared-memory elements (16-byte reads).
+__device__ __forceinline__ void lds4(const float* p, float (&v)[4]) {
+  const float4 x = *reinterpret_cast<const float4*>(p);
+  v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+}
+__device__ __forceinline__ void lds4(const double* p, double (&v)[4]) {
+  const double2 x = reinterpret_cast<const double2*>(p)[0];
+  const double2 y = reinterpret_cast<const double2*>(p)[1];
+  v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
 }
 // acc (+)= sign * A(64 x 64, row stride LDL) * X(64 x 64, row stride LDX) on
 // the thread's 4 x 4 register tile (rows tr*4.., columns tc*4..).
-template <bool kSub>
-__device__ __forceinline__ void tile_mma(float (&acc)[4][4], const float* A, const float* X,
-                                         int tr, int tc) {
+template <bool kSub, typename T>
+__device__ __forceinline__ void tile_mma(T (&acc)[4][4], const T* A, const T* X, int tr,
+                                         int tc) {
 #pragma unroll 8
   for (int k = 0; k < NB; ++k) {
-    float a4[4];
+    T a4[4], x4[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) a4[q] = A[(tr * 4 + q) * LDL + k];
-    const float4 x = *reinterpret_cast<const float4*>(X + k * LDX + tc * 4);
-    const float x4[4] = {x.x, x.y, x.z, x.w};
+    lds4(X + k * LDX + tc * 4, x4);
 #pragma unroll
     for (int p = 0; p < 4; ++p)
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        acc[p][q] = kSub ? fmaf(-a4[p], x4[q], acc[p][q]) : fmaf(a4[p], x4[q], acc[p][q]);
+        acc[p][q] = kSub ? fma(-a4[p], x4[q], acc[p][q]) : fma(a4[p], x4[q], acc[p][q]);
   }
 }
 
@@ -140,17 +160,19 @@ __device__ __forceinline__ int wait_flag(const int* f, int* err) {
 
 // sync layout: sync[0] = ticket counter, sync[1 + b*nchunk + c] = flag of
 // block row b, chunk c (0 = not ready, 1 = ready, -1 = poisoned).
-// All zero at launch.  W: kInvStride floats per block row ([W_j | M_j]).
-__global__ void __launch_bounds__(256, 2) trsm_wave(View L, int n, View B, int m, float alpha,
-                                                    const float* __restrict__ W, int* sync,
-                                                    int* err, const int* abort_flag) {
-  extern __shared__ __align__(16) float dyn_tsv[];
-  float* Ls0 = dyn_tsv;
-  float* Ls1 = Ls0 + NB * LDL;
-  float* Ws = Ls1 + NB * LDL;
-  float* Xs0 = Ws + NB * LDL;
-  float* Xs1 = Xs0 + NB * LDX;
-  float* Ts = Xs1 + NB * LDX;
+// All zero at launch.  W: kInvStride elements per block row ([W_j | M_j]).
+// FP32: two CTAs per SM (102 KB of shared memory each); FP64: one (204 KB).
+template <typename T>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+    trsm_wave(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const T* __restrict__ W,
+              int* sync, int* err, const int* abort_flag) {
+  extern __shared__ __align__(16) unsigned char dyn_tsv_raw[];
+  T* Ls0 = reinterpret_cast<T*>(dyn_tsv_raw);
+  T* Ls1 = Ls0 + NB * LDL;
+  T* Ws = Ls1 + NB * LDL;
+  T* Xs0 = Ws + NB * LDL;
+  T* Xs1 = Xs0 + NB * LDX;
+  T* Ts = Xs1 + NB * LDX;
   __shared__ int sh_ticket, sh_state, sh_ready[2], sh_last;
   if (abort_flag && *abort_flag != INT_MAX) return;
   const int tid = threadIdx.x;
@@ -163,19 +185,19 @@ __global__ void __launch_bounds__(256, 2) trsm_wave(View L, int n, View B, int m
   const int rows = min(NB, n - r0), cols = min(NB, m - c0);
   const int tr = tid / 16, tc = tid % 16;  // 4 x 4 register tile
   int* flags = sync + 1;
-  const View Bt = sub(B, r0, c0);
-  const float* Wj = W + (int64_t)j * kInvStride;
+  const ViewT<T> Bt = sub(B, r0, c0);
+  const T* Wj = W + (int64_t)j * kInvStride;
   auto xview = [&](int i) { return sub(B, (int64_t)i * NB, c0); };
   auto lview = [&](int i) { return sub(L, r0, (int64_t)i * NB); };
 
-  float acc[4][4];
+  T acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
+    for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
 
   // Loads that depend on no other CTA: W_j, B_jc, the first L tile.
-  float xr[16];
+  T xr[16];
   load_ws(Ws, Wj);
   load_regs(xr, Bt, rows, cols);
   store_regs(Ts, xr, Bt);
@@ -195,10 +217,10 @@ __global__ void __launch_bounds__(256, 2) trsm_wave(View L, int n, View B, int m
   cp_commit();
 
   for (int i = 0; i < iend && !poisoned; ++i) {
-    float* Lb = (i & 1) ? Ls1 : Ls0;
-    float* Xb = (i & 1) ? Xs1 : Xs0;
-    float* Ln = (i & 1) ? Ls0 : Ls1;
-    float* Xn = (i & 1) ? Xs0 : Xs1;
+    T* Lb = (i & 1) ? Ls1 : Ls0;
+    T* Xb = (i & 1) ? Xs1 : Xs0;
+    T* Ln = (i & 1) ? Ls0 : Ls1;
+    T* Xn = (i & 1) ? Xs0 : Xs1;
     const bool more = i + 1 < iend;
     if (tid == 0) sh_ready[i & 1] = more ? ld_acquire(&flags[(i + 1) * nchunk + c]) : 0;
     cp_wait_all();
@@ -241,9 +263,9 @@ __global__ void __launch_bounds__(256, 2) trsm_wave(View L, int n, View B, int m
   for (int p = 0; p < 4; ++p)
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      float* tp = Ts + (tr * 4 + p) * LDX + tc * 4 + q;
-      *tp = fmaf(alpha, *tp, -acc[p][q]);
-      acc[p][q] = 0.f;
+      T* tp = Ts + (tr * 4 + p) * LDX + tc * 4 + q;
+      *tp = fma(alpha, *tp, -acc[p][q]);
+      acc[p][q] = T(0);
     }
   __syncthreads();
   tile_mma<false>(acc, Ws, Ts, tr, tc);

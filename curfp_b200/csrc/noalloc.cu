@@ -63,7 +63,7 @@ float* scratch_address() {
 // static array.
 class NoAllocExec : public rfp::CudaExec {
  public:
-  NoAllocExec(curfpContext* ctx, float* scratch) : CudaExec(ctx), scratch_(scratch) {}
+  NoAllocExec(curfpContext* ctx, float* scratch) : rfp::CudaExec(ctx), scratch_(scratch) {}
 
   float* workspace(size_t nfloats) override {
     return nfloats <= kInvFloats ? scratch_ : nullptr;
