@@ -565,3 +565,10 @@ def ssfr2(arf: torch.Tensor, x: torch.Tensor, y: torch.Tensor, *, alpha: float =
     if y.numel() != n:
         raise ValueError(f"y must have {n} elements, got {y.numel()}")
     ssfr2_raw(_get_handle(), _op(transr), _fill(uplo), n, alpha, x, 1, y, 1, arf)
+
+
+# FP64 (D-prefix) twins (reference curfp/__init__.py:1347-2090).
+from ._double import *  # noqa: E402,F401,F403
+from ._double import __all__ as _double_all  # noqa: E402
+
+__all__ += _double_all

@@ -43,6 +43,21 @@ SIGNATURES = {
                         ctypes.POINTER(_f), _p, _i],
     "curfpGetKernelLaunchCount": [_h, ctypes.POINTER(ctypes.c_longlong)],
     "curfpReleaseWorkspace": [_h],
+    "curfpDsfrk": [_h, _i, _i, _i, _i, _i, ctypes.POINTER(_d), _p, _i, ctypes.POINTER(_d), _p],
+    "curfpDsfr2k": [_h, _i, _i, _i, _i, _i, ctypes.POINTER(_d), _p, _i, _p, _i,
+                    ctypes.POINTER(_d), _p],
+    "curfpDpftrf": [_h, _i, _i, _i, _p, ctypes.POINTER(_i)],
+    "curfpDpftrs": [_h, _i, _i, _i, _i, _p, _p, _i],
+    "curfpDpftri": [_h, _i, _i, _i, _p],
+    "curfpDstrttf": [_h, _i, _i, _i, _p, _i, _p],
+    "curfpDstfttr": [_h, _i, _i, _i, _p, _p, _i],
+    "curfpDsfmm": [_h, _i, _i, _i, _i, _i, ctypes.POINTER(_d), _p, _p, _i, ctypes.POINTER(_d),
+                   _p, _i],
+    "curfpDsfmv": [_h, _i, _i, _i, ctypes.POINTER(_d), _p, _p, _i, ctypes.POINTER(_d), _p, _i],
+    "curfpDsfr": [_h, _i, _i, _i, ctypes.POINTER(_d), _p, _i, _p],
+    "curfpDsfr2": [_h, _i, _i, _i, ctypes.POINTER(_d), _p, _i, _p, _i, _p],
+    "curfpDlansf": [_h, _i, _i, _i, _i, _p, ctypes.POINTER(_d)],
+    "curfpDpfcon": [_h, _i, _i, _i, _p, _d, ctypes.POINTER(_d)],
     "curfpSlansf": [_h, _i, _i, _i, _i, _p, ctypes.POINTER(_f)],
     "curfpSsfmm": [_h, _i, _i, _i, _i, _i, ctypes.POINTER(_f), _p, _p, _i,
                    ctypes.POINTER(_f), _p, _i],

@@ -74,16 +74,18 @@ inline bool symm_attr() {
 
 // Flags a zero on the diagonal of the factor (the condition on which the
 // reference's SPOTRI reports failure, src/curfp_spftri.cu:318,326).
-__global__ void diag_zero_check(Geometry g, const float* arf, int* flag) {
+template <typename T>
+__global__ void diag_zero_check(Geometry g, const T* arf, int* flag) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < g.n && arf[rfp::diag_offset(g, i)] == 0.0f) atomicMin(flag, (int)i + 1);
+  if (i < g.n && arf[rfp::diag_offset(g, i)] == T(0)) atomicMin(flag, (int)i + 1);
 }
 
 // Copy between the logical lower triangle of a dense n x n view (element
 // (P,Q) at src/dst[P*drs + Q*dcs]) and an RFP array; dense -> RFP multiplies
 // the diagonal by diag_scale.
-curfpStatus_t pack_strided(curfpHandle_t h, int transr, int lower, int n, const float* src,
-                           float* dst, int64_t drs, int64_t dcs, int to_rfp,
+template <typename T>
+curfpStatus_t pack_strided(curfpHandle_t h, int transr, int lower, int n, const T* src,
+                           T* dst, int64_t drs, int64_t dcs, int to_rfp,
                            float diag_scale) {
   Geometry g = rfp::geometry(n, transr, lower);
   rfp::kpack::PackArgs a{};
@@ -92,8 +94,8 @@ curfpStatus_t pack_strided(curfpHandle_t h, int transr, int lower, int n, const 
   a.dcs = dcs;
   a.diag_scale = diag_scale;
   if (tiles == 0) return CURFP_STATUS_SUCCESS;
-  rfp::ProfScope ps(h->prof, h->stream, rfp::K_PACK, 0, 4.0 * n * ((double)n + 1));
-  rfp::kpack::pack_kernel<float>
+  rfp::ProfScope ps(h->prof, h->stream, rfp::K_PACK, 0, (double)sizeof(T) * n * ((double)n + 1));
+  rfp::kpack::pack_kernel<T>
       <<<tiles, dim3(rfp::kpack::TX, rfp::kpack::TY), 0, h->stream>>>(a, src, dst,
                                                                      to_rfp);
   ++h->launches;
@@ -101,8 +103,9 @@ curfpStatus_t pack_strided(curfpHandle_t h, int transr, int lower, int n, const 
 }
 
 // strttf / stfttr on a row-major n x n matrix with leading dimension lda.
-curfpStatus_t pack(curfpHandle_t h, int transr, int lower, int n, const float* src,
-                   float* dst, int64_t lda, int to_rfp) {
+template <typename T>
+curfpStatus_t pack(curfpHandle_t h, int transr, int lower, int n, const T* src,
+                   T* dst, int64_t lda, int to_rfp) {
   return pack_strided(h, transr, lower, n, src, dst, lower ? lda : 1, lower ? 1 : lda,
                       to_rfp, 1.0f);
 }
@@ -138,7 +141,8 @@ int symm_launch(curfpHandle_t h, const Geometry& g, const float* A, const float*
 
 }  // namespace
 
-extern "C" {
+// Entry points: C linkage from their declarations in include/curfp.h (the
+// shared implementations below are C++ templates over the element type).
 
 // src/curfp_handle.cpp:4-26
 curfpStatus_t curfpCreate(curfpHandle_t* handle) {
@@ -223,18 +227,19 @@ curfpStatus_t curfpGetStream(curfpHandle_t handle, cudaStream_t* stream) {
 // Checks and quick returns: src/curfp_ssfrk.cpp:147-161.  The leading
 // dimension bound is the one the reference's cuBLAS calls enforce
 // (lda >= rows of the A sub-blocks for trans=N, >= k for trans=T).
+template <typename T>
 static curfpStatus_t ssfrk_impl(curfpHandle_t handle, curfpOperation_t transr,
                                 curfpFillMode_t uplo, curfpOperation_t trans, int n,
-                                int k, const float* alpha, const float* A, int lda,
-                                const float* beta, float* C, int math) {
+                                int k, const T* alpha, const T* A, int lda,
+                                const T* beta, T* C, int math) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (n < 0 || k < 0 || lda < 1) return CURFP_STATUS_INVALID_VALUE;
   if (!alpha || !beta) return CURFP_STATUS_INVALID_VALUE;
   if (n == 0) return CURFP_STATUS_SUCCESS;
-  if ((*alpha == 0.0f || k == 0) && *beta == 1.0f) return CURFP_STATUS_SUCCESS;
-  if (*alpha == 0.0f && *beta == 0.0f) {
+  if ((*alpha == T(0) || k == 0) && *beta == T(1)) return CURFP_STATUS_SUCCESS;
+  if (*alpha == T(0) && *beta == T(0)) {
     size_t nt = (size_t)n * (n + 1) / 2;
-    return cudaMemsetAsync(C, 0, nt * sizeof(float), handle->stream) == cudaSuccess
+    return cudaMemsetAsync(C, 0, nt * sizeof(T), handle->stream) == cudaSuccess
                ? CURFP_STATUS_SUCCESS
                : CURFP_STATUS_EXECUTION_FAILED;
   }
@@ -242,7 +247,7 @@ static curfpStatus_t ssfrk_impl(curfpHandle_t handle, curfpOperation_t transr,
   const int n1 = n1_of(n, lower), nmax = n1 > n - n1 ? n1 : n - n1;
   if (lda < (trans == CURFP_OP_N ? nmax : (k > 1 ? k : 1)))
     return CURFP_STATUS_INVALID_VALUE;
-  CudaExec ex(handle);
+  rfp::CudaExecT<T> ex(handle);
   return status_of(rfp::plan::ssfrk(ex, transr == CURFP_OP_T, lower,
                                     trans == CURFP_OP_T, n, k, *alpha, A, lda,
                                     *beta, C, math));
@@ -265,19 +270,19 @@ curfpStatus_t curfpSsfrkEx(curfpHandle_t handle, curfpOperation_t transr,
 }
 
 // src/curfp_ssfr2k.cpp:121-232
-curfpStatus_t curfpSsfr2k(curfpHandle_t handle, curfpOperation_t transr,
-                          curfpFillMode_t uplo, curfpOperation_t trans, int n,
-                          int k, const float* alpha, const float* A, int lda,
-                          const float* B, int ldb, const float* beta,
-                          float* C) {
+template <typename T>
+static curfpStatus_t sfr2k_impl(curfpHandle_t handle, curfpOperation_t transr,
+                                curfpFillMode_t uplo, curfpOperation_t trans, int n, int k,
+                                const T* alpha, const T* A, int lda, const T* B, int ldb,
+                                const T* beta, T* C) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (n < 0 || k < 0 || lda < 1 || ldb < 1) return CURFP_STATUS_INVALID_VALUE;
   if (!alpha || !beta) return CURFP_STATUS_INVALID_VALUE;
   if (n == 0) return CURFP_STATUS_SUCCESS;
-  if ((*alpha == 0.0f || k == 0) && *beta == 1.0f) return CURFP_STATUS_SUCCESS;
-  if (*alpha == 0.0f && *beta == 0.0f) {
+  if ((*alpha == T(0) || k == 0) && *beta == T(1)) return CURFP_STATUS_SUCCESS;
+  if (*alpha == T(0) && *beta == T(0)) {
     size_t nt = (size_t)n * (n + 1) / 2;
-    return cudaMemsetAsync(C, 0, nt * sizeof(float), handle->stream) == cudaSuccess
+    return cudaMemsetAsync(C, 0, nt * sizeof(T), handle->stream) == cudaSuccess
                ? CURFP_STATUS_SUCCESS
                : CURFP_STATUS_EXECUTION_FAILED;
   }
@@ -285,17 +290,26 @@ curfpStatus_t curfpSsfr2k(curfpHandle_t handle, curfpOperation_t transr,
   const int n1 = n1_of(n, lower), nmax = n1 > n - n1 ? n1 : n - n1;
   const int need = trans == CURFP_OP_N ? nmax : (k > 1 ? k : 1);
   if (lda < need || ldb < need) return CURFP_STATUS_INVALID_VALUE;
-  CudaExec ex(handle);
+  rfp::CudaExecT<T> ex(handle);
   return status_of(rfp::plan::ssfr2k(ex, transr == CURFP_OP_T, lower,
                                      trans == CURFP_OP_T, n, k, *alpha, A, lda,
                                      B, ldb, *beta, C));
 }
 
+curfpStatus_t curfpSsfr2k(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, curfpOperation_t trans, int n,
+                          int k, const float* alpha, const float* A, int lda,
+                          const float* B, int ldb, const float* beta,
+                          float* C) {
+  return sfr2k_impl(handle, transr, uplo, trans, n, k, alpha, A, lda, B, ldb, beta, C);
+}
+
 // src/curfp_spftrf.cpp:182-292.  One stream, no host synchronisation until
 // the single info read-back at the end (the reference syncs after each of its
 // two SPOTRF calls).  A failed pivot makes every later kernel return early.
+template <typename T>
 static curfpStatus_t spftrf_impl(curfpHandle_t handle, curfpOperation_t transr,
-                                 curfpFillMode_t uplo, int n, float* A, int* info,
+                                 curfpFillMode_t uplo, int n, T* A, int* info,
                                  int math) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (n < 0) return CURFP_STATUS_INVALID_VALUE;
@@ -303,7 +317,7 @@ static curfpStatus_t spftrf_impl(curfpHandle_t handle, curfpOperation_t transr,
   *info = 0;
   if (n == 0) return CURFP_STATUS_SUCCESS;
   if (!reset_info(handle)) return CURFP_STATUS_EXECUTION_FAILED;
-  CudaExec ex(handle, handle->d_info);
+  rfp::CudaExecT<T> ex(handle, handle->d_info);
   int rc = rfp::plan::spftrf(ex, transr == CURFP_OP_T,
                              uplo == CURFP_FILL_MODE_LOWER, n, A, math);
   if (rc) return status_of(rc);
@@ -328,39 +342,51 @@ curfpStatus_t curfpSpftrfEx(curfpHandle_t handle, curfpOperation_t transr,
 }
 
 // src/curfp_spftrs.cpp:215-302
-curfpStatus_t curfpSpftrs(curfpHandle_t handle, curfpOperation_t transr,
-                          curfpFillMode_t uplo, int n, int nrhs, const float* A,
-                          float* B, int ldb) {
+template <typename T>
+static curfpStatus_t pftrs_impl(curfpHandle_t handle, curfpOperation_t transr,
+                                curfpFillMode_t uplo, int n, int nrhs, const T* A, T* B,
+                                int ldb) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (n < 0 || nrhs < 0 || ldb < 1) return CURFP_STATUS_INVALID_VALUE;
   if (n == 0 || nrhs == 0) return CURFP_STATUS_SUCCESS;
   const int lower = uplo == CURFP_FILL_MODE_LOWER;
   const int n1 = n1_of(n, lower), nmax = n1 > n - n1 ? n1 : n - n1;
   if (ldb < nmax) return CURFP_STATUS_INVALID_VALUE;
-  CudaExec ex(handle);
+  rfp::CudaExecT<T> ex(handle);
   return status_of(rfp::plan::spftrs(ex, transr == CURFP_OP_T, lower, n, nrhs,
                                      A, B, ldb));
 }
 
+curfpStatus_t curfpSpftrs(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, int n, int nrhs, const float* A,
+                          float* B, int ldb) {
+  return pftrs_impl(handle, transr, uplo, n, nrhs, A, B, ldb);
+}
+
 // src/curfp_spftri.cu:159-388.  A zero on the factor's diagonal is reported
 // as EXECUTION_FAILED before anything is overwritten.
-curfpStatus_t curfpSpftri(curfpHandle_t handle, curfpOperation_t transr,
-                          curfpFillMode_t uplo, int n, float* arf) {
+template <typename T>
+static curfpStatus_t pftri_impl(curfpHandle_t handle, curfpOperation_t transr,
+                                curfpFillMode_t uplo, int n, T* arf) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (n < 0) return CURFP_STATUS_INVALID_VALUE;
   if (n == 0) return CURFP_STATUS_SUCCESS;
   const int tr = transr == CURFP_OP_T, lower = uplo == CURFP_FILL_MODE_LOWER;
   Geometry g = rfp::geometry(n, tr, lower);
   if (!reset_info(handle)) return CURFP_STATUS_EXECUTION_FAILED;
-  diag_zero_check<<<(n + 255) / 256, 256, 0, handle->stream>>>(g, arf,
-                                                              handle->d_info);
+  diag_zero_check<T><<<(n + 255) / 256, 256, 0, handle->stream>>>(g, arf, handle->d_info);
   ++handle->launches;
   if (!ok_launch()) return CURFP_STATUS_EXECUTION_FAILED;
   int h = 0, err = 0;
   if (!read_info(handle, &h, &err)) return CURFP_STATUS_EXECUTION_FAILED;
   if (h != INT_MAX) return CURFP_STATUS_EXECUTION_FAILED;
-  CudaExec ex(handle);
+  rfp::CudaExecT<T> ex(handle);
   return status_of(rfp::plan::spftri(ex, tr, lower, n, arf));
+}
+
+curfpStatus_t curfpSpftri(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, int n, float* arf) {
+  return pftri_impl(handle, transr, uplo, n, arf);
 }
 
 // src/curfp_strttf.cu:420-462 (n == 1 handled by the same kernel).
@@ -440,10 +466,11 @@ curfpStatus_t curfpSsfmmAcc64(curfpHandle_t handle, curfpOperation_t transr,
 // C^T = alpha A B^T + beta C^T on transposed views.  B and C are column-major
 // m x n; the leading dimensions must cover m (the bound the reference's cuBLAS
 // calls enforce).  alpha = 0 reads neither A nor B; beta = 0 does not read C.
-curfpStatus_t curfpSsfmm(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
-                         curfpSideMode_t side, int m, int n, const float* alpha,
-                         const float* arf, const float* B, int ldb, const float* beta,
-                         float* C, int ldc) {
+template <typename T>
+static curfpStatus_t sfmm_impl(curfpHandle_t handle, curfpOperation_t transr,
+                               curfpFillMode_t uplo, curfpSideMode_t side, int m, int n,
+                               const T* alpha, const T* arf, const T* B, int ldb, const T* beta,
+                               T* C, int ldc) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (m < 0 || n < 0 || ldb < 1 || ldc < 1) return CURFP_STATUS_INVALID_VALUE;
   if (!alpha || !beta) return CURFP_STATUS_INVALID_VALUE;
@@ -451,51 +478,66 @@ curfpStatus_t curfpSsfmm(curfpHandle_t handle, curfpOperation_t transr, curfpFil
   if (side != CURFP_SIDE_LEFT && side != CURFP_SIDE_RIGHT) return CURFP_STATUS_INVALID_VALUE;
   if (ldb < m || ldc < m) return CURFP_STATUS_INVALID_VALUE;
   const bool left = side == CURFP_SIDE_LEFT;
-  rfp::View Bv{const_cast<float*>(B), 1, ldb}, Cv{C, 1, ldc};
+  rfp::ViewT<T> Bv{const_cast<T*>(B), 1, ldb}, Cv{C, 1, ldc};
   if (!left) {
     Bv = rfp::tr(Bv);
     Cv = rfp::tr(Cv);
   }
-  CudaExec ex(handle);
+  rfp::CudaExecT<T> ex(handle);
   return status_of(rfp::plan::rfp_symm(ex, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER,
                                        left ? m : n, arf, Bv, Cv, left ? n : m, *alpha,
                                        *beta));
 }
 
+curfpStatus_t curfpSsfmm(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                         curfpSideMode_t side, int m, int n, const float* alpha,
+                         const float* arf, const float* B, int ldb, const float* beta,
+                         float* C, int ldc) {
+  return sfmm_impl(handle, transr, uplo, side, m, n, alpha, arf, B, ldb, beta, C, ldc);
+}
+
 // src/curfp_ssfmv.cpp:134-255: y := alpha A x + beta y.  Increments follow
 // BLAS (a negative increment walks the vector backwards); zero is rejected.
-curfpStatus_t curfpSsfmv(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
-                         int n, const float* alpha, const float* arf, const float* x,
-                         int incx, const float* beta, float* y, int incy) {
+template <typename T>
+static curfpStatus_t sfmv_impl(curfpHandle_t handle, curfpOperation_t transr,
+                               curfpFillMode_t uplo, int n, const T* alpha, const T* arf,
+                               const T* x, int incx, const T* beta, T* y, int incy) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (n < 0) return CURFP_STATUS_INVALID_VALUE;
   if (n == 0) return CURFP_STATUS_SUCCESS;
   if (!alpha || !beta || incx == 0 || incy == 0) return CURFP_STATUS_INVALID_VALUE;
   const int64_t ox = incx < 0 ? -(int64_t)(n - 1) * incx : 0;
   const int64_t oy = incy < 0 ? -(int64_t)(n - 1) * incy : 0;
-  rfp::View X{const_cast<float*>(x) + ox, incx, 1}, Y{y + oy, incy, 1};
-  CudaExec ex(handle);
+  rfp::ViewT<T> X{const_cast<T*>(x) + ox, incx, 1}, Y{y + oy, incy, 1};
+  rfp::CudaExecT<T> ex(handle);
   return status_of(rfp::plan::rfp_symm(ex, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER,
                                        n, arf, X, Y, 1, *alpha, *beta));
 }
 
+curfpStatus_t curfpSsfmv(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                         int n, const float* alpha, const float* arf, const float* x,
+                         int incx, const float* beta, float* y, int incy) {
+  return sfmv_impl(handle, transr, uplo, n, alpha, arf, x, incx, beta, y, incy);
+}
+
 namespace {
-// Shared body of curfpSsfr / curfpSsfr2 (y == nullptr: rank 1).
+// Shared body of the rank-1 / rank-2 updates (y == nullptr: rank 1).
+template <typename T>
 curfpStatus_t rank_update(curfpHandle_t h, curfpOperation_t transr, curfpFillMode_t uplo, int n,
-                          const float* alpha, const float* x, int incx, const float* y,
-                          int incy, float* arf) {
+                          const T* alpha, const T* x, int incx, const T* y, int incy, T* arf) {
   if (!h) return CURFP_STATUS_NOT_INITIALIZED;
   if (n < 0 || !alpha) return CURFP_STATUS_INVALID_VALUE;
-  if (n == 0 || *alpha == 0.0f) return CURFP_STATUS_SUCCESS;
+  if (n == 0 || *alpha == T(0)) return CURFP_STATUS_SUCCESS;
   if (incx == 0 || (y && incy == 0) || !x || !arf) return CURFP_STATUS_INVALID_VALUE;
   Geometry g = rfp::geometry(n, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER);
   rfp::kpack::PackArgs a{};
   const int tiles = rfp::kpack::pack_blocks(g, &a);
-  const float* xb = x + (incx < 0 ? -(int64_t)(n - 1) * incx : 0);
-  const float* yb = y ? y + (incy < 0 ? -(int64_t)(n - 1) * incy : 0) : nullptr;
+  const T* xb = x + (incx < 0 ? -(int64_t)(n - 1) * incx : 0);
+  const T* yb = y ? y + (incy < 0 ? -(int64_t)(n - 1) * incy : 0) : nullptr;
   const double nt = (double)n * (n + 1) / 2;
-  rfp::ProfScope ps(h->prof, h->stream, rfp::K_PACK, (y ? 4.0 : 2.0) * nt, 8.0 * nt);
-  rfp::kpack::rank_update<<<tiles, dim3(rfp::kpack::TX, rfp::kpack::TY), 0, h->stream>>>(
+  rfp::ProfScope ps(h->prof, h->stream, rfp::K_PACK, (y ? 4.0 : 2.0) * nt,
+                    2.0 * sizeof(T) * nt);
+  rfp::kpack::rank_update<T><<<tiles, dim3(rfp::kpack::TX, rfp::kpack::TY), 0, h->stream>>>(
       a, arf, xb, incx, yb, incy, *alpha, y ? 1 : 0);
   ++h->launches;
   return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
@@ -505,7 +547,7 @@ curfpStatus_t rank_update(curfpHandle_t h, curfpOperation_t transr, curfpFillMod
 // src/curfp_ssfr.cpp:99-173: C := alpha x x^T + C (alpha == 0: no-op).
 curfpStatus_t curfpSsfr(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
                         int n, const float* alpha, const float* x, int incx, float* arf) {
-  return rank_update(handle, transr, uplo, n, alpha, x, incx, nullptr, 0, arf);
+  return rank_update<float>(handle, transr, uplo, n, alpha, x, incx, nullptr, 0, arf);
 }
 
 // src/curfp_ssfr2.cpp:94-190: C := alpha (x y^T + y x^T) + C (alpha == 0: no-op).
@@ -513,7 +555,81 @@ curfpStatus_t curfpSsfr2(curfpHandle_t handle, curfpOperation_t transr, curfpFil
                          int n, const float* alpha, const float* x, int incx, const float* y,
                          int incy, float* arf) {
   if (!y && handle && n > 0 && alpha && *alpha != 0.0f) return CURFP_STATUS_INVALID_VALUE;
-  return rank_update(handle, transr, uplo, n, alpha, x, incx, y ? y : x, incy, arf);
+  return rank_update<float>(handle, transr, uplo, n, alpha, x, incx, y ? y : x, incy, arf);
+}
+
+// ---------------------------------------------------------------------------
+// D-prefix (FP64) twins: the same planner and kernels instantiated for
+// double (SIMT DFMA contractions; reference src/curfp_d*.cpp / .cu).
+// ---------------------------------------------------------------------------
+
+curfpStatus_t curfpDsfrk(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                         curfpOperation_t trans, int n, int k, const double* alpha,
+                         const double* A, int lda, const double* beta, double* C) {
+  return ssfrk_impl(handle, transr, uplo, trans, n, k, alpha, A, lda, beta, C, 0);
+}
+
+curfpStatus_t curfpDsfr2k(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                          curfpOperation_t trans, int n, int k, const double* alpha,
+                          const double* A, int lda, const double* B, int ldb,
+                          const double* beta, double* C) {
+  return sfr2k_impl(handle, transr, uplo, trans, n, k, alpha, A, lda, B, ldb, beta, C);
+}
+
+curfpStatus_t curfpDpftrf(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                          int n, double* A, int* info) {
+  return spftrf_impl(handle, transr, uplo, n, A, info, 0);
+}
+
+curfpStatus_t curfpDpftrs(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                          int n, int nrhs, const double* A, double* B, int ldb) {
+  return pftrs_impl(handle, transr, uplo, n, nrhs, A, B, ldb);
+}
+
+curfpStatus_t curfpDpftri(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                          int n, double* arf) {
+  return pftri_impl(handle, transr, uplo, n, arf);
+}
+
+curfpStatus_t curfpDstrttf(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                           int n, const double* A, int lda, double* arf) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (n < 0 || lda < n) return CURFP_STATUS_INVALID_VALUE;
+  if (n == 0) return CURFP_STATUS_SUCCESS;
+  return pack(handle, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER, n, A, arf, lda, 1);
+}
+
+curfpStatus_t curfpDstfttr(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                           int n, const double* arf, double* A, int lda) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (n < 0 || lda < n) return CURFP_STATUS_INVALID_VALUE;
+  if (n == 0) return CURFP_STATUS_SUCCESS;
+  return pack(handle, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER, n, arf, A, lda, 0);
+}
+
+curfpStatus_t curfpDsfmm(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                         curfpSideMode_t side, int m, int n, const double* alpha,
+                         const double* arf, const double* B, int ldb, const double* beta,
+                         double* C, int ldc) {
+  return sfmm_impl(handle, transr, uplo, side, m, n, alpha, arf, B, ldb, beta, C, ldc);
+}
+
+curfpStatus_t curfpDsfmv(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                         int n, const double* alpha, const double* arf, const double* x,
+                         int incx, const double* beta, double* y, int incy) {
+  return sfmv_impl(handle, transr, uplo, n, alpha, arf, x, incx, beta, y, incy);
+}
+
+curfpStatus_t curfpDsfr(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                        int n, const double* alpha, const double* x, int incx, double* arf) {
+  return rank_update<double>(handle, transr, uplo, n, alpha, x, incx, nullptr, 0, arf);
+}
+
+curfpStatus_t curfpDsfr2(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                         int n, const double* alpha, const double* x, int incx, const double* y,
+                         int incy, double* arf) {
+  if (!y && handle && n > 0 && alpha && *alpha != 0.0) return CURFP_STATUS_INVALID_VALUE;
+  return rank_update<double>(handle, transr, uplo, n, alpha, x, incx, y ? y : x, incy, arf);
 }
 
 // ---------------------------------------------------------------------------
@@ -716,4 +832,3 @@ curfpStatus_t curfpGetKernelLaunchCount(curfpHandle_t handle, long long* count) 
   return CURFP_STATUS_SUCCESS;
 }
 
-}  // extern "C"

@@ -31,13 +31,32 @@ constexpr int kThreads = 256;
 struct Stats {
   double sum;          // sum a^2 (norms) or sum |x| (estimator)
   double diag;         // sum of squared diagonal elements
-  unsigned long long key;  // max |a| bits (norms); (|x| bits << 32) | ~index (argmax)
+  unsigned long long key;  // norms: bits of max |a| (float or double)
   unsigned long long colmax;  // max column sum (fixed point, see colsum)
   int mismatch;        // estimator: count of sign(x_i) != isgn_i
-  int pad;
-  float xj;            // estimator: |x[j]| for the caller's previous index j
-  float pad2;
+  int argmax;          // estimator: first index of max |x|
+  double xmax;         // estimator: max |x|
+  double xj;           // estimator: |x[j]| for the caller's previous index j
 };
+
+// Non-negative values order as their bit patterns.
+__device__ __forceinline__ unsigned long long abs_key(float v) {
+  return __float_as_uint(v) & 0x7fffffffu;  // NaN keeps the largest patterns
+}
+__device__ __forceinline__ unsigned long long abs_key(double v) {
+  return (unsigned long long)__double_as_longlong(v) & 0x7fffffffffffffffull;
+}
+// The value of a key (host and device): max |a| as double.
+__host__ __device__ inline double key_value(unsigned long long key, bool is_double) {
+  if (is_double) {
+    union { unsigned long long u; double d; } c;
+    c.u = key;
+    return c.d;
+  }
+  union { unsigned u; float f; } c;
+  c.u = (unsigned)key;
+  return (double)c.f;
+}
 
 constexpr int kMaxParts = 148 * 8;  // grid cap of the flat passes (per-CTA partials)
 
@@ -74,38 +93,48 @@ __device__ __forceinline__ double block_reduce(double s, unsigned long long m, d
   return t;
 }
 
-__device__ __forceinline__ unsigned abs_bits(float v) {
-  return __float_as_uint(v) & 0x7fffffffu;  // NaN keeps the largest patterns
+// One 16-byte vector of elements.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; static constexpr int n = 4; };
+template <> struct Vec16<double> { using type = double2; static constexpr int n = 2; };
+__device__ __forceinline__ void acc_vec(const float4& v, double& s, unsigned long long& m) {
+  s += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
+  const unsigned long long a = max(abs_key(v.x), abs_key(v.y)), b = max(abs_key(v.z), abs_key(v.w));
+  m = max(m, max(a, b));
+}
+__device__ __forceinline__ void acc_vec(const double2& v, double& s, unsigned long long& m) {
+  s += v.x * v.x + v.y * v.y;
+  m = max(m, max(abs_key(v.x), abs_key(v.y)));
 }
 
 // sum a^2 (per-CTA partial into part[blockIdx.x]) and max |a| over the flat
 // array (count elements).  Launch with at most kMaxParts CTAs.
-__global__ void __launch_bounds__(kThreads) flat_stats(const float* __restrict__ a, int64_t count,
+template <typename T>
+__global__ void __launch_bounds__(kThreads) flat_stats(const T* __restrict__ a, int64_t count,
                                                        double* part, Stats* st) {
+  using V = typename Vec16<T>::type;
+  constexpr int VN = Vec16<T>::n;
   double s = 0.0;
-  unsigned m = 0;
+  unsigned long long m = 0;
   const int64_t tid = (int64_t)blockIdx.x * kThreads + threadIdx.x;
   const int64_t stride = (int64_t)gridDim.x * kThreads;
-  const int64_t lead = (int64_t)(((16 - (reinterpret_cast<uintptr_t>(a) & 15)) & 15) >> 2);
+  const int64_t lead =
+      (int64_t)(((16 - (reinterpret_cast<uintptr_t>(a) & 15)) & 15) / sizeof(T));
   const int64_t head = lead < count ? lead : count;
   if (tid < head) {
-    const float v = a[tid];
-    s += (double)v * v;
-    m = max(m, abs_bits(v));
+    const double v = (double)a[tid];
+    s += v * v;
+    m = max(m, abs_key(a[tid]));
   }
-  const int64_t nvec = (count - head) >> 2;
-  const float4* a4 = reinterpret_cast<const float4*>(a + head);
-  for (int64_t e = tid; e < nvec; e += stride) {
-    const float4 v = __ldg(a4 + e);
-    s += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
-    m = max(max(m, abs_bits(v.x)), max(abs_bits(v.y), max(abs_bits(v.z), abs_bits(v.w))));
+  const int64_t nvec = (count - head) / VN;
+  const V* av = reinterpret_cast<const V*>(a + head);
+  for (int64_t e = tid; e < nvec; e += stride) acc_vec(__ldg(av + e), s, m);
+  for (int64_t e = head + VN * nvec + tid; e < count; e += stride) {
+    const double v = (double)a[e];
+    s += v * v;
+    m = max(m, abs_key(a[e]));
   }
-  for (int64_t e = head + 4 * nvec + tid; e < count; e += stride) {
-    const float v = a[e];
-    s += (double)v * v;
-    m = max(m, abs_bits(v));
-  }
-  block_reduce(s, (unsigned long long)m, part + blockIdx.x, &st->key);
+  block_reduce(s, m, part + blockIdx.x, &st->key);
 }
 
 // st->sum := part[0] + ... + part[np - 1] in a fixed order (one CTA).
@@ -118,12 +147,13 @@ __global__ void __launch_bounds__(kThreads) sum_parts(const double* __restrict__
 }
 
 // sum of squared diagonal elements (one CTA, fixed order).
-__global__ void __launch_bounds__(kThreads) diag_sumsq(Geometry g, const float* __restrict__ a,
+template <typename T>
+__global__ void __launch_bounds__(kThreads) diag_sumsq(Geometry g, const T* __restrict__ a,
                                                        Stats* st) {
   double s = 0.0;
   for (int64_t i = threadIdx.x; i < g.n; i += kThreads) {
-    const float v = a[diag_offset(g, i)];
-    s += (double)v * v;
+    const double v = (double)a[diag_offset(g, i)];
+    s += v * v;
   }
   const double t = block_reduce(s, 0ull, nullptr, nullptr);
   if (threadIdx.x == 0) st->diag = t;
@@ -131,11 +161,10 @@ __global__ void __launch_bounds__(kThreads) diag_sumsq(Geometry g, const float* 
 
 // Fixed-point exponent of the column sums: every column sum is at most
 // n max|a| < 2^(e_max), so sums scaled by 2^(62 - e_max) fit in 63 bits.
-__device__ __forceinline__ int colsum_shift(const Stats* st, int n) {
-  const float amax = __uint_as_float((unsigned)st->key);
-  if (!(amax > 0.f) || !(amax <= 3.0e38f)) return 0;  // zero, inf or NaN: handled by the caller
+__host__ __device__ inline int colsum_shift(double amax, int n) {
+  if (!(amax > 0.0) || !(amax <= 1.0e300)) return 0;  // zero, inf or NaN: handled by the caller
   int e;
-  frexp((double)amax * (double)n, &e);  // amax * n < 2^e
+  frexp(amax * (double)n, &e);  // amax * n < 2^e
   return 62 - e;
 }
 
@@ -145,8 +174,9 @@ __device__ __forceinline__ int colsum_shift(const Stats* st, int n) {
 // partial is combined in a fixed order; across tiles the integer atomics are
 // exact, so the result does not depend on scheduling.  col (n words) must
 // start at zero.
+template <typename T>
 __global__ void __launch_bounds__(kpack::TX * kpack::TY) colsum(const kpack::PackArgs args,
-                                                                const float* __restrict__ arf,
+                                                                const T* __restrict__ arf,
                                                                 int n, const Stats* st,
                                                                 unsigned long long* col) {
   using namespace kpack;
@@ -162,7 +192,7 @@ __global__ void __launch_bounds__(kpack::TX * kpack::TY) colsum(const kpack::Pac
   const int p0 = tp * TS, q0 = tq * TS;
   const int prow = B.rows - p0, qcol = B.cols - q0;
   const int64_t P0 = (int64_t)B.p_base + p0, Q0 = (int64_t)B.q_base + q0;
-  const float* base = arf + B.off + (int64_t)p0 * B.rs + (int64_t)q0 * B.cs;
+  const T* base = arf + B.off + (int64_t)p0 * B.rs + (int64_t)q0 * B.cs;
   // warp along the contiguous dimension: lane index L, warp index W
   const bool qc = (B.cs == 1 || B.cs == -1);
   const int64_t sl = qc ? B.cs : B.rs, sw = qc ? B.rs : B.cs;
@@ -175,11 +205,11 @@ __global__ void __launch_bounds__(kpack::TX * kpack::TY) colsum(const kpack::Pac
     for (int h = 0; h < TS / TX; ++h) {
       const int l = tx + TX * h;
       const int lp = qc ? w : l, lq = qc ? l : w;
-      float v = 0.f;
+      double v = 0.0;
       if (lp < prow && lq < qcol && (!B.tri || p0 + lp >= q0 + lq))
-        v = fabsf(base[(int64_t)l * sl + (int64_t)w * sw]);
+        v = fabs((double)base[(int64_t)l * sl + (int64_t)w * sw]);
       // column q gets every element; row p only the off-diagonal ones
-      const float vr = (P0 + lp != Q0 + lq) ? v : 0.f;
+      const double vr = (P0 + lp != Q0 + lq) ? v : 0.0;
       if (qc) { accL[h] += v; accW += vr; }
       else    { accL[h] += vr; accW += v; }
     }
@@ -189,7 +219,7 @@ __global__ void __launch_bounds__(kpack::TX * kpack::TY) colsum(const kpack::Pac
 #pragma unroll
   for (int h = 0; h < TS / TX; ++h) lpart[ty][tx + TX * h] = accL[h];
   __syncthreads();
-  const int shift = colsum_shift(st, n);
+  const int shift = colsum_shift(key_value(st->key, sizeof(T) == 8), n);
   if (lin < 2 * TS) {
     const int i = lin % TS;
     const bool lane_side = lin < TS;  // lane-indexed (L) or warp-indexed (W) partial
@@ -224,58 +254,77 @@ __global__ void __launch_bounds__(kThreads) max_of(const unsigned long long* __r
 // Estimator vectors (one right-hand side, length n)
 // ---------------------------------------------------------------------------
 
-__global__ void fill(float* x, int n, float v) {
+template <typename T>
+__global__ void fill(T* x, int n, T v) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) x[i] = v;
 }
 
 // x := sign(x), isgn := sign(x) (sign(0) = +1)
-__global__ void sign_save(float* x, float* isgn, int n) {
+template <typename T>
+__global__ void sign_save(T* x, T* isgn, int n) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {
-    const float s = x[i] >= 0.f ? 1.f : -1.f;
+    const T s = x[i] >= T(0) ? T(1) : T(-1);
     x[i] = s;
     isgn[i] = s;
   }
 }
 
 // x := e_j (0-based j)
-__global__ void unit(float* x, int n, int j) {
+template <typename T>
+__global__ void unit(T* x, int n, int j) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) x[i] = i == j ? 1.f : 0.f;
+  if (i < n) x[i] = i == j ? T(1) : T(0);
 }
 
 // x_i := (-1)^i (1 + i / (n - 1))   (x_0 = 1 for n = 1)
-__global__ void altsgn(float* x, int n) {
+template <typename T>
+__global__ void altsgn(T* x, int n) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {
-    const float sc = n > 1 ? 1.f + (float)i / (float)(n - 1) : 1.f;
+    const T sc = n > 1 ? T(1) + (T)i / (T)(n - 1) : T(1);
     x[i] = (i & 1) ? -sc : sc;
   }
 }
 
-// sum |x| (FP64), first index of max |x|, the number of i with
-// sign(x_i) != isgn_i (zeros match; isgn may be null) and |x[j]| for the
-// given j.  One CTA, fixed-order sums.
-__global__ void __launch_bounds__(kThreads) vstats(const float* __restrict__ x,
-                                                   const float* __restrict__ isgn, int n, int j,
+// sum |x| (FP64), the first index of max |x| and that maximum, the number of
+// i with sign(x_i) != isgn_i (zeros match; isgn may be null) and |x[j]| for
+// the given j.  One CTA, fixed-order reductions.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) vstats(const T* __restrict__ x,
+                                                   const T* __restrict__ isgn, int n, int j,
                                                    Stats* st) {
-  double s = 0.0;
-  unsigned long long key = 0;
-  int mis = 0;
+  __shared__ double sv[kThreads / 32];
+  __shared__ int si[kThreads / 32];
+  double s = 0.0, best = -1.0;
+  int bi = 0, mis = 0;
   for (int64_t i = threadIdx.x; i < n; i += kThreads) {
-    const float v = x[i];
-    s += fabs((double)v);
-    const unsigned long long k = ((unsigned long long)abs_bits(v) << 32) |
-                                 (unsigned long long)(0xffffffffu - (unsigned)i);
-    key = k > key ? k : key;
-    if (isgn) mis += (v != 0.f && (v > 0.f ? 1.f : -1.f) != isgn[i]);
-    if (i == j) st->xj = fabsf(v);
+    const T v = x[i];
+    const double a = fabs((double)v);
+    s += a;
+    if (a > best) { best = a; bi = (int)i; }  // increasing i: ties keep the first
+    if (isgn) mis += (v != T(0) && (v > T(0) ? T(1) : T(-1)) != isgn[i]);
+    if (i == j) st->xj = a;
   }
-  for (int o = 16; o; o >>= 1) mis += __shfl_xor_sync(0xffffffffu, mis, o);
-  if ((threadIdx.x & 31) == 0 && mis) atomicAdd(&st->mismatch, mis);
-  const double t = block_reduce(s, key, nullptr, &st->key);
-  if (threadIdx.x == 0) st->sum = t;
+  for (int o = 16; o; o >>= 1) {
+    const double b2 = __shfl_xor_sync(0xffffffffu, best, o);
+    const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (b2 > best || (b2 == best && i2 < bi)) { best = b2; bi = i2; }
+    mis += __shfl_xor_sync(0xffffffffu, mis, o);
+  }
+  const int w = threadIdx.x / 32;
+  if ((threadIdx.x & 31) == 0) { sv[w] = best; si[w] = bi; if (mis) atomicAdd(&st->mismatch, mis); }
+  const double t = block_reduce(s, 0ull, nullptr, nullptr);  // synchronises the CTA
+  if (threadIdx.x == 0) {
+    best = sv[0];
+    bi = si[0];
+    for (int k = 1; k < kThreads / 32; ++k)
+      if (sv[k] > best || (sv[k] == best && si[k] < bi)) { best = sv[k]; bi = si[k]; }
+    st->sum = t;
+    st->argmax = bi;
+    st->xmax = best;
+  }
 }
 
 }  // namespace knorm

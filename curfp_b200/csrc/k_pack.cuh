@@ -171,10 +171,11 @@ __global__ void __launch_bounds__(TX * TY) pack_kernel(const PackArgs args,
 //   two = 1:  a(p,q) += x_p (alpha y_q) + y_p (alpha x_q)    (ssfr2, SSYR2 form)
 // x and y element i at x[i * incx] (the caller shifts the base for negative
 // increments).
-static __global__ void __launch_bounds__(TX * TY)
-    rank_update(const PackArgs args, float* arf, const float* __restrict__ x, int64_t incx,
-                const float* __restrict__ y, int64_t incy, float alpha, int two) {
-  __shared__ float xp[TS], xq[TS], yp[TS], yq[TS];
+template <typename T>
+__global__ void __launch_bounds__(TX * TY)
+    rank_update(const PackArgs args, T* arf, const T* __restrict__ x, int64_t incx,
+                const T* __restrict__ y, int64_t incy, T alpha, int two) {
+  __shared__ T xp[TS], xq[TS], yp[TS], yq[TS];
   int t = blockIdx.x, bi = 0;
   while (bi + 1 < args.nblocks && t >= args.b[bi + 1].tile_begin) ++bi;
   const PackBlock& B = args.b[bi];
@@ -185,15 +186,15 @@ static __global__ void __launch_bounds__(TX * TY)
   const int64_t P0 = (int64_t)B.p_base + p0, Q0 = (int64_t)B.q_base + q0;
   const int tx = threadIdx.x, ty = threadIdx.y, lin = ty * TX + tx;
   if (lin < TS) {
-    xp[lin] = lin < prow ? x[(P0 + lin) * incx] : 0.f;
-    xq[lin] = lin < qcol ? alpha * x[(Q0 + lin) * incx] : 0.f;
+    xp[lin] = lin < prow ? x[(P0 + lin) * incx] : T(0);
+    xq[lin] = lin < qcol ? alpha * x[(Q0 + lin) * incx] : T(0);
     if (two) {
-      yp[lin] = lin < prow ? y[(P0 + lin) * incy] : 0.f;
-      yq[lin] = lin < qcol ? alpha * y[(Q0 + lin) * incy] : 0.f;
+      yp[lin] = lin < prow ? y[(P0 + lin) * incy] : T(0);
+      yq[lin] = lin < qcol ? alpha * y[(Q0 + lin) * incy] : T(0);
     }
   }
   __syncthreads();
-  float* base = arf + B.off + (int64_t)p0 * B.rs + (int64_t)q0 * B.cs;
+  T* base = arf + B.off + (int64_t)p0 * B.rs + (int64_t)q0 * B.cs;
   const bool qc = (B.cs == 1 || B.cs == -1);
   const int64_t sl = qc ? B.cs : B.rs, sw = qc ? B.rs : B.cs;
 #pragma unroll
@@ -203,8 +204,8 @@ static __global__ void __launch_bounds__(TX * TY)
       const int l = tx + TX * h, w = ty + TY * r;
       const int lp = qc ? w : l, lq = qc ? l : w;
       if (lp < prow && lq < qcol && (!B.tri || p0 + lp >= q0 + lq)) {
-        float* e = base + (int64_t)l * sl + (int64_t)w * sw;
-        *e = two ? fmaf(yp[lp], xq[lq], fmaf(xp[lp], yq[lq], *e)) : fmaf(xp[lp], xq[lq], *e);
+        T* e = base + (int64_t)l * sl + (int64_t)w * sw;
+        *e = two ? fma(yp[lp], xq[lq], fma(xp[lp], yq[lq], *e)) : fma(xp[lp], xq[lq], *e);
       }
     }
   }

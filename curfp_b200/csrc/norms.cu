@@ -39,17 +39,18 @@ inline bool read_stats(curfpHandle_t h, const Stats* d, Stats* out) {
 
 }  // namespace
 
-extern "C" {
-
-// Reference src/curfp_slansf.cu:280-435: argument checks, n = 0 -> 0, an
-// unknown norm -> INVALID_VALUE.  MAX is the largest |element| of the flat
-// array, FRO = sqrt(2 sum a^2 - sum diag^2), ONE the largest column sum.
-curfpStatus_t curfpSlansf(curfpHandle_t handle, curfpNormType_t norm, curfpOperation_t transr,
-                          curfpFillMode_t uplo, int n, const float* arf, float* result) {
+// Reference src/curfp_slansf.cu:280-435 (and src/curfp_dlansf.cu): argument
+// checks, n = 0 -> 0, an unknown norm -> INVALID_VALUE.  MAX is the largest
+// |element| of the flat array, FRO = sqrt(2 sum a^2 - sum diag^2), ONE the
+// largest column sum.
+template <typename T>
+static curfpStatus_t lansf_impl(curfpHandle_t handle, curfpNormType_t norm,
+                                curfpOperation_t transr, curfpFillMode_t uplo, int n,
+                                const T* arf, T* result) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (!result) return CURFP_STATUS_INVALID_VALUE;
   if (n < 0) return CURFP_STATUS_INVALID_VALUE;
-  *result = 0.0f;
+  *result = T(0);
   if (n == 0) return CURFP_STATUS_SUCCESS;
   if (norm != CURFP_NORM_MAX && norm != CURFP_NORM_ONE && norm != CURFP_NORM_FRO)
     return CURFP_STATUS_INVALID_VALUE;
@@ -69,13 +70,13 @@ curfpStatus_t curfpSlansf(curfpHandle_t handle, curfpNormType_t norm, curfpOpera
     return CURFP_STATUS_EXECUTION_FAILED;
   const int fb = blocks_for((nt + 3) / 4, kMaxParts);
   {
-    rfp::ProfScope ps(handle->prof, s, rfp::K_NORM, 0, 4.0 * (double)nt);
-    flat_stats<<<fb, kThreads, 0, s>>>(arf, nt, part, st);  // max |a| (all norms), sum a^2
+    rfp::ProfScope ps(handle->prof, s, rfp::K_NORM, 0, (double)sizeof(T) * nt);
+    flat_stats<T><<<fb, kThreads, 0, s>>>(arf, nt, part, st);  // max |a| (all norms), sum a^2
     ++handle->launches;
   }
   if (norm == CURFP_NORM_FRO) {
     sum_parts<<<1, kThreads, 0, s>>>(part, fb, st);
-    diag_sumsq<<<1, kThreads, 0, s>>>(g, arf, st);
+    diag_sumsq<T><<<1, kThreads, 0, s>>>(g, arf, st);
     handle->launches += 2;
   } else if (norm == CURFP_NORM_ONE) {
     auto* col = reinterpret_cast<unsigned long long*>(static_cast<char*>(tail) + parts);
@@ -83,72 +84,68 @@ curfpStatus_t curfpSlansf(curfpHandle_t handle, curfpNormType_t norm, curfpOpera
       return CURFP_STATUS_EXECUTION_FAILED;
     rfp::kpack::PackArgs a{};
     const int tiles = rfp::kpack::pack_blocks(g, &a);
-    rfp::ProfScope ps(handle->prof, s, rfp::K_NORM, 0, 4.0 * (double)nt + 16.0 * n);
-    colsum<<<tiles, dim3(rfp::kpack::TX, rfp::kpack::TY), 0, s>>>(a, arf, n, st, col);
+    rfp::ProfScope ps(handle->prof, s, rfp::K_NORM, 0, (double)sizeof(T) * nt + 16.0 * n);
+    colsum<T><<<tiles, dim3(rfp::kpack::TX, rfp::kpack::TY), 0, s>>>(a, arf, n, st, col);
     max_of<<<blocks_for(n, kGridCap), kThreads, 0, s>>>(col, n, st);
     handle->launches += 2;
   }
   if (cudaGetLastError() != cudaSuccess) return CURFP_STATUS_EXECUTION_FAILED;
   Stats hs;
   if (!read_stats(handle, st, &hs)) return CURFP_STATUS_EXECUTION_FAILED;
-  const unsigned mb = (unsigned)hs.key;
-  float amax;
-  std::memcpy(&amax, &mb, sizeof amax);
+  const double amax = key_value(hs.key, sizeof(T) == 8);
   if (norm == CURFP_NORM_MAX) {
-    *result = amax;
+    *result = (T)amax;
   } else if (norm == CURFP_NORM_FRO) {
     const double f2 = 2.0 * hs.sum - hs.diag;
-    *result = f2 > 0.0 ? (float)std::sqrt(f2) : 0.0f;
-    if (!(amax <= 3.0e38f)) *result = amax;  // inf or NaN element
-  } else if (!(amax > 0.0f) || !(amax <= 3.0e38f)) {
-    *result = amax;  // zero matrix (0), inf or NaN element
+    *result = f2 > 0.0 ? (T)std::sqrt(f2) : T(0);
+    if (!(amax <= 1.0e300)) *result = (T)amax;  // inf or NaN element
+  } else if (!(amax > 0.0) || !(amax <= 1.0e300)) {
+    *result = (T)amax;  // zero matrix (0), inf or NaN element
   } else {
-    // the fixed-point scale of colsum_shift
-    int e;
-    std::frexp((double)amax * (double)n, &e);
-    *result = (float)std::ldexp((double)hs.colmax, -(62 - e));
+    *result = (T)std::ldexp((double)hs.colmax, -colsum_shift(amax, n));
   }
   return CURFP_STATUS_SUCCESS;
 }
 
-// Reference src/curfp_spfcon.cu:88-271: LAPACK SLACN2's reverse-communication
-// loop written as a state machine, with A^-T = A^-1 for the SPD matrix so
-// every step applies the same solve.  As there: at most ITMAX = 5
-// iterations, no cycling test (SLACN2's "est <= estold" exit), the
-// convergence test of the e_j loop compares |x| at the previous and the new
-// argmax, and the final alternating-sign vector may raise the estimate.  The
-// repeated-sign test counts sign changes directly (zeros count as matching,
-// as in the reference's dot-product form of the test).  Each step launches
-// one fused statistics kernel and reads back one record.
-curfpStatus_t curfpSpfcon(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
-                          int n, const float* arf, float anorm, float* rcond) {
+// Reference src/curfp_spfcon.cu:88-271 (and src/curfp_dpfcon.cu): LAPACK
+// SLACN2's reverse-communication loop written as a state machine, with A^-T =
+// A^-1 for the SPD matrix so every step applies the same solve.  As there: at
+// most ITMAX = 5 iterations, no cycling test (SLACN2's "est <= estold" exit),
+// the convergence test of the e_j loop compares |x| at the previous and the
+// new argmax, and the final alternating-sign vector may raise the estimate.
+// The repeated-sign test counts sign changes directly (zeros count as
+// matching, as in the reference's dot-product form of the test).  Each step
+// launches one fused statistics kernel and reads back one record.
+template <typename T>
+static curfpStatus_t pfcon_impl(curfpHandle_t handle, curfpOperation_t transr,
+                                curfpFillMode_t uplo, int n, const T* arf, T anorm, T* rcond) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (!rcond) return CURFP_STATUS_INVALID_VALUE;
-  *rcond = 0.0f;
-  if (n == 0 || anorm == 0.0f) return CURFP_STATUS_SUCCESS;
+  *rcond = T(0);
+  if (n == 0 || anorm == T(0)) return CURFP_STATUS_SUCCESS;
   if (n < 0) return CURFP_STATUS_INVALID_VALUE;
   if (!arf) return CURFP_STATUS_INVALID_VALUE;
   const int tr = transr == CURFP_OP_T, lower = uplo == CURFP_FILL_MODE_LOWER;
   void* tail = nullptr;
-  const size_t vec = ((size_t)n * sizeof(float) + 255) & ~(size_t)255;
+  const size_t vec = ((size_t)n * sizeof(T) + 255) & ~(size_t)255;
   Stats* st = scratch(handle, 2 * vec, &tail);
   if (!st) return CURFP_STATUS_ALLOC_FAILED;
-  float* x = static_cast<float*>(tail);
-  float* isgn = reinterpret_cast<float*>(static_cast<char*>(tail) + vec);
+  T* x = static_cast<T*>(tail);
+  T* isgn = reinterpret_cast<T*>(static_cast<char*>(tail) + vec);
   cudaStream_t s = handle->stream;
   using namespace rfp::knorm;
   const int vb = (int)((n + 255) / 256);
   Stats hs;
   auto solve = [&]() -> curfpStatus_t {
-    rfp::CudaExec ex(handle);
+    rfp::CudaExecT<T> ex(handle);
     const int rc = rfp::plan::spftrs(ex, tr, lower, n, 1, arf, x, n);
     return rc == 0 ? CURFP_STATUS_SUCCESS
                    : (rc == 2 ? CURFP_STATUS_ALLOC_FAILED : CURFP_STATUS_EXECUTION_FAILED);
   };
-  auto stats = [&](const float* sg, int j) -> bool {
+  auto stats = [&](const T* sg, int j) -> bool {
     if (cudaMemsetAsync(st, 0, sizeof(Stats), s) != cudaSuccess) return false;
-    rfp::ProfScope ps(handle->prof, s, rfp::K_NORM, 0, 8.0 * n);
-    vstats<<<1, kThreads, 0, s>>>(x, sg, n, j, st);
+    rfp::ProfScope ps(handle->prof, s, rfp::K_NORM, 0, 2.0 * sizeof(T) * n);
+    vstats<T><<<1, kThreads, 0, s>>>(x, sg, n, j, st);
     ++handle->launches;
     return cudaGetLastError() == cudaSuccess && read_stats(handle, st, &hs);
   };
@@ -157,57 +154,53 @@ curfpStatus_t curfpSpfcon(curfpHandle_t handle, curfpOperation_t transr, curfpFi
     return cudaGetLastError() == cudaSuccess;
   };
   const int kItMax = 5;
-  float est = 0.0f;
+  T est = T(0);
   int j = 0, iter = 0, jump = 0;
   for (;;) {
     curfpStatus_t rc;
     switch (jump) {
       case 0:  // x = 1/n
-        fill<<<vb, 256, 0, s>>>(x, n, 1.0f / (float)n);
+        fill<T><<<vb, 256, 0, s>>>(x, n, T(1) / (T)n);
         if (!launched()) return CURFP_STATUS_EXECUTION_FAILED;
         jump = 1;
         break;
       case 1:  // x = A^-1 (1/n)
         if (!stats(nullptr, 0)) return CURFP_STATUS_EXECUTION_FAILED;
-        est = (float)hs.sum;
+        est = (T)hs.sum;
         if (n == 1) goto done;
-        sign_save<<<vb, 256, 0, s>>>(x, isgn, n);
+        sign_save<T><<<vb, 256, 0, s>>>(x, isgn, n);
         if (!launched()) return CURFP_STATUS_EXECUTION_FAILED;
         jump = 2;
         break;
       case 2:  // x = A^-1 sign(x)
         if (!stats(nullptr, 0)) return CURFP_STATUS_EXECUTION_FAILED;
-        j = (int)(0xffffffffu - (unsigned)(hs.key & 0xffffffffu));
+        j = hs.argmax;
         iter = 2;
-        unit<<<vb, 256, 0, s>>>(x, n, j);
+        unit<T><<<vb, 256, 0, s>>>(x, n, j);
         if (!launched()) return CURFP_STATUS_EXECUTION_FAILED;
         jump = 3;
         break;
       case 3:  // x = A^-1 e_j
         if (!stats(isgn, 0)) return CURFP_STATUS_EXECUTION_FAILED;
-        est = (float)hs.sum;
+        est = (T)hs.sum;
         if (hs.mismatch == 0) {  // repeated sign vector: converged
-          altsgn<<<vb, 256, 0, s>>>(x, n);
+          altsgn<T><<<vb, 256, 0, s>>>(x, n);
           jump = 5;
         } else {
-          sign_save<<<vb, 256, 0, s>>>(x, isgn, n);
+          sign_save<T><<<vb, 256, 0, s>>>(x, isgn, n);
           jump = 4;
         }
         if (!launched()) return CURFP_STATUS_EXECUTION_FAILED;
         break;
       case 4: {  // x = A^-1 sign(x)
         if (!stats(nullptr, j)) return CURFP_STATUS_EXECUTION_FAILED;
-        const int jn = (int)(0xffffffffu - (unsigned)(hs.key & 0xffffffffu));
-        unsigned top = (unsigned)(hs.key >> 32);
-        float xnew;
-        std::memcpy(&xnew, &top, sizeof xnew);
-        if (hs.xj != xnew && iter < kItMax) {
-          j = jn;
+        if (hs.xj != hs.xmax && iter < kItMax) {
+          j = hs.argmax;
           ++iter;
-          unit<<<vb, 256, 0, s>>>(x, n, j);
+          unit<T><<<vb, 256, 0, s>>>(x, n, j);
           jump = 3;
         } else {
-          altsgn<<<vb, 256, 0, s>>>(x, n);
+          altsgn<T><<<vb, 256, 0, s>>>(x, n);
           jump = 5;
         }
         if (!launched()) return CURFP_STATUS_EXECUTION_FAILED;
@@ -215,7 +208,7 @@ curfpStatus_t curfpSpfcon(curfpHandle_t handle, curfpOperation_t transr, curfpFi
       }
       default: {  // 5: x = A^-1 altsgn
         if (!stats(nullptr, 0)) return CURFP_STATUS_EXECUTION_FAILED;
-        const float temp = 2.0f * (float)hs.sum / (3.0f * (float)n);
+        const T temp = T(2) * (T)hs.sum / (T(3) * (T)n);
         if (temp > est) est = temp;
         goto done;
       }
@@ -223,8 +216,26 @@ curfpStatus_t curfpSpfcon(curfpHandle_t handle, curfpOperation_t transr, curfpFi
     if ((rc = solve()) != CURFP_STATUS_SUCCESS) return rc;
   }
 done:
-  if (est > 0.0f) *rcond = (1.0f / est) / anorm;
+  if (est > T(0)) *rcond = (T(1) / est) / anorm;
   return CURFP_STATUS_SUCCESS;
 }
 
-}  // extern "C"
+curfpStatus_t curfpSlansf(curfpHandle_t handle, curfpNormType_t norm, curfpOperation_t transr,
+                          curfpFillMode_t uplo, int n, const float* arf, float* result) {
+  return lansf_impl(handle, norm, transr, uplo, n, arf, result);
+}
+
+curfpStatus_t curfpDlansf(curfpHandle_t handle, curfpNormType_t norm, curfpOperation_t transr,
+                          curfpFillMode_t uplo, int n, const double* arf, double* result) {
+  return lansf_impl(handle, norm, transr, uplo, n, arf, result);
+}
+
+curfpStatus_t curfpSpfcon(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                          int n, const float* arf, float anorm, float* rcond) {
+  return pfcon_impl(handle, transr, uplo, n, arf, anorm, rcond);
+}
+
+curfpStatus_t curfpDpfcon(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
+                          int n, const double* arf, double anorm, double* rcond) {
+  return pfcon_impl(handle, transr, uplo, n, arf, anorm, rcond);
+}

@@ -308,6 +308,55 @@ curfpStatus_t curfpSpfcon(curfpHandle_t handle, curfpOperation_t transr,
                           curfpFillMode_t uplo, int n, const float *arf,
                           float anorm, float *rcond);
 
+/* ---------------------------------------------------------------------------
+ * D-prefix (FP64) twins — reference include/curfp.h:357-545.  Same planner
+ * and kernels as the S routines, instantiated for double (SIMT DFMA
+ * contractions), same argument checks and status codes.
+ * ---------------------------------------------------------------------------*/
+curfpStatus_t curfpDsfrk(curfpHandle_t handle, curfpOperation_t transr,
+                         curfpFillMode_t uplo, curfpOperation_t trans, int n,
+                         int k, const double *alpha, const double *A, int lda,
+                         const double *beta, double *C);
+curfpStatus_t curfpDsfr2k(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, curfpOperation_t trans, int n,
+                          int k, const double *alpha, const double *A, int lda,
+                          const double *B, int ldb, const double *beta,
+                          double *C);
+curfpStatus_t curfpDpftrf(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, int n, double *A, int *info);
+curfpStatus_t curfpDpftrs(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, int n, int nrhs, const double *A,
+                          double *B, int ldb);
+curfpStatus_t curfpDpftri(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, int n, double *arf);
+curfpStatus_t curfpDstrttf(curfpHandle_t handle, curfpOperation_t transr,
+                           curfpFillMode_t uplo, int n, const double *A, int lda,
+                           double *arf);
+curfpStatus_t curfpDstfttr(curfpHandle_t handle, curfpOperation_t transr,
+                           curfpFillMode_t uplo, int n, const double *arf,
+                           double *A, int lda);
+curfpStatus_t curfpDsfmm(curfpHandle_t handle, curfpOperation_t transr,
+                         curfpFillMode_t uplo, curfpSideMode_t side, int m, int n,
+                         const double *alpha, const double *arf, const double *B,
+                         int ldb, const double *beta, double *C, int ldc);
+curfpStatus_t curfpDsfmv(curfpHandle_t handle, curfpOperation_t transr,
+                         curfpFillMode_t uplo, int n, const double *alpha,
+                         const double *arf, const double *x, int incx,
+                         const double *beta, double *y, int incy);
+curfpStatus_t curfpDsfr(curfpHandle_t handle, curfpOperation_t transr,
+                        curfpFillMode_t uplo, int n, const double *alpha,
+                        const double *x, int incx, double *arf);
+curfpStatus_t curfpDsfr2(curfpHandle_t handle, curfpOperation_t transr,
+                         curfpFillMode_t uplo, int n, const double *alpha,
+                         const double *x, int incx, const double *y, int incy,
+                         double *arf);
+curfpStatus_t curfpDlansf(curfpHandle_t handle, curfpNormType_t norm,
+                          curfpOperation_t transr, curfpFillMode_t uplo, int n,
+                          const double *arf, double *result);
+curfpStatus_t curfpDpfcon(curfpHandle_t handle, curfpOperation_t transr,
+                          curfpFillMode_t uplo, int n, const double *arf,
+                          double anorm, double *rcond);
+
 /* Release the handle's workspaces (staging planes of the split-BF16 path,
  * refinement and adjoint scratch): waits for the handle's stream, frees every
  * buffer and returns the device pool's unused memory to the driver.  The

@@ -113,3 +113,22 @@ class RefLib:
                                    ctypes.c_void_p(x.data_ptr()), incx,
                                    ctypes.c_void_p(y.data_ptr()), incy,
                                    ctypes.c_void_p(arf.data_ptr()))
+
+    def dsfrk(self, tr, ul, trans, n, k, alpha, A, lda, beta, C):
+        a, b = ctypes.c_double(alpha), ctypes.c_double(beta)
+        return self.lib.curfpDsfrk(self.h, tr, ul, trans, n, k, ctypes.byref(a),
+                                   ctypes.c_void_p(A.data_ptr()), lda, ctypes.byref(b),
+                                   ctypes.c_void_p(C.data_ptr()))
+
+    def dpftrf(self, tr, ul, n, C):
+        info = ctypes.c_int(0)
+        st = self.lib.curfpDpftrf(self.h, tr, ul, n, ctypes.c_void_p(C.data_ptr()),
+                                  ctypes.byref(info))
+        return st, info.value
+
+    def dpftrs(self, tr, ul, n, nrhs, C, B, ldb):
+        return self.lib.curfpDpftrs(self.h, tr, ul, n, nrhs, ctypes.c_void_p(C.data_ptr()),
+                                    ctypes.c_void_p(B.data_ptr()), ldb)
+
+    def dpftri(self, tr, ul, n, C):
+        return self.lib.curfpDpftri(self.h, tr, ul, n, ctypes.c_void_p(C.data_ptr()))

@@ -170,3 +170,38 @@ def test_ssfr_ssfr2_vs_reference(curfp, ref, n, tr, ul):
     curfp.ssfr2(a_our, x, y, alpha=-0.5, transr=TR[tr], uplo=UL[ul])
     torch.cuda.synchronize()
     assert (a_our - a_ref).abs().max().item() <= 2e-6 * a_ref.abs().max().item()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,k", [(65, 32), (1000, 128), (1001, 128)])
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+def test_double_pipeline_vs_reference(curfp, ref, n, k, tr, ul):
+    """The FP64 twins against the reference's own curfpD* routines (cuBLAS /
+    cuSOLVER in FP64) on the same inputs: agreement to FP64 summation-order
+    spread (1e-12 relative on O(1) data, cond ~ 45)."""
+    g = torch.Generator(device="cuda").manual_seed(n + 5 * tr + ul)
+    A = torch.randn(n, k, device="cuda", dtype=torch.float64, generator=g) / k ** 0.5
+    nt = n * (n + 1) // 2
+    C_ref = torch.empty(nt, device="cuda", dtype=torch.float64)
+    C_our = torch.empty_like(C_ref)
+    assert ref.dsfrk(tr, ul, 1, n, k, 1.0, A, k, 0.0, C_ref) == 0
+    curfp.dsfrk(A, C_our, transr=TR[tr], uplo=UL[ul])
+    torch.cuda.synchronize()
+    assert (C_our - C_ref).abs().max().item() <= 1e-13
+    curfp.add_to_diagonal(C_ref, 1.0, transr=TR[tr], uplo=UL[ul])
+    C_our.copy_(C_ref)
+    st, info = ref.dpftrf(tr, ul, n, C_ref)
+    assert st == 0 and info == 0
+    assert curfp.dpftrf(C_our, transr=TR[tr], uplo=UL[ul]) == 0
+    assert ((C_our - C_ref).abs().max() / C_ref.abs().max()).item() <= 1e-12
+    B = torch.randn(8, n, device="cuda", dtype=torch.float64, generator=g)
+    X_ref, X_our = B.clone(), B.clone()
+    assert ref.dpftrs(tr, ul, n, 8, C_ref, X_ref, n) == 0
+    curfp.dpftrs_raw(curfp._get_handle(), tr, ul, n, 8, C_our, X_our, n)
+    torch.cuda.synchronize()
+    assert ((X_our - X_ref).abs().max() / X_ref.abs().max()).item() <= 1e-12
+    I_ref, I_our = C_ref.clone(), C_our.clone()
+    assert ref.dpftri(tr, ul, n, I_ref) == 0
+    curfp.dpftri(I_our, transr=TR[tr], uplo=UL[ul])
+    torch.cuda.synchronize()
+    assert ((I_our - I_ref).abs().max() / I_ref.abs().max()).item() <= 1e-12
