@@ -73,6 +73,7 @@ constexpr int kTrsvMaxRhs = 512; // wavefront solve for at most this many RHS
 constexpr int kTrsvMaxRhsTc = 64;  // ... when the updates may use the tensor cores
 constexpr int kWaveLeaf = 512;   // recursive TRSM hands blocks <= this to the wavefront solve
 constexpr int kWaveLeafWide = 512;  // ... when there are more than 4 * kTrsvMaxRhs RHS
+constexpr int kWaveLeafWideTc = 512;  // ... and the updates may use the tensor cores
 constexpr int kNotSupported = -1;
 
 template <typename T>

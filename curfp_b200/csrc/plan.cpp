@@ -50,7 +50,7 @@ int trsm_rec(ExecT<T>& ex, ViewT<T> L, int n, ViewT<T> B, int m, Scalar<T> alpha
   // Few right-hand sides: the whole block goes to the wavefront solve (its
   // chain is short relative to the work).  Many right-hand sides: small
   // leaves, so that most of the work is in the (tensor-core) GEMM updates.
-  if (n <= (m <= kTrsvMaxRhs * 4 ? kWaveLeaf : kWaveLeafWide)) {
+  if (n <= (m <= kTrsvMaxRhs * 4 ? kWaveLeaf : (math ? kWaveLeafWideTc : kWaveLeafWide))) {
     int rc = ex.trsm_wave(L, n, B, m, alpha, Wb);
     if (rc != kNotSupported) return rc;
   }

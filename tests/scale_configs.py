@@ -17,6 +17,11 @@ Run as a script (pytest does not collect it):
       Precision form at n = 65536, k = 2048, 256 RHS, per shift lambda:
       split-BF16 ssfrk + spftrf + FP64-residual refined spftrs against the
       plain FP32 form, errors against the exact FP64 solution.
+  python tests/scale_configs.py next [--next-n 32768] [--next-nd 16384]
+      The routines beyond the Cholesky path at n = 32768 (slansf, spfcon,
+      ssfmv, ssfmm with 64 RHS, ssfr, ssfr2) and the FP64 twins at n = 16384
+      (dsfrk k = 512, dpftrf, dpftrs with 64 RHS, dpftri), each beside the
+      reference build.
   python tests/scale_configs.py c5
       n = 131072, k = 4096, lambda = 1e-2: split-BF16 ssfrk + spftrf + refined
       spftrs (64 RHS), then the fused GP NLL forward + backward (X = A, s = 1,
@@ -612,6 +617,101 @@ def nll_c5(orc: GramOracle, A, lam, args) -> dict:
     return out
 
 
+# ---------------------------------------------------------------------------
+# The routines beyond the Cholesky path: norms, condition estimate,
+# symmetric multiplies, rank updates, and the FP64 twins
+# ---------------------------------------------------------------------------
+
+def run_next(args):
+    from helpers import REF_LIB, RefLib
+    ours = Ours()
+    ref = RefLib() if REF_LIB.exists() else None
+    lib, h = ours.lib, ours.h.ptr
+    n, k, tr, ul = args.next_n, 1024, 1, 1
+    nt = n * (n + 1) // 2
+    A = gen_A(n, k, seed=n + 3)
+    C = torch.empty(nt, device="cuda")
+    ours.ssfrk(tr, ul, n, k, A, C)
+    ours.add_diag(tr, ul, n, 1.0, C)
+    F = C.clone()
+    ours.spftrf(tr, ul, n, F)
+    W, R = args.warmup, args.reps
+    res = {"config": "next-ops", "n": n, "variant": "TU",
+           "timing": f"warmup {W}, median of {R}", "ops": {}}
+    o = res["ops"]
+    fl = ctypes.c_float(0.0)
+
+    def both(name, ours_fn, ref_fn, flops=None, nbytes=None, prep=None):
+        d = {"ours": rate(cuda_ms(ours_fn, prep, W, R), flops, nbytes)}
+        if ref is not None and ref_fn is not None:
+            d["reference"] = rate(cuda_ms(ref_fn, prep, W, R), flops, nbytes)
+        o[name] = d
+
+    for norm, nm in ((0, "slansf_max"), (1, "slansf_one"), (2, "slansf_fro")):
+        both(nm, lambda: lib.curfpSlansf(h, norm, tr, ul, n, vp(C), ctypes.byref(fl)),
+             (lambda: ref.slansf(norm, tr, ul, n, C)) if ref else None, nbytes=4.0 * nt)
+        o[nm]["value_ours"] = ours.slansf(norm, tr, ul, n, C)
+        if ref:
+            o[nm]["value_reference"] = ref.slansf(norm, tr, ul, n, C)[1]
+    anorm = ours.slansf(1, tr, ul, n, C)
+    both("spfcon", lambda: ours.spfcon(tr, ul, n, F, anorm),
+         (lambda: ref.spfcon(tr, ul, n, F, anorm)) if ref else None)
+    o["spfcon"]["rcond_ours"] = ours.spfcon(tr, ul, n, F, anorm)
+    if ref:
+        o["spfcon"]["rcond_reference"] = ref.spfcon(tr, ul, n, F, anorm)[1]
+    x = torch.randn(n, device="cuda")
+    y = torch.zeros(n, device="cuda")
+    a1, b0 = ctypes.c_float(1.0), ctypes.c_float(0.0)
+    both("ssfmv", lambda: lib.curfpSsfmv(h, tr, ul, n, ctypes.byref(a1), vp(C), vp(x), 1,
+                                        ctypes.byref(b0), vp(y), 1),
+         (lambda: ref.ssfmv(tr, ul, n, 1.0, C, x, 1, 0.0, y, 1)) if ref else None,
+         flops=2.0 * n * n, nbytes=4.0 * nt)
+    Bm = torch.randn(64, n, device="cuda")
+    Ym = torch.zeros(64, n, device="cuda")
+    both("ssfmm_64", lambda: lib.curfpSsfmm(h, tr, ul, 0, n, 64, ctypes.byref(a1), vp(C),
+                                           vp(Bm), n, ctypes.byref(b0), vp(Ym), n),
+         (lambda: ref.ssfmm(tr, ul, 0, n, 64, 1.0, C, Bm, n, 0.0, Ym, n)) if ref else None,
+         flops=2.0 * n * n * 64)
+    Cw = C.clone()
+    both("ssfr", lambda: lib.curfpSsfr(h, tr, ul, n, ctypes.byref(a1), vp(x), 1, vp(Cw)),
+         (lambda: ref.ssfr(tr, ul, n, 1.0, x, 1, Cw)) if ref else None, nbytes=8.0 * nt)
+    both("ssfr2", lambda: lib.curfpSsfr2(h, tr, ul, n, ctypes.byref(a1), vp(x), 1, vp(y), 1,
+                                        vp(Cw)),
+         (lambda: ref.ssfr2(tr, ul, n, 1.0, x, 1, y, 1, Cw)) if ref else None, nbytes=8.0 * nt)
+    del Cw, C, F, A
+    torch.cuda.empty_cache()
+    # FP64 twins
+    nd, kd = args.next_nd, 512
+    ntd = nd * (nd + 1) // 2
+    Ad = gen_A(nd, kd, seed=nd).double()
+    Cd = torch.empty(ntd, device="cuda", dtype=torch.float64)
+    ad, bd = ctypes.c_double(1.0), ctypes.c_double(0.0)
+    info = ctypes.c_int(0)
+    both("dsfrk", lambda: lib.curfpDsfrk(h, tr, ul, 1, nd, kd, ctypes.byref(ad), vp(Ad), kd,
+                                        ctypes.byref(bd), vp(Cd)),
+         (lambda: ref.dsfrk(tr, ul, 1, nd, kd, 1.0, Ad, kd, 0.0, Cd)) if ref else None,
+         flops=nd * (nd + 1) * float(kd))
+    import curfp_b200 as cf
+    cf.add_to_diagonal(Cd, 1.0)
+    Fd = torch.empty_like(Cd)
+    both("dpftrf", lambda: lib.curfpDpftrf(h, tr, ul, nd, vp(Fd), ctypes.byref(info)),
+         (lambda: ref.dpftrf(tr, ul, nd, Fd)) if ref else None, flops=chol_flops(nd),
+         prep=lambda: Fd.copy_(Cd))
+    Fd.copy_(Cd)
+    lib.curfpDpftrf(h, tr, ul, nd, vp(Fd), ctypes.byref(info))
+    Bd = torch.randn(64, nd, device="cuda", dtype=torch.float64)
+    Xd = torch.empty_like(Bd)
+    both("dpftrs_64", lambda: lib.curfpDpftrs(h, tr, ul, nd, 64, vp(Fd), vp(Xd), nd),
+         (lambda: ref.dpftrs(tr, ul, nd, 64, Fd, Xd, nd)) if ref else None,
+         flops=2.0 * nd * nd * 64, prep=lambda: Xd.copy_(Bd))
+    Zd = torch.empty_like(Fd)
+    both("dpftri", lambda: lib.curfpDpftri(h, tr, ul, nd, vp(Zd)),
+         (lambda: ref.dpftri(tr, ul, nd, Zd)) if ref else None, flops=2.0 * nd ** 3 / 3.0,
+         prep=lambda: Zd.copy_(Fd))
+    res["fp64_n"] = nd
+    emit(res, args.out)
+
+
 def nll_exact(orc: GramOracle, y):
     """Exact FP64 loss and gradients (X, s, sigma2) of the GP NLL at X = A,
     s = 1, sigma2 = lam:  alpha = C^-1 y, loss = 1/2 y^T alpha + 1/2 log det C,
@@ -629,7 +729,9 @@ def nll_exact(orc: GramOracle, y):
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("what", choices=["c2", "lapack", "c3", "c5"])
+    ap.add_argument("what", choices=["c2", "lapack", "c3", "c5", "next"])
+    ap.add_argument("--next-n", type=int, default=32768)
+    ap.add_argument("--next-nd", type=int, default=16384)
     ap.add_argument("--n", type=int, nargs="+", default=[32768, 32767])
     ap.add_argument("--variants", default="all")
     ap.add_argument("--lam", type=float, nargs="+", default=[0.1, 0.001])
@@ -647,7 +749,8 @@ def main():
     args = ap.parse_args()
     if args.what != "lapack":
         torch.cuda.init()
-    {"c2": run_c2, "lapack": run_lapack, "c3": run_c3, "c5": run_c5}[args.what](args)
+    {"c2": run_c2, "lapack": run_lapack, "c3": run_c3, "c5": run_c5,
+     "next": run_next}[args.what](args)
 
 
 if __name__ == "__main__":
