@@ -18,7 +18,7 @@ The RFP matrix (2.1 GB) is larger than L2 (126 MB): no extra L2 flush.
       runs one small workload of one kernel family a few times and exits (no
       timing): the commands the ncu summaries under profiles/ were made with.
       Cases: ssfrk-bf16, ssfrk-fp32, chol-bf16, chol-fp32, solve, refine, pack,
-      nll-fused.
+      norms, rank, nll-fused.
 
 --impl reference times the reference's algorithm on the host cores: LAPACK's
 RFP routines (spftrf/spftrs via scipy/OpenBLAS, all threads), which the
@@ -479,7 +479,7 @@ def run_ours(args, rank, world, local):
 
 
 CASES = ("ssfrk-bf16", "ssfrk-fp32", "chol-bf16", "chol-fp32", "solve", "refine", "pack",
-         "nll-fused")
+         "norms", "rank", "nll-fused")
 
 
 def run_case(args):
@@ -537,6 +537,20 @@ def run_case(args):
         for _ in range(reps):
             arf = curfp.strttf(D)
             curfp.stfttr(arf)
+    elif case == "norms":
+        C = spd()
+        prof_on()
+        for _ in range(reps):
+            curfp.slansf(C, "1")
+            curfp.slansf(C, "F")
+    elif case == "rank":
+        C = spd()
+        x = torch.randn(n, device="cuda", generator=g)
+        y = torch.randn(n, device="cuda", generator=g)
+        prof_on()
+        for _ in range(reps):
+            curfp.ssfr(C, x, alpha=1e-3)
+            curfp.ssfr2(C, x, y, alpha=1e-3)
     elif case == "nll-fused":
         X = torch.randn(n, k, device="cuda", generator=g)
         y = torch.randn(n, device="cuda", generator=g)
