@@ -13,6 +13,7 @@
 #include "context.h"
 #include "k_pack.cuh"
 #include "k_refine.cuh"
+#include "k_symv.cuh"
 
 using rfp::CudaExec;
 using rfp::Geometry;
@@ -508,10 +509,21 @@ static curfpStatus_t sfmv_impl(curfpHandle_t handle, curfpOperation_t transr,
   if (!alpha || !beta || incx == 0 || incy == 0) return CURFP_STATUS_INVALID_VALUE;
   const int64_t ox = incx < 0 ? -(int64_t)(n - 1) * incx : 0;
   const int64_t oy = incy < 0 ? -(int64_t)(n - 1) * incy : 0;
-  rfp::ViewT<T> X{const_cast<T*>(x) + ox, incx, 1}, Y{y + oy, incy, 1};
-  rfp::CudaExecT<T> ex(handle);
-  return status_of(rfp::plan::rfp_symm(ex, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER,
-                                       n, arf, X, Y, 1, *alpha, *beta));
+  const int tr = transr == CURFP_OP_T, lower = uplo == CURFP_FILL_MODE_LOWER;
+  if (*alpha == T(0)) {  // y := beta y, neither A nor x read
+    rfp::ViewT<T> X{const_cast<T*>(x) + ox, incx, 1}, Y{y + oy, incy, 1};
+    rfp::CudaExecT<T> ex(handle);
+    return status_of(rfp::plan::rfp_symm(ex, tr, lower, n, arf, X, Y, 1, *alpha, *beta));
+  }
+  const Geometry g = rfp::geometry(n, tr, lower);
+  const double nt = (double)n * (n + 1) / 2;
+  rfp::ProfScope ps(handle->prof, handle->stream, rfp::K_SGEMM, 4.0 * nt,
+                    2.0 * sizeof(T) * nt);
+  rfp::ksymv::symv_rows<T><<<(n + rfp::ksymv::TB - 1) / rfp::ksymv::TB, rfp::ksymv::kThreads, 0,
+                             handle->stream>>>(g, arf, x + ox, incx, y + oy, incy, *alpha,
+                                               *beta);
+  ++handle->launches;
+  return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
 }
 
 curfpStatus_t curfpSsfmv(curfpHandle_t handle, curfpOperation_t transr, curfpFillMode_t uplo,
