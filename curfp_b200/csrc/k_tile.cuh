@@ -66,7 +66,8 @@ static_assert(T == kTrsmLeaf && T == kTriTile, "tile kernels assume one tile siz
 // Lower-triangular Cholesky of an n x n tile (n <= 128), one CTA of 256
 // threads, the tile in shared memory.  Blocked by 32 columns:
 //   (1) warp 0 factors the 32 x 32 diagonal block in registers (lane = row,
-//       pivots broadcast with warp shuffles, no block barrier inside);
+//       pivots broadcast with warp shuffles, warp-uniform control flow, no
+//       block barrier inside);
 //   (2) the rows below solve against it (one thread per row, forward
 //       substitution with broadcast reads of the factor);
 //   (3) all threads apply the rank-32 update to the trailing triangle.
@@ -111,24 +112,27 @@ __global__ void __launch_bounds__(256) potrf_tile(ViewT<E> L, int n, int info_ba
 #pragma unroll
       for (int k = 0; k < 32; ++k) a[k] = (lane < w && k < w) ? s[c0 + lane][c0 + k] : E(0);
       int fail = 0;
+      // The exit tests are warp-uniform (w is, and the pivot test goes
+      // through a vote), so the loop body runs without divergence handling;
+      // the shuffles of one step are issued together before their FMAs.
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
-        if (j < w && !fail) {
-          const E d = __shfl_sync(0xffffffffu, a[j], j);
-          if (!(d > E(0))) {
-            fail = c0 + j + 1;
-          } else {
-            // the column is scaled by multiplication, branch-free across the warp
-            const E r = rsqrt_nr(d);
-            a[j] = (lane == j) ? d * r : (lane > j ? a[j] * r : a[j]);
-            if (lane == j) rdiag[j] = r;
-#pragma unroll
-            for (int k = j + 1; k < 32; ++k) {
-              const E lkj = __shfl_sync(0xffffffffu, a[j], k);
-              if (lane >= k) a[k] = fma(-a[j], lkj, a[k]);
-            }
-          }
+        if (j >= w) break;
+        const E d = __shfl_sync(0xffffffffu, a[j], j);
+        if (__any_sync(0xffffffffu, !(d > E(0)))) {
+          fail = c0 + j + 1;
+          break;
         }
+        // the column is scaled by multiplication, branch-free across the warp
+        const E r = rsqrt_nr(d);
+        a[j] = (lane == j) ? d * r : (lane > j ? a[j] * r : a[j]);
+        if (lane == j) rdiag[j] = r;
+        E lk[32];
+#pragma unroll
+        for (int k = j + 1; k < 32; ++k) lk[k] = __shfl_sync(0xffffffffu, a[j], k);
+#pragma unroll
+        for (int k = j + 1; k < 32; ++k)
+          if (lane >= k) a[k] = fma(-a[j], lk[k], a[k]);
       }
       if (lane < w) {
 #pragma unroll
