@@ -226,23 +226,35 @@ int CudaExecT<T>::lauum_tile(ViewT<T> L, int n) {
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
+namespace {
+// The wavefront solve with NC right-hand-side columns per CTA.
+template <typename T, int NC>
+int launch_wave(curfpContext* ctx, const int* abort_flag, ViewT<T> L, int n, ViewT<T> B, int m,
+                T alpha, const T* W) {
+  const int nblk = (n + ktrsv::NB - 1) / ktrsv::NB, nchunk = (m + NC - 1) / NC;
+  const size_t words = 1 + (size_t)nblk * nchunk;
+  int* sync = static_cast<int*>(grow_buffer(ctx, &ctx->tsv, &ctx->tsv_bytes, words * 4));
+  if (!sync) return 2;
+  if (cudaMemsetAsync(sync, 0, words * 4, ctx->stream) != cudaSuccess) return 4;
+  constexpr int smem = ktrsv::smem_bytes<T, NC>();
+  static const bool attr = smem_attr(ktrsv::trsm_wave<T, NC>, smem);
+  if (!attr) return 4;
+  ProfScope ps(ctx->prof, ctx->stream, K_TRSV, (double)n * n * m,
+               (double)n * n * sizeof(T) / 2.0);
+  ktrsv::trsm_wave<T, NC><<<nblk * nchunk, 256, smem, ctx->stream>>>(L, n, B, m, alpha, W, sync,
+                                                                    ctx->d_info + 1, abort_flag);
+  ++ctx->launches;
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+}  // namespace
+
+// Up to 8 right-hand sides: 8-column chunks (the per-block products of the
+// chain shrink with the chunk); otherwise 64-column chunks.
 template <typename T>
 int CudaExecT<T>::trsm_wave(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const T* W) {
   if (n <= 0 || m <= 0) return 0;
-  const int nblk = (n + ktrsv::NB - 1) / ktrsv::NB, nchunk = (m + ktrsv::NB - 1) / ktrsv::NB;
-  const size_t words = 1 + (size_t)nblk * nchunk;
-  int* sync = static_cast<int*>(grow_buffer(ctx_, &ctx_->tsv, &ctx_->tsv_bytes, words * 4));
-  if (!sync) return 2;
-  if (cudaMemsetAsync(sync, 0, words * 4, ctx_->stream) != cudaSuccess) return 4;
-  constexpr int smem = ktrsv::smem_bytes<T>();
-  static const bool attr = smem_attr(ktrsv::trsm_wave<T>, smem);
-  if (!attr) return 4;
-  ProfScope ps(ctx_->prof, ctx_->stream, K_TRSV, (double)n * n * m,
-               (double)n * n * sizeof(T) / 2.0);
-  ktrsv::trsm_wave<T><<<nblk * nchunk, 256, smem, ctx_->stream>>>(L, n, B, m, alpha, W, sync,
-                                                                 ctx_->d_info + 1, abort_);
-  ++ctx_->launches;
-  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+  if (m <= 8) return launch_wave<T, 8>(ctx_, abort_, L, n, B, m, alpha, W);
+  return launch_wave<T, 64>(ctx_, abort_, L, n, B, m, alpha, W);
 }
 
 template class CudaExecT<float>;

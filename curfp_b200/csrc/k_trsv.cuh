@@ -33,11 +33,26 @@ namespace ktrsv {
 
 constexpr int NB = 64;
 constexpr int LDL = NB + 1;  // L / W / M tiles: scalar reads down a row, conflict-free both ways
-constexpr int LDX = NB + 4;  // X / T tiles: 16-byte reads along a row
 constexpr uint64_t WAIT_NS = 2000000000ull;
+
+// Right-hand-side chunk of one CTA: NC columns, each thread a TR x TC
+// register tile of the 64 x NC block; EPT elements of an X tile per thread;
+// X / T tiles with row stride LDX.  NC = 64 for many right-hand sides, NC = 8
+// for few (a single vector keeps the chain's per-block product small).
+template <int NC> struct Chunk;
+template <> struct Chunk<64> {
+  static constexpr int TR = 4, TC = 4, EPT = 16, LDX = NB + 4;  // 16-byte reads along a row
+};
+template <> struct Chunk<8> {
+  static constexpr int TR = 2, TC = 1, EPT = 2, LDX = 8;
+};
+constexpr int LDX = Chunk<64>::LDX;
+
 // Ls[2], Ws (L tiles; W_j; M_j reuses Ls[0]) and Xs[2], Ts (X tiles; B_jc / T)
-template <typename T>
-constexpr int smem_bytes() { return (3 * NB * LDL + 3 * NB * LDX) * (int)sizeof(T); }
+template <typename T, int NC = 64>
+constexpr int smem_bytes() {
+  return (3 * NB * LDL + 3 * NB * Chunk<NC>::LDX) * (int)sizeof(T);
+}
 constexpr int SMEM = smem_bytes<float>();
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
@@ -83,26 +98,27 @@ __device__ __forceinline__ void load_tile(T* s, ViewT<T> v, int rows, int cols) 
     cp1(s + a * LD + b, ok ? v.p + (int64_t)a * v.rs + (int64_t)b * v.cs : v.p, ok);
   }
 }
-// Tile of B / X (written by CTAs of this launch): L2-only loads into
-// registers (ld.global.cg), stored to shared memory by store_regs.
-template <typename T>
-__device__ __forceinline__ void load_regs(T (&r)[16], ViewT<T> v, int rows, int cols) {
+// Tile of B / X (64 x NC, written by CTAs of this launch): L2-only loads
+// into registers (ld.global.cg), stored to shared memory by store_regs.
+template <int NC, typename T>
+__device__ __forceinline__ void load_regs(T (&r)[Chunk<NC>::EPT], ViewT<T> v, int rows,
+                                          int cols) {
   const bool rowcont = (v.cs == 1 || v.cs == -1) && !(v.rs == 1 || v.rs == -1);
 #pragma unroll
-  for (int u = 0; u < 16; ++u) {
+  for (int u = 0; u < Chunk<NC>::EPT; ++u) {
     const int e = threadIdx.x + 256 * u;
-    const int a = rowcont ? e / NB : e % NB, b = rowcont ? e % NB : e / NB;
+    const int a = rowcont ? e / NC : e % NB, b = rowcont ? e % NC : e / NB;
     r[u] = (a < rows && b < cols) ? __ldcg(v.p + (int64_t)a * v.rs + (int64_t)b * v.cs) : T(0);
   }
 }
-template <typename T>
-__device__ __forceinline__ void store_regs(T* s, const T (&r)[16], ViewT<T> v) {
+template <int NC, typename T>
+__device__ __forceinline__ void store_regs(T* s, const T (&r)[Chunk<NC>::EPT], ViewT<T> v) {
   const bool rowcont = (v.cs == 1 || v.cs == -1) && !(v.rs == 1 || v.rs == -1);
 #pragma unroll
-  for (int u = 0; u < 16; ++u) {
+  for (int u = 0; u < Chunk<NC>::EPT; ++u) {
     const int e = threadIdx.x + 256 * u;
-    const int a = rowcont ? e / NB : e % NB, b = rowcont ? e % NB : e / NB;
-    s[a * LDX + b] = r[u];
+    const int a = rowcont ? e / NC : e % NB, b = rowcont ? e % NC : e / NB;
+    s[a * Chunk<NC>::LDX + b] = r[u];
   }
 }
 // 64 x 64 column-major workspace tile -> s[a][b] (row stride LDL).
@@ -126,20 +142,26 @@ __device__ __forceinline__ void lds4(const double* p, double (&v)[4]) {
 }
 // acc (+)= sign * A(64 x 64, row stride LDL) * X(64 x 64, row stride LDX) on
 // the thread's 4 x 4 register tile (rows tr*4.., columns tc*4..).
-template <bool kSub, typename T>
-__device__ __forceinline__ void tile_mma(T (&acc)[4][4], const T* A, const T* X, int tr,
-                                         int tc) {
+template <bool kSub, int NC, typename T>
+__device__ __forceinline__ void tile_mma(T (&acc)[Chunk<NC>::TR][Chunk<NC>::TC], const T* A,
+                                         const T* X, int tr, int tc) {
+  constexpr int TR = Chunk<NC>::TR, TC = Chunk<NC>::TC, LX = Chunk<NC>::LDX;
 #pragma unroll 8
   for (int k = 0; k < NB; ++k) {
-    T a4[4], x4[4];
+    T a[TR], x[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) a4[q] = A[(tr * 4 + q) * LDL + k];
-    lds4(X + k * LDX + tc * 4, x4);
+    for (int q = 0; q < TR; ++q) a[q] = A[(tr * TR + q) * LDL + k];
+    if constexpr (TC == 4) {
+      lds4(X + k * LX + tc * 4, x);
+    } else {
 #pragma unroll
-    for (int p = 0; p < 4; ++p)
+      for (int q = 0; q < TC; ++q) x[q] = X[k * LX + tc * TC + q];
+    }
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        acc[p][q] = kSub ? fma(-a4[p], x4[q], acc[p][q]) : fma(a4[p], x4[q], acc[p][q]);
+    for (int p = 0; p < TR; ++p)
+#pragma unroll
+      for (int q = 0; q < TC; ++q)
+        acc[p][q] = kSub ? fma(-a[p], x[q], acc[p][q]) : fma(a[p], x[q], acc[p][q]);
   }
 }
 
@@ -162,45 +184,47 @@ __device__ __forceinline__ int wait_flag(const int* f, int* err) {
 // block row b, chunk c (0 = not ready, 1 = ready, -1 = poisoned).
 // All zero at launch.  W: kInvStride elements per block row ([W_j | M_j]).
 // FP32: two CTAs per SM (102 KB of shared memory each); FP64: one (204 KB).
-template <typename T>
+template <typename T, int NC = 64>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     trsm_wave(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const T* __restrict__ W,
               int* sync, int* err, const int* abort_flag) {
+  constexpr int TR = Chunk<NC>::TR, TC = Chunk<NC>::TC, EPT = Chunk<NC>::EPT;
+  constexpr int LX = Chunk<NC>::LDX;
   extern __shared__ __align__(16) unsigned char dyn_tsv_raw[];
   T* Ls0 = reinterpret_cast<T*>(dyn_tsv_raw);
   T* Ls1 = Ls0 + NB * LDL;
   T* Ws = Ls1 + NB * LDL;
   T* Xs0 = Ws + NB * LDL;
-  T* Xs1 = Xs0 + NB * LDX;
-  T* Ts = Xs1 + NB * LDX;
+  T* Xs1 = Xs0 + NB * LX;
+  T* Ts = Xs1 + NB * LX;
   __shared__ int sh_ticket, sh_state, sh_ready[2], sh_last;
   if (abort_flag && *abort_flag != INT_MAX) return;
   const int tid = threadIdx.x;
-  const int nchunk = (m + NB - 1) / NB;
+  const int nchunk = (m + NC - 1) / NC;
   if (tid == 0) sh_ticket = atomicAdd(sync, 1);
   __syncthreads();
   const int t = sh_ticket;
   const int j = t / nchunk, c = t % nchunk;
-  const int r0 = j * NB, c0 = c * NB;
-  const int rows = min(NB, n - r0), cols = min(NB, m - c0);
-  const int tr = tid / 16, tc = tid % 16;  // 4 x 4 register tile
+  const int r0 = j * NB, c0 = c * NC;
+  const int rows = min(NB, n - r0), cols = min(NC, m - c0);
+  const int tr = tid / (NC / TC), tc = tid % (NC / TC);  // TR x TC register tile
   int* flags = sync + 1;
   const ViewT<T> Bt = sub(B, r0, c0);
   const T* Wj = W + (int64_t)j * kInvStride;
   auto xview = [&](int i) { return sub(B, (int64_t)i * NB, c0); };
   auto lview = [&](int i) { return sub(L, r0, (int64_t)i * NB); };
 
-  T acc[4][4];
+  T acc[TR][TC];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < TR; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+    for (int b = 0; b < TC; ++b) acc[a][b] = T(0);
 
   // Loads that depend on no other CTA: W_j, B_jc, the first L tile.
-  T xr[16];
+  T xr[EPT];
   load_ws(Ws, Wj);
-  load_regs(xr, Bt, rows, cols);
-  store_regs(Ts, xr, Bt);
+  load_regs<NC>(xr, Bt, rows, cols);
+  store_regs<NC>(Ts, xr, Bt);
   const int iend = j - 1;  // products in the loop: i < iend
   bool poisoned = false;
   if (iend > 0) {
@@ -210,8 +234,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     if (sh_state < 0) {
       poisoned = true;
     } else {
-      load_regs(xr, xview(0), NB, cols);
-      store_regs(Xs0, xr, xview(0));
+      load_regs<NC>(xr, xview(0), NB, cols);
+      store_regs<NC>(Xs0, xr, xview(0));
     }
   }
   cp_commit();
@@ -228,8 +252,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     const bool ready = more && sh_ready[i & 1] > 0;
     if (more) load_tile<LDL>(Ln, lview(i + 1), rows, NB);
     cp_commit();
-    if (ready) load_regs(xr, xview(i + 1), NB, cols);
-    tile_mma<false>(acc, Lb, Xb, tr, tc);
+    if (ready) load_regs<NC>(xr, xview(i + 1), NB, cols);
+    tile_mma<false, NC>(acc, Lb, Xb, tr, tc);
     if (more) {
       if (!ready) {
         if (tid == 0) sh_state = wait_flag(&flags[(i + 1) * nchunk + c], err);
@@ -238,9 +262,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
           poisoned = true;
           break;
         }
-        load_regs(xr, xview(i + 1), NB, cols);
+        load_regs<NC>(xr, xview(i + 1), NB, cols);
       }
-      store_regs(Xn, xr, xview(i + 1));
+      store_regs<NC>(Xn, xr, xview(i + 1));
     }
   }
   if (poisoned) {
@@ -258,17 +282,17 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
   const bool ready = j > 0 && sh_last > 0;
   if (j > 0) load_ws(Ls0, Wj + NB * NB);
   cp_commit();
-  if (ready) load_regs(xr, xview(j - 1), NB, cols);
+  if (ready) load_regs<NC>(xr, xview(j - 1), NB, cols);
 #pragma unroll
-  for (int p = 0; p < 4; ++p)
+  for (int p = 0; p < TR; ++p)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      T* tp = Ts + (tr * 4 + p) * LDX + tc * 4 + q;
+    for (int q = 0; q < TC; ++q) {
+      T* tp = Ts + (tr * TR + p) * LX + tc * TC + q;
       *tp = fma(alpha, *tp, -acc[p][q]);
       acc[p][q] = T(0);
     }
   __syncthreads();
-  tile_mma<false>(acc, Ws, Ts, tr, tc);
+  tile_mma<false, NC>(acc, Ws, Ts, tr, tc);
   if (j > 0) {
     if (!ready) {
       if (tid == 0) sh_state = wait_flag(&flags[(j - 1) * nchunk + c], err);
@@ -279,18 +303,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
         if (tid == 0) st_release(&flags[j * nchunk + c], -1);
         return;
       }
-      load_regs(xr, xview(j - 1), NB, cols);
+      load_regs<NC>(xr, xview(j - 1), NB, cols);
     }
-    store_regs(Xs0, xr, xview(j - 1));
+    store_regs<NC>(Xs0, xr, xview(j - 1));
     cp_wait_all();
     __syncthreads();
-    tile_mma<true>(acc, Ls0, Xs0, tr, tc);  // X_j = Y - M_j X_{j-1}
+    tile_mma<true, NC>(acc, Ls0, Xs0, tr, tc);  // X_j = Y - M_j X_{j-1}
   }
 #pragma unroll
-  for (int p = 0; p < 4; ++p)
+  for (int p = 0; p < TR; ++p)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int a = tr * 4 + p, b = tc * 4 + q;
+    for (int q = 0; q < TC; ++q) {
+      const int a = tr * TR + p, b = tc * TC + q;
       if (a < rows && b < cols) Bt.p[(int64_t)a * Bt.rs + (int64_t)b * Bt.cs] = acc[p][q];
     }
   __threadfence();
