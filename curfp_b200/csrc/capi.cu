@@ -516,13 +516,18 @@ static curfpStatus_t sfmv_impl(curfpHandle_t handle, curfpOperation_t transr,
     return status_of(rfp::plan::rfp_symm(ex, tr, lower, n, arf, X, Y, 1, *alpha, *beta));
   }
   const Geometry g = rfp::geometry(n, tr, lower);
+  const rfp::ksymv::Parts P = rfp::ksymv::parts(n);
+  T* part = static_cast<T*>(rfp::grow_buffer(handle, &handle->ws, &handle->ws_bytes,
+                                             (size_t)(P.n_row + P.n_col) * sizeof(T)));
+  if (!part) return CURFP_STATUS_ALLOC_FAILED;
   const double nt = (double)n * (n + 1) / 2;
-  rfp::ProfScope ps(handle->prof, handle->stream, rfp::K_SGEMM, 4.0 * nt,
-                    2.0 * sizeof(T) * nt);
-  rfp::ksymv::symv_rows<T><<<(n + rfp::ksymv::TB - 1) / rfp::ksymv::TB, rfp::ksymv::kThreads, 0,
-                             handle->stream>>>(g, arf, x + ox, incx, y + oy, incy, *alpha,
-                                               *beta);
-  ++handle->launches;
+  rfp::ProfScope ps(handle->prof, handle->stream, rfp::K_SGEMM, 4.0 * nt, sizeof(T) * nt);
+  rfp::ksymv::symv_tiles<T>
+      <<<(unsigned)rfp::ksymv::strips_before(P.tiles), rfp::ksymv::kThreads, 0, handle->stream>>>(
+          g, arf, x + ox, incx, part);
+  rfp::ksymv::symv_reduce<T><<<P.tiles, rfp::ksymv::kThreads, 0, handle->stream>>>(
+      n, part, y + oy, incy, *alpha, *beta);
+  handle->launches += 2;
   return ok_launch() ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
 }
 

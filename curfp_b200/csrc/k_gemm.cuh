@@ -6,7 +6,7 @@
 // contiguous one, so RFP blocks (T1, S, T2 in any of the 8 variants, their
 // transposes and their index reversals) are addressed in place, never
 // unpacked.  One CTA computes a BM x BN tile with 256 threads, each holding a
-// (BM/16) x (BN/16) register tile; A and B tiles of depth 16 are loaded into
+// (BM/16) x (BN/16) register tile; A and B tiles of depth 8-32 are loaded into
 // registers one tile ahead (float4 loads where the operand's unit stride,
 // base and other stride allow it -- RFP leading dimensions are often odd --
 // scalar loads with zero fill otherwise) and stored to double-buffered,
@@ -66,11 +66,13 @@ __device__ __forceinline__ void tile_coords(const Prob<T>& P, int lt, int& ti,
 // for A, n for B).  Groups of 4 consecutive r are permuted within aligned
 // groups of 8 by kk: the inner loop still reads aligned float4 runs, and the
 // transposing stores of k-contiguous operands hit 32 distinct banks (depth
-// 16: 4 threads per row, 8 rows per warp, col4 ^ 2*((kk>>2)&3); depth 8: 2
-// threads per row, 16 rows per warp, col4 ^ 4*((kk>>2)&1)).
+// 32: 8 threads per row, 4 rows per warp, col4 ^ ((kk>>2)&7); depth 16: 4
+// threads per row, 8 rows per warp, col4 ^ 2*((kk>>2)&3); depth 8: 2 threads
+// per row, 16 rows per warp, col4 ^ 4*((kk>>2)&1)).
 template <int BK>
 __device__ __forceinline__ int swz(int r, int kk) {
-  const int h = BK == 8 ? (((kk >> 2) & 1) << 2) : (((kk >> 2) & 3) << 1);
+  const int h = BK == 8 ? (((kk >> 2) & 1) << 2)
+                        : (BK == 16 ? (((kk >> 2) & 3) << 1) : ((kk >> 2) & 7));
   return (((r >> 2) ^ h) << 2) | (r & 3);
 }
 
@@ -194,8 +196,9 @@ __global__ void __launch_bounds__(kThreads, 2) sgemm_batch(const Batch<T> batch)
   constexpr int TM = BM / 16, TN = BN / 16;
   constexpr int GM = TM / 4, GN = TN / 4;
   // depth 8 for the 128 x 128 tile keeps the register staging within the
-  // 128-register budget of two CTAs per SM
-  constexpr int BK = BM >= 128 ? 8 : 16;
+  // 128-register budget of two CTAs per SM; the FP32 64 x 64 tile takes 32
+  // (its FMAs per k-tile then cover the global-load latency of the next one)
+  constexpr int BK = BM >= 128 ? 8 : (sizeof(T) == 4 ? 32 : 16);
   __shared__ __align__(16) T sa[2][BK][BM];
   __shared__ __align__(16) T sb[2][BK][BN];
 

@@ -1,16 +1,28 @@
 // k_symv.cuh — y := alpha A x + beta y for a symmetric A held in RFP (any
 // variant), one right-hand side (ssfmv / dsfmv).
 //
-// Bandwidth-bound: each CTA owns 64 rows of y and sweeps the 64-wide column
-// blocks; the 64 x 64 tile (rows i0.., columns j0..) of the symmetric matrix
-// is read through the RFP block that stores it, with the warp along the
-// block's contiguous dimension, so the reads coalesce (each stored element is
-// read twice over the launch, once per symmetric half).  A tile that lies in
-// one RFP block and off the diagonal is addressed by a base pointer and two
-// strides; the diagonal tiles (and any tile across the n1 boundary) take
-// per-element offsets.  Products are summed in the element type in a fixed
-// order (registers, then a fixed-order combine through shared memory): the
-// result is bitwise repeatable.
+// Bandwidth-bound, and every stored element is read exactly once.  The
+// logical lower triangle is cut into 64 x 64 tiles (I >= J).  A tile (I, J)
+// feeds both halves of the symmetric product: its rows, A_IJ x_J -> y_I, and
+// its columns, A_IJ^T x_I -> y_J.  CTA (I, s) walks the strip of up to S
+// tiles J in [sS, sS + S) of tile row I:
+//   * the row products of its tiles accumulate in registers and leave as one
+//     64-vector per strip (row_part[I][s]);
+//   * the column products leave as one 64-vector per tile
+//     (col_part[J][I - J]; the diagonal tile contributes its strictly lower
+//     part here and its lower part, diagonal included, to the row product).
+// symv_reduce then forms y_J = alpha (sum_s row_part[J][s] + sum_I
+// col_part[J][I - J]) + beta y_J.  Partials are written once and summed in a
+// fixed order (registers, shuffle butterflies whose tree is the same in every
+// lane, fixed-order combines through shared memory): the result is bitwise
+// repeatable.  The partials take n^2 / 128 + n^2 / (64 S) elements.
+//
+// Tile reads follow the contiguous dimension of the RFP block that stores the
+// tile: "row-fast" tiles (unit stride along i) put lanes on rows l, l + 32
+// and warps on 8 columns each, "column-fast" tiles the transpose; a warp
+// load is 32 consecutive elements either way.  Diagonal tiles and tiles
+// across the n1 boundary take per-element offsets.  The next tile's elements
+// are loaded while the current one is reduced.
 #pragma once
 #include <cstdint>
 
@@ -19,120 +31,256 @@
 namespace rfp {
 namespace ksymv {
 
-constexpr int TB = 64;
+constexpr int TB = 64;        // tile edge
+constexpr int S = 16;         // tiles per strip
 constexpr int kThreads = 256;
 
-// x[j0 .. j0 + 15] (BLAS increment inc, zero past n): four 16-byte loads when
-// the run is contiguous and aligned.
-__device__ __forceinline__ void load16(const float* x, int j0, int64_t inc, int n,
-                                       float (&v)[16]) {
-  const float* p = x + (int64_t)j0 * inc;
-  if (inc == 1 && j0 + 16 <= n && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const float4 w = __ldg(reinterpret_cast<const float4*>(p) + q);
-      v[4 * q] = w.x; v[4 * q + 1] = w.y; v[4 * q + 2] = w.z; v[4 * q + 3] = w.w;
-    }
-  } else {
-#pragma unroll
-    for (int r = 0; r < 16; ++r) v[r] = j0 + r < n ? __ldg(p + r * inc) : 0.f;
-  }
+// Layout of the partials for T = ceil(n / 64) tile rows.
+struct Parts {
+  int tiles;      // T
+  int strips;     // ceil(T / S): row_part stride per tile row
+  int64_t n_row;  // T * strips * 64 elements
+  int64_t n_col;  // T (T + 1) / 2 * 64 elements
+};
+RFP_HD Parts parts(int n) {
+  Parts p;
+  p.tiles = (n + TB - 1) / TB;
+  p.strips = (p.tiles + S - 1) / S;
+  p.n_row = (int64_t)p.tiles * p.strips * TB;
+  p.n_col = (int64_t)p.tiles * (p.tiles + 1) / 2 * TB;
+  return p;
 }
-__device__ __forceinline__ void load16(const double* x, int j0, int64_t inc, int n,
-                                       double (&v)[16]) {
-  const double* p = x + (int64_t)j0 * inc;
-  if (inc == 1 && j0 + 16 <= n && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+// Strips over tile rows 0 .. I-1: sum_{i < I} (floor(i / S) + 1).
+RFP_HD int64_t strips_before(int64_t I) {
+  const int64_t q = I / S, r = I - q * S;
+  return I + S * q * (q - 1) / 2 + q * r;
+}
+// First col_part entry of tile column J: sum_{j < J} (T - j).
+RFP_HD int64_t col_base(int64_t J, int64_t T) { return J * T - J * (J - 1) / 2; }
+
+enum : int { kRowFast = 0, kColFast = 1, kSlow = 2 };
+
+// Sum over the 32 lanes of 8 values: returns, in lane L, the total of value
+// L >> 2 (reduce-scatter halving the values per step, then two exchanges).
+template <typename E>
+__device__ __forceinline__ E warp_sum8(E (&v)[8], int lane) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const double2 w = __ldg(reinterpret_cast<const double2*>(p) + q);
-      v[2 * q] = w.x; v[2 * q + 1] = w.y;
-    }
-  } else {
-#pragma unroll
-    for (int r = 0; r < 16; ++r) v[r] = j0 + r < n ? __ldg(p + r * inc) : 0.0;
+  for (int q = 0; q < 4; ++q) {  // lanes with bit 4 keep values 4..7
+    const bool hi = lane & 16;
+    const E send = hi ? v[q] : v[q + 4], keep = hi ? v[q + 4] : v[q];
+    v[q] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
   }
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {  // bit 3 keeps values 2, 3 of the four
+    const bool hi = lane & 8;
+    const E send = hi ? v[q] : v[q + 2], keep = hi ? v[q + 2] : v[q];
+    v[q] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  {
+    const bool hi = lane & 4;
+    const E send = hi ? v[0] : v[1], keep = hi ? v[1] : v[0];
+    v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  E s = v[0];
+  s += __shfl_xor_sync(0xffffffffu, s, 2);
+  s += __shfl_xor_sync(0xffffffffu, s, 1);
+  return s;  // value index (bit4 << 2) | (bit3 << 1) | bit2 = lane >> 2
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kThreads)
-    symv_rows(Geometry g, const T* __restrict__ arf, const T* __restrict__ x, int64_t incx,
-              T* y, int64_t incy, T alpha, T beta) {
+template <typename E>
+struct Tile {
+  E v[16];   // row-fast / slow: v[8a + b] = (row l + 32a, col 8w + b);
+             // column-fast: v[8a + b] = (row 8w + b, col l + 32a)
+  int kind;
+};
+
+// Tile (I, J) of the logical lower triangle into registers (zero outside
+// the matrix; the diagonal tile keeps i >= j).
+template <typename E>
+__device__ __forceinline__ void load_tile(const Geometry& g, const E* __restrict__ arf, int I,
+                                          int J, int lane, int w, Tile<E>& t) {
   const int n = g.n;
-  const int i0 = blockIdx.x * TB;
-  const int tid = threadIdx.x, tl = tid % TB, tg = tid / TB;  // tg in 0..3
-  T acc_row = T(0);        // warp along i: this thread's row tl
-  T acc_rows[16];          // warp along j: rows 16 tg + r
+  const int64_t i0 = (int64_t)I * TB, j0 = (int64_t)J * TB;
+  const int64_t im = min((int64_t)n - 1, i0 + TB - 1), jm = min((int64_t)n - 1, j0 + TB - 1);
+  const bool one_block = (i0 < g.n1) == (im < g.n1) && (j0 < g.n1) == (jm < g.n1);
+  if (I != J && one_block) {
+    const BlockGeom& bg = j0 < g.n1 ? (i0 < g.n1 ? g.b11 : g.b21) : g.b22;
+    const int64_t ib = i0 < g.n1 ? 0 : g.n1, jb = j0 < g.n1 ? 0 : g.n1;
+    const E* base = arf + bg.off + (i0 - ib) * bg.rs + (j0 - jb) * bg.cs;
+    if (bg.rs == 1 || bg.rs == -1) {
+      t.kind = kRowFast;
 #pragma unroll
-  for (int r = 0; r < 16; ++r) acc_rows[r] = T(0);
-
-  for (int j0 = 0; j0 < n; j0 += TB) {
-    const bool lower = i0 >= j0;
-    const int64_t pb = lower ? i0 : j0, qb = lower ? j0 : i0;
-    const int64_t pm = min((int64_t)n - 1, pb + TB - 1), qm = min((int64_t)n - 1, qb + TB - 1);
-    const bool one_block = (pb < g.n1) == (pm < g.n1) && (qb < g.n1) == (qm < g.n1);
-    if (i0 != j0 && one_block) {
-      const BlockGeom& bg = qb < g.n1 ? (pb < g.n1 ? g.b11 : g.b21) : g.b22;
-      const int64_t pbase = pb < g.n1 ? 0 : g.n1, qbase = qb < g.n1 ? 0 : g.n1;
-      const T* base = arf + bg.off + (pb - pbase) * bg.rs + (qb - qbase) * bg.cs;
-      // element (li, lj) of the tile: lower tile (p, q) = (i, j), upper (j, i)
-      const int64_t s_li = lower ? bg.rs : bg.cs, s_lj = lower ? bg.cs : bg.rs;
-      const bool i_fast = (s_li == 1 || s_li == -1);
-      if (i_fast) {  // this thread: row tl, the 16 consecutive columns 16 tg + r
-        const bool row_ok = i0 + tl < n;
-        const int jb = j0 + 16 * tg;
-        T xs[16];
-        load16(x, jb, incx, n, xs);
-        T s = T(0);
+      for (int a = 0; a < 2; ++a)
 #pragma unroll
-        for (int r = 0; r < 16; ++r) {
-          if (row_ok && jb + r < n)
-            s = fma(base[(int64_t)tl * s_li + (int64_t)(16 * tg + r) * s_lj], xs[r], s);
+        for (int b = 0; b < 8; ++b) {
+          const int64_t li = lane + 32 * a, lj = 8 * w + b;
+          t.v[8 * a + b] = (i0 + li < n && j0 + lj < n) ? __ldg(base + li * bg.rs + lj * bg.cs)
+                                                         : E(0);
         }
-        acc_row += s;
-      } else {  // this thread: column tl, the 16 consecutive rows 16 tg + r
-        const bool col_ok = j0 + tl < n;
-        const T xv = col_ok ? x[(j0 + tl) * incx] : T(0);
+    } else {
+      t.kind = kColFast;
 #pragma unroll
-        for (int r = 0; r < 16; ++r) {
-          const int li = 16 * tg + r;
-          if (col_ok && i0 + li < n)
-            acc_rows[r] = fma(base[(int64_t)li * s_li + (int64_t)tl * s_lj], xv, acc_rows[r]);
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+          const int64_t li = 8 * w + b, lj = lane + 32 * a;
+          t.v[8 * a + b] = (i0 + li < n && j0 + lj < n) ? __ldg(base + li * bg.rs + lj * bg.cs)
+                                                         : E(0);
         }
-      }
-    } else {  // diagonal tile or a tile across the n1 boundary
-      const int64_t i = i0 + tl;
-      T s = T(0);
-#pragma unroll 4
-      for (int r = 0; r < 16; ++r) {
-        const int64_t j = j0 + 16 * tg + r;
-        if (i < n && j < n)
-          s = fma(arf[i >= j ? lower_offset(g, i, j) : lower_offset(g, j, i)], x[j * incx], s);
-      }
-      acc_row += s;
     }
-  }
-
-  // Fixed-order combine: row li gets the four acc_row of threads (li, tg) and
-  // the 64 acc_rows[li % 16] of the threads with tg == li / 16.
-  __shared__ T part_a[4][TB];
-  __shared__ T part_b[2 * 4][16];  // [warp][r]: one partial per warp of each row group
-  part_a[tg][tl] = acc_row;
-  const int warp = tid / 32, lane = tid % 32;
+  } else {
+    t.kind = kSlow;
 #pragma unroll
-  for (int r = 0; r < 16; ++r) {
-    T v = acc_rows[r];
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) part_b[warp][r] = v;
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const int64_t i = i0 + lane + 32 * a, j = j0 + 8 * w + b;
+        t.v[8 * a + b] = (i < n && j < n && i >= j) ? __ldg(arf + lower_offset(g, i, j)) : E(0);
+      }
   }
+}
+
+template <typename E>
+__device__ __forceinline__ E xval(const E* __restrict__ x, int64_t inc, int64_t i, int n) {
+  return i < n ? __ldg(x + i * inc) : E(0);
+}
+
+// grid: strips_before(T) CTAs; part: [row_part | col_part] (parts(n)).
+template <typename E>
+__global__ void __launch_bounds__(kThreads)
+    symv_tiles(Geometry g, const E* __restrict__ arf, const E* __restrict__ x, int64_t incx,
+               E* __restrict__ part) {
+  const int n = g.n;
+  const Parts P = parts(n);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  // (I, s) of this CTA: the largest I with strips_before(I) <= blockIdx.x
+  int lo = 0, hi = P.tiles - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (strips_before(mid) <= (int64_t)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const int I = lo;
+  const int s = (int)((int64_t)blockIdx.x - strips_before(I));
+  const int Jb = s * S, Je = min(Jb + S, I + 1);
+  const int64_t i0 = (int64_t)I * TB;
+  E* row_part = part + ((int64_t)I * P.strips + s) * TB;
+  E* col_part = part + P.n_row;  // tile (I, J): + (col_base(J) + I - J) * 64
+
+  // x over the tile row: lanes' rows (row-fast / slow) and the warp's rows
+  // (column-fast)
+  E xi_l[2], xi_w[8];
+#pragma unroll
+  for (int a = 0; a < 2; ++a) xi_l[a] = xval(x, incx, i0 + lane + 32 * a, n);
+#pragma unroll
+  for (int b = 0; b < 8; ++b) xi_w[b] = xval(x, incx, i0 + 8 * w + b, n);
+
+  E racc_l[2] = {E(0), E(0)};  // row products of rows l, l + 32 (this warp's columns)
+  E racc_w = E(0);             // row products of row 8w + (lane >> 2) (column-fast tiles)
+  // column-fast tiles alternate between two buffers (counted over those
+  // tiles only, so a buffer is rewritten only after a barrier that follows
+  // its readers)
+  __shared__ E cbuf[2][8][TB];
+  __shared__ E rbuf[9][TB];
+  int ncf = 0;
+
+  Tile<E> cur, nxt;
+  load_tile(g, arf, I, Jb, lane, w, cur);
+  for (int J = Jb; J < Je; ++J) {
+    if (J + 1 < Je) load_tile(g, arf, I, J + 1, lane, w, nxt);
+    const int64_t j0 = (int64_t)J * TB;
+    E* cp = col_part + (col_base(J, P.tiles) + (I - J)) * TB;
+    if (cur.kind != kColFast) {
+      // rows: v[8a + b] x_{j0 + 8w + b}; columns: sum over the 64 rows
+      E xj[8], cv[8];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) xj[b] = xval(x, incx, j0 + 8 * w + b, n);
+      const bool diag = I == J;
+#pragma unroll
+      for (int a = 0; a < 2; ++a) {
+        E r = E(0);
+#pragma unroll
+        for (int b = 0; b < 8; ++b) r = fma(cur.v[8 * a + b], xj[b], r);
+        racc_l[a] += r;
+      }
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        E c0 = cur.v[b], c1 = cur.v[8 + b];
+        if (diag) {  // strictly lower part only
+          if (lane <= 8 * w + b) c0 = E(0);
+          if (lane + 32 <= 8 * w + b) c1 = E(0);
+        }
+        cv[b] = fma(c1, xi_l[1], c0 * xi_l[0]);
+      }
+      const E tot = warp_sum8(cv, lane);
+      if ((lane & 3) == 0) cp[8 * w + (lane >> 2)] = tot;
+    } else {
+      // rows 8w + b: sum over the 64 columns (lanes); columns l, l + 32: sum
+      // over this warp's 8 rows, then over the warps
+      E xj0 = xval(x, incx, j0 + lane, n), xj1 = xval(x, incx, j0 + lane + 32, n);
+      E rv[8];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) rv[b] = fma(cur.v[8 + b], xj1, cur.v[b] * xj0);
+      racc_w += warp_sum8(rv, lane);
+      E c0 = E(0), c1 = E(0);
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        c0 = fma(cur.v[b], xi_w[b], c0);
+        c1 = fma(cur.v[8 + b], xi_w[b], c1);
+      }
+      E (*cb)[TB] = cbuf[ncf++ & 1];
+      cb[w][lane] = c0;
+      cb[w][lane + 32] = c1;
+      __syncthreads();
+      if (threadIdx.x < TB) {
+        E t = cb[0][threadIdx.x];
+#pragma unroll
+        for (int q = 1; q < 8; ++q) t += cb[q][threadIdx.x];
+        cp[threadIdx.x] = t;
+      }
+    }
+    cur = nxt;
+  }
+  // row product of the strip: the 8 warps' lane sums, then the column-fast sums
+  rbuf[w][lane] = racc_l[0];
+  rbuf[w][lane + 32] = racc_l[1];
+  if ((lane & 3) == 0) rbuf[8][8 * w + (lane >> 2)] = racc_w;
   __syncthreads();
-  if (tid < TB) {
-    const int li = tid, i = i0 + li;
+  if (threadIdx.x < TB) {
+    E t = rbuf[0][threadIdx.x];
+#pragma unroll
+    for (int q = 1; q < 9; ++q) t += rbuf[q][threadIdx.x];
+    row_part[threadIdx.x] = t;
+  }
+}
+
+// y_J (64 rows per CTA) from the partials: four groups of 64 threads sum
+// quarters of the column list, then thread r adds the strips' row products
+// and the four quarters in order.
+template <typename E>
+__global__ void __launch_bounds__(kThreads)
+    symv_reduce(int n, const E* __restrict__ part, E* y, int64_t incy, E alpha, E beta) {
+  const Parts P = parts(n);
+  const int J = blockIdx.x, r = threadIdx.x % TB, q = threadIdx.x / TB;
+  const int64_t cnt = P.tiles - J;  // col_part entries I = J .. T-1
+  const int64_t per = (cnt + 3) / 4, b0 = q * per, b1 = min(cnt, b0 + per);
+  const E* cp = part + P.n_row + col_base(J, P.tiles) * TB + r;
+  E t = E(0);
+  for (int64_t e = b0; e < b1; ++e) t += cp[e * TB];
+  __shared__ E qs[4][TB];
+  qs[q][r] = t;
+  __syncthreads();
+  if (q == 0) {
+    const int64_t i = (int64_t)J * TB + r;
     if (i < n) {
-      const int grp = li / 16, r = li % 16;  // threads with tg == grp: warps 2 grp, 2 grp + 1
-      T s = part_a[0][li] + part_a[1][li] + part_a[2][li] + part_a[3][li];
-      s += part_b[2 * grp][r] + part_b[2 * grp + 1][r];
-      T* yi = y + (int64_t)i * incy;
-      *yi = beta == T(0) ? alpha * s : fma(beta, *yi, alpha * s);
+      E sum = E(0);
+      const E* rp = part + (int64_t)J * P.strips * TB + r;
+      const int ns = J / S + 1;
+      for (int s = 0; s < ns; ++s) sum += rp[(int64_t)s * TB];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) sum += qs[k][r];
+      E* yi = y + i * incy;
+      *yi = beta == E(0) ? alpha * sum : fma(beta, *yi, alpha * sum);
     }
   }
 }

@@ -133,3 +133,27 @@ def test_ssfr_ssfr2_vs_fp64(curfp, orc, n, tr, ul, incx, incy):
     a3 = dev(arf)
     curfp.ssfr_raw(h, tr, ul, n, 0.0, torch.full((n,), float("nan"), device="cuda"), 1, a3)
     np.testing.assert_array_equal(host(a3), arf)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [129, 20001])
+@pytest.mark.parametrize("tr,ul", [(1, 1), (0, 0), (1, 0), (0, 1)])
+def test_ssfmv_large_repeatable(curfp, n, tr, ul):
+    """ssfmv against a dense FP64 torch product of the unpacked matrix
+    (n = 20001: 2e8 stored elements, every 64 x 64 tile kind), and two calls
+    agree bit for bit."""
+    g = torch.Generator(device="cuda").manual_seed(n + tr + 2 * ul)
+    M = torch.randn(n, n, device="cuda", generator=g)
+    kw = dict(transr=TR[tr], uplo=UL[ul])
+    arf = curfp.strttf(M, **kw)
+    T = (M.triu() if ul else M.tril()).double()
+    S = T + (T.triu(1).T if ul else T.tril(-1).T)
+    del M, T
+    x = torch.randn(n, device="cuda", generator=g)
+    y0 = torch.randn(n, device="cuda", generator=g)
+    y1, y2 = y0.clone(), y0.clone()
+    curfp.ssfmv(arf, x, y1, alpha=-0.5, beta=2.0, **kw)
+    curfp.ssfmv(arf, x, y2, alpha=-0.5, beta=2.0, **kw)
+    assert torch.equal(y1, y2)
+    want = -0.5 * (S @ x.double()) + 2.0 * y0.double()
+    assert (y1.double() - want).abs().max().item() <= tol(n) * want.abs().max().item()
