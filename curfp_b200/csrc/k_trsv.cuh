@@ -310,13 +310,22 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     __syncthreads();
     tile_mma<true, NC>(acc, Ls0, Xs0, tr, tc);  // X_j = Y - M_j X_{j-1}
   }
+  // X_jc -> B through shared memory (Xs1 is free here), so that the global
+  // stores run along B's contiguous dimension like the loads of load_regs.
 #pragma unroll
   for (int p = 0; p < TR; ++p)
 #pragma unroll
-    for (int q = 0; q < TC; ++q) {
-      const int a = tr * TR + p, b = tc * TC + q;
-      if (a < rows && b < cols) Bt.p[(int64_t)a * Bt.rs + (int64_t)b * Bt.cs] = acc[p][q];
+    for (int q = 0; q < TC; ++q) Xs1[(tr * TR + p) * LX + tc * TC + q] = acc[p][q];
+  __syncthreads();
+  {
+    const bool rowcont = (Bt.cs == 1 || Bt.cs == -1) && !(Bt.rs == 1 || Bt.rs == -1);
+#pragma unroll
+    for (int u = 0; u < EPT; ++u) {
+      const int e = tid + 256 * u;
+      const int a = rowcont ? e / NC : e % NB, b = rowcont ? e % NC : e / NB;
+      if (a < rows && b < cols) Bt.p[(int64_t)a * Bt.rs + (int64_t)b * Bt.cs] = Xs1[a * LX + b];
     }
+  }
   __threadfence();
   __syncthreads();
   if (tid == 0) st_release(&flags[j * nchunk + c], 1);
