@@ -32,7 +32,9 @@ namespace rfp {
 namespace ktrsv {
 
 constexpr int NB = 64;
-constexpr int LDL = NB + 1;  // L / W / M tiles: scalar reads down a row, conflict-free both ways
+// L / W / M tiles are held k-major (element (a, b) at s[b * LDL + a]) so that
+// the products read four consecutive rows of a column with one 16-byte load.
+constexpr int LDL = NB + 4;
 constexpr uint64_t WAIT_NS = 2000000000ull;
 
 // Right-hand-side chunk of one CTA: NC columns, each thread a TR x TC
@@ -48,10 +50,13 @@ template <> struct Chunk<8> {
 };
 constexpr int LDX = Chunk<64>::LDX;
 
-// Ls[2], Ws (L tiles; W_j; M_j reuses Ls[0]) and Xs[2], Ts (X tiles; B_jc / T)
+// Ls[2], Ws (L tiles; W_j; M_j reuses Ls[0]) and Xs[2], Ts (X tiles; B_jc / T);
+// 8-column chunks add the partial sums of their k-split products.
+constexpr int LDP = NB + 1;  // row stride of the partial sums
+template <int NC> constexpr int kparts() { return NC == 8 ? 4 * 8 * LDP : 0; }
 template <typename T, int NC = 64>
 constexpr int smem_bytes() {
-  return (3 * NB * LDL + 3 * NB * Chunk<NC>::LDX) * (int)sizeof(T);
+  return (3 * NB * LDL + 3 * NB * Chunk<NC>::LDX + kparts<NC>()) * (int)sizeof(T);
 }
 constexpr int SMEM = smem_bytes<float>();
 
@@ -82,9 +87,9 @@ __device__ __forceinline__ void cp1(double* smem, const double* g, bool pred) {
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Read-only tile (rows x cols of a strided view; L) -> s[a][b] (row stride
-// LD) by cp.async, zero fill outside; the thread mapping follows the view's
-// contiguous dimension.  (cp.async of 4 bytes caches in L1, which is not
+// Read-only tile (rows x cols of a strided view; L) -> element (a, b) at
+// s[b * LD + a] by cp.async, zero fill outside; the thread mapping follows
+// the view's contiguous dimension.  (cp.async of 4 bytes caches in L1, which is not
 // coherent with other CTAs' stores: only data that no CTA of this launch
 // writes goes this way.)
 template <int LD, typename T>
@@ -95,7 +100,7 @@ __device__ __forceinline__ void load_tile(T* s, ViewT<T> v, int rows, int cols) 
     const int e = threadIdx.x + 256 * u;
     const int a = rowcont ? e / NB : e % NB, b = rowcont ? e % NB : e / NB;
     const bool ok = a < rows && b < cols;
-    cp1(s + a * LD + b, ok ? v.p + (int64_t)a * v.rs + (int64_t)b * v.cs : v.p, ok);
+    cp1(s + b * LD + a, ok ? v.p + (int64_t)a * v.rs + (int64_t)b * v.cs : v.p, ok);
   }
 }
 // Tile of B / X (64 x NC, written by CTAs of this launch): L2-only loads
@@ -121,13 +126,13 @@ __device__ __forceinline__ void store_regs(T* s, const T (&r)[Chunk<NC>::EPT], V
     s[a * Chunk<NC>::LDX + b] = r[u];
   }
 }
-// 64 x 64 column-major workspace tile -> s[a][b] (row stride LDL).
+// 64 x 64 column-major workspace tile -> element (a, b) at s[b * LDL + a].
 template <typename T>
 __device__ __forceinline__ void load_ws(T* s, const T* w) {
 #pragma unroll 4
   for (int u = 0; u < 16; ++u) {
     const int e = threadIdx.x + 256 * u;
-    cp1(s + (e % NB) * LDL + e / NB, w + e, true);
+    cp1(s + (e / NB) * LDL + e % NB, w + e, true);
   }
 }
 // Four consecutive shared-memory elements (16-byte reads).
@@ -140,28 +145,56 @@ __device__ __forceinline__ void lds4(const double* p, double (&v)[4]) {
   const double2 y = reinterpret_cast<const double2*>(p)[1];
   v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
 }
-// acc (+)= sign * A(64 x 64, row stride LDL) * X(64 x 64, row stride LDX) on
-// the thread's 4 x 4 register tile (rows tr*4.., columns tc*4..).
+// acc (+)= sign * A(64 x 64, k-major, stride LDL) * X(64 x NC, row stride LDX)
+// on the thread's TR x TC register tile (rows tr*TR.., columns tc*TC..).
+// 64 columns: per k one 16-byte read of A's column and one of X's row feed 16
+// FMAs.  8 columns: the k range is split over four groups of 64 threads
+// (thread = row), whose partial sums meet in P (4 x 8 rows of LDP) in group
+// order;
+// the call contains two block barriers, so every thread of the CTA makes it.
 template <bool kSub, int NC, typename T>
 __device__ __forceinline__ void tile_mma(T (&acc)[Chunk<NC>::TR][Chunk<NC>::TC], const T* A,
-                                         const T* X, int tr, int tc) {
+                                         const T* X, int tr, int tc, T* P) {
   constexpr int TR = Chunk<NC>::TR, TC = Chunk<NC>::TC, LX = Chunk<NC>::LDX;
+  if constexpr (NC == 64) {
 #pragma unroll 8
-  for (int k = 0; k < NB; ++k) {
-    T a[TR], x[4];
-#pragma unroll
-    for (int q = 0; q < TR; ++q) a[q] = A[(tr * TR + q) * LDL + k];
-    if constexpr (TC == 4) {
+    for (int k = 0; k < NB; ++k) {
+      T a[4], x[4];
+      lds4(A + k * LDL + tr * 4, a);
       lds4(X + k * LX + tc * 4, x);
-    } else {
 #pragma unroll
-      for (int q = 0; q < TC; ++q) x[q] = X[k * LX + tc * TC + q];
+      for (int p = 0; p < TR; ++p)
+#pragma unroll
+        for (int q = 0; q < TC; ++q)
+          acc[p][q] = kSub ? fma(-a[p], x[q], acc[p][q]) : fma(a[p], x[q], acc[p][q]);
+    }
+  } else {
+    static_assert(NC == 8 && TC == 1, "8-column chunk layout");
+    const int r = threadIdx.x % NB, g = threadIdx.x / NB;
+    T part[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) part[q] = T(0);
+#pragma unroll 4
+    for (int kk = 0; kk < NB / 4; ++kk) {
+      const int k = g * (NB / 4) + kk;
+      const T a = A[k * LDL + r];
+      T x[8];
+      lds4(X + k * LX, *reinterpret_cast<T(*)[4]>(x));
+      lds4(X + k * LX + 4, *reinterpret_cast<T(*)[4]>(x + 4));
+#pragma unroll
+      for (int q = 0; q < 8; ++q) part[q] = fma(a, x[q], part[q]);
     }
 #pragma unroll
-    for (int p = 0; p < TR; ++p)
+    for (int q = 0; q < 8; ++q) P[(g * 8 + q) * LDP + r] = part[q];
+    __syncthreads();
 #pragma unroll
-      for (int q = 0; q < TC; ++q)
-        acc[p][q] = kSub ? fma(-a[p], x[q], acc[p][q]) : fma(a[p], x[q], acc[p][q]);
+    for (int p = 0; p < TR; ++p) {
+      const int row = tr * TR + p;
+      const T v = ((P[tc * LDP + row] + P[(8 + tc) * LDP + row]) + P[(16 + tc) * LDP + row]) +
+                  P[(24 + tc) * LDP + row];
+      acc[p][0] = kSub ? acc[p][0] - v : acc[p][0] + v;
+    }
+    __syncthreads();
   }
 }
 
@@ -197,6 +230,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
   T* Xs0 = Ws + NB * LDL;
   T* Xs1 = Xs0 + NB * LX;
   T* Ts = Xs1 + NB * LX;
+  T* Ps = Ts + NB * LX;  // k-split partial sums (8-column chunks)
   __shared__ int sh_ticket, sh_state, sh_ready[2], sh_last;
   if (abort_flag && *abort_flag != INT_MAX) return;
   const int tid = threadIdx.x;
@@ -253,7 +287,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     if (more) load_tile<LDL>(Ln, lview(i + 1), rows, NB);
     cp_commit();
     if (ready) load_regs<NC>(xr, xview(i + 1), NB, cols);
-    tile_mma<false, NC>(acc, Lb, Xb, tr, tc);
+    tile_mma<false, NC>(acc, Lb, Xb, tr, tc, Ps);
     if (more) {
       if (!ready) {
         if (tid == 0) sh_state = wait_flag(&flags[(i + 1) * nchunk + c], err);
@@ -292,7 +326,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
       acc[p][q] = T(0);
     }
   __syncthreads();
-  tile_mma<false, NC>(acc, Ws, Ts, tr, tc);
+  tile_mma<false, NC>(acc, Ws, Ts, tr, tc, Ps);
   if (j > 0) {
     if (!ready) {
       if (tid == 0) sh_state = wait_flag(&flags[(j - 1) * nchunk + c], err);
@@ -308,7 +342,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     store_regs<NC>(Xs0, xr, xview(j - 1));
     cp_wait_all();
     __syncthreads();
-    tile_mma<true, NC>(acc, Ls0, Xs0, tr, tc);  // X_j = Y - M_j X_{j-1}
+    tile_mma<true, NC>(acc, Ls0, Xs0, tr, tc, Ps);  // X_j = Y - M_j X_{j-1}
   }
   // X_jc -> B through shared memory (Xs1 is free here), so that the global
   // stores run along B's contiguous dimension like the loads of load_regs.
