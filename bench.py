@@ -479,7 +479,7 @@ def run_ours(args, rank, world, local):
 
 
 CASES = ("ssfrk-bf16", "ssfrk-fp32", "chol-bf16", "chol-fp32", "solve", "refine", "pack",
-         "norms", "rank", "nll-fused")
+         "norms", "rank", "symv", "nll-fused")
 
 
 def run_case(args):
@@ -551,6 +551,13 @@ def run_case(args):
         for _ in range(reps):
             curfp.ssfr(C, x, alpha=1e-3)
             curfp.ssfr2(C, x, y, alpha=1e-3)
+    elif case == "symv":
+        C = spd()
+        x = torch.randn(n, device="cuda", generator=g)
+        y = torch.zeros(n, device="cuda")
+        prof_on()
+        for _ in range(reps):
+            curfp.ssfmv(C, x, y)
     elif case == "nll-fused":
         X = torch.randn(n, k, device="cuda", generator=g)
         y = torch.randn(n, device="cuda", generator=g)

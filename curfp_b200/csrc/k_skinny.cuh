@@ -48,7 +48,7 @@ __device__ __forceinline__ void store_out(const Args<T>& a, int i, int c, T s) {
 template <typename T, int N>
 __global__ void __launch_bounds__(kThreads) skinny_rows(const Args<T> a, const int* abort_flag) {
   if (abort_flag && *abort_flag != INT_MAX) return;
-  constexpr int U = sizeof(T) == 4 ? 16 : 8;  // columns per warp block
+  constexpr int U = sizeof(T) == 4 ? 32 : 16;  // columns per warp block (loads in flight)
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = blockIdx.x * 32 + lane;
   const T* Ai = a.A + (int64_t)min(i, a.m - 1) * a.a_rs;

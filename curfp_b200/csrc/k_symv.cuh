@@ -95,7 +95,9 @@ struct Tile {
 };
 
 // Tile (I, J) of the logical lower triangle into registers (zero outside
-// the matrix; the diagonal tile keeps i >= j).
+// the matrix; the diagonal tile keeps i >= j).  Inside one RFP block the
+// addresses advance by pointer increments from one per-thread base; tiles
+// wholly inside the matrix load without bounds predicates.
 template <typename E>
 __device__ __forceinline__ void load_tile(const Geometry& g, const E* __restrict__ arf, int I,
                                           int J, int lane, int w, Tile<E>& t) {
@@ -104,29 +106,34 @@ __device__ __forceinline__ void load_tile(const Geometry& g, const E* __restrict
   const int64_t im = min((int64_t)n - 1, i0 + TB - 1), jm = min((int64_t)n - 1, j0 + TB - 1);
   const bool one_block = (i0 < g.n1) == (im < g.n1) && (j0 < g.n1) == (jm < g.n1);
   if (I != J && one_block) {
-    const BlockGeom& bg = j0 < g.n1 ? (i0 < g.n1 ? g.b11 : g.b21) : g.b22;
-    const int64_t ib = i0 < g.n1 ? 0 : g.n1, jb = j0 < g.n1 ? 0 : g.n1;
-    const E* base = arf + bg.off + (i0 - ib) * bg.rs + (j0 - jb) * bg.cs;
-    if (bg.rs == 1 || bg.rs == -1) {
-      t.kind = kRowFast;
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 8; ++b) {
-          const int64_t li = lane + 32 * a, lj = 8 * w + b;
-          t.v[8 * a + b] = (i0 + li < n && j0 + lj < n) ? __ldg(base + li * bg.rs + lj * bg.cs)
-                                                         : E(0);
-        }
+    int64_t off, rs, cs, ib, jb;
+    if (j0 >= g.n1) {
+      off = g.b22.off; rs = g.b22.rs; cs = g.b22.cs; ib = g.n1; jb = g.n1;
+    } else if (i0 >= g.n1) {
+      off = g.b21.off; rs = g.b21.rs; cs = g.b21.cs; ib = g.n1; jb = 0;
     } else {
-      t.kind = kColFast;
+      off = g.b11.off; rs = g.b11.rs; cs = g.b11.cs; ib = 0; jb = 0;
+    }
+    const E* base = arf + off + (i0 - ib) * rs + (j0 - jb) * cs;
+    const bool full = i0 + TB <= n;  // j0 < i0 here, so the columns are inside too
+    const bool rowf = rs == 1 || rs == -1;
+    t.kind = rowf ? kRowFast : kColFast;
+    // row-fast: (row lane + 32a, col 8w + b); column-fast: (row 8w + b, col lane + 32a)
+    const int64_t s_lane = rowf ? rs : cs, s_b = rowf ? cs : rs;
+    const E* pw = base + (int64_t)lane * s_lane + (int64_t)(8 * w) * s_b;
 #pragma unroll
-      for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < 2; ++a) {
+      const E* q = pw + (int64_t)(32 * a) * s_lane;
+      if (full) {
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
-          const int64_t li = 8 * w + b, lj = lane + 32 * a;
-          t.v[8 * a + b] = (i0 + li < n && j0 + lj < n) ? __ldg(base + li * bg.rs + lj * bg.cs)
-                                                         : E(0);
+        for (int b = 0; b < 8; ++b, q += s_b) t.v[8 * a + b] = __ldg(q);
+      } else {
+#pragma unroll
+        for (int b = 0; b < 8; ++b, q += s_b) {
+          const int64_t i = i0 + (rowf ? lane + 32 * a : 8 * w + b);
+          t.v[8 * a + b] = i < n ? __ldg(q) : E(0);
         }
+      }
     }
   } else {
     t.kind = kSlow;
@@ -193,8 +200,13 @@ __global__ void __launch_bounds__(kThreads)
     if (cur.kind != kColFast) {
       // rows: v[8a + b] x_{j0 + 8w + b}; columns: sum over the 64 rows
       E xj[8], cv[8];
+      {
+        const E* xq = x + (j0 + 8 * w) * incx;
+        const bool xin = j0 + TB <= n;
 #pragma unroll
-      for (int b = 0; b < 8; ++b) xj[b] = xval(x, incx, j0 + 8 * w + b, n);
+        for (int b = 0; b < 8; ++b, xq += incx)
+          xj[b] = (xin || j0 + 8 * w + b < n) ? __ldg(xq) : E(0);
+      }
       const bool diag = I == J;
 #pragma unroll
       for (int a = 0; a < 2; ++a) {
