@@ -171,7 +171,17 @@ int CudaExecT<double>::gemm(const GemmProbT<double>* p, int count) {
     const int rc = launch_skinny<double>(p[0], abort_, ctx_);
     if (rc >= 0) return rc;
   }
-  return launch_gemm<double, 64, 64>(p, count, abort_, ctx_);  // 16 accumulators per thread
+  // 128 x 128 tiles (64 accumulators per thread, one CTA per SM) when they
+  // fill the machine, else 64 x 64
+  int64_t t128 = 0;
+  bool inplace = false;
+  for (int i = 0; i < count; ++i) {
+    const int64_t tm = (p[i].m + 127) / 128, tn = (p[i].n + 127) / 128;
+    t128 += p[i].c_lower ? tm * (tm + 1) / 2 : tm * tn;
+    inplace = inplace || p[i].inplace;
+  }
+  if (t128 >= 148 && !inplace) return launch_gemm<double, 128, 128>(p, count, abort_, ctx_);
+  return launch_gemm<double, 64, 64>(p, count, abort_, ctx_);
 }
 
 template <>

@@ -191,7 +191,8 @@ __device__ __forceinline__ void k_range(int k, int a_tri, int b_tri, int m0, int
 }
 
 template <typename T, int BM, int BN>
-__global__ void __launch_bounds__(kThreads, 2) sgemm_batch(const Batch<T> batch) {
+__global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 && BM >= 128) ? 1 : 2)
+    sgemm_batch(const Batch<T> batch) {
   if (batch.abort_flag && *batch.abort_flag != INT_MAX) return;
   constexpr int TM = BM / 16, TN = BN / 16;
   constexpr int GM = TM / 4, GN = TN / 4;

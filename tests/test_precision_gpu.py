@@ -121,11 +121,13 @@ def test_refined_solve(curfp, n, lam):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n,nr", [(300, 7), (1000, 70), (4097, 64)])
 @pytest.mark.parametrize("tr,ul", VARIANTS)
-def test_symm_acc64(curfp, orc, tr, ul):
+def test_symm_acc64(curfp, orc, tr, ul, n, nr):
+    """Single k pass (n = 300) and k split over CTAs with FP64 atomics
+    (n = 1000, 4097), one and several 64-column blocks."""
     from curfp_b200 import precision as P
-    n, nr = 300, 7
-    rng = np.random.default_rng(2)
+    rng = np.random.default_rng(2 + n)
     M = rng.standard_normal((n, n)).astype(np.float32)
     M = M + M.T
     arf = orc.strttf(tr, ul, n, M.astype(np.float64)).astype(np.float32)
