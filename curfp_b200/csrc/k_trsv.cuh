@@ -360,9 +360,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
       if (a < rows && b < cols) Bt.p[(int64_t)a * Bt.rs + (int64_t)b * Bt.cs] = Xs1[a * LX + b];
     }
   }
-  __threadfence();
+  // The block's stores are ordered before thread 0's fence by the barrier;
+  // the fence and the release then publish them at GPU scope.
   __syncthreads();
-  if (tid == 0) st_release(&flags[j * nchunk + c], 1);
+  if (tid == 0) {
+    __threadfence();
+    st_release(&flags[j * nchunk + c], 1);
+  }
 }
 
 }  // namespace ktrsv
