@@ -296,13 +296,18 @@ int launch_wave(curfpContext* ctx, const int* abort_flag, ViewT<T> L, int n, Vie
   int* sync = static_cast<int*>(grow_buffer(ctx, &ctx->tsv, &ctx->tsv_bytes, words * 4));
   if (!sync) return 2;
   if (cudaMemsetAsync(sync, 0, words * 4, ctx->stream) != cudaSuccess) return 4;
+  // With at most two chunks the chain of block rows sets the time: the
+  // shared-memory request is padded to one CTA per SM, so the chain's product
+  // does not share its SM with another CTA's accumulation.
   constexpr int smem = ktrsv::smem_bytes<T, NC>();
-  static const bool attr = smem_attr(ktrsv::trsm_wave<T, NC>, smem);
+  constexpr int smem_one = ktrsv::smem_limit<T, NC>();
+  static const bool attr = smem_attr(ktrsv::trsm_wave<T, NC>, smem_one);
   if (!attr) return 4;
+  const int smem_launch = nchunk <= 2 ? smem_one : smem;
   ProfScope ps(ctx->prof, ctx->stream, K_TRSV, (double)n * n * m,
                (double)n * n * sizeof(T) / 2.0);
-  ktrsv::trsm_wave<T, NC><<<nblk * nchunk, 256, smem, ctx->stream>>>(L, n, B, m, alpha, W, sync,
-                                                                    ctx->d_info + 1, abort_flag);
+  ktrsv::trsm_wave<T, NC><<<nblk * nchunk, 256, smem_launch, ctx->stream>>>(
+      L, n, B, m, alpha, W, sync, ctx->d_info + 1, abort_flag);
   ++ctx->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
@@ -328,7 +333,7 @@ int launch_trsm_wave_fixed(curfpContext* ctx, const int* abort_flag, View L, int
   if (words > sync_words) return 3;
   if (cudaMemsetAsync(sync, 0, words * 4, ctx->stream) != cudaSuccess) return 4;
   if (cudaFuncSetAttribute(ktrsv::trsm_wave<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           ktrsv::SMEM) != cudaSuccess)
+                           ktrsv::smem_limit<float>()) != cudaSuccess)
     return 4;
   ProfScope ps(ctx->prof, ctx->stream, K_TRSV, (double)n * n * m, (double)n * n * 2.0);
   ktrsv::trsm_wave<float><<<nblk * nchunk, 256, ktrsv::SMEM, ctx->stream>>>(

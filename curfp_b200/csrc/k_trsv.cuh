@@ -59,6 +59,12 @@ constexpr int smem_bytes() {
   return (3 * NB * LDL + 3 * NB * Chunk<NC>::LDX + kparts<NC>()) * (int)sizeof(T);
 }
 constexpr int SMEM = smem_bytes<float>();
+// The dynamic shared-memory limit set on every instantiation: its own need,
+// or at least 116 KB so that a launch may ask for one CTA per SM.
+template <typename T, int NC = 64>
+constexpr int smem_limit() {
+  return smem_bytes<T, NC>() > 116 * 1024 ? smem_bytes<T, NC>() : 116 * 1024;
+}
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
