@@ -6,6 +6,7 @@
 
 #include "context.h"
 #include "k_gemm.cuh"
+#include "gemm_route.h"
 #include "k_skinny.cuh"
 #include "k_tile.cuh"
 #include "k_trsv.cuh"
@@ -84,27 +85,13 @@ int launch_gemm(const GemmProbT<T>* p, int count, const int* abort_flag,
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
-// A single full product with at most 8 columns (or, through C^T = B^T A^T,
-// at most 8 rows) and at least 2^20 elements of A: the bandwidth-bound
-// skinny kernels (k_skinny.cuh), which read A once along its unit-stride
-// dimension.  Returns -1 when the problem does not qualify.
+// The few-column kernels (k_skinny.cuh) for the products gemm_route.h
+// routes to them; -1 when it does not.
 template <typename T>
 int launch_skinny(const GemmProbT<T>& g0, const int* abort_flag, curfpContext* ctx) {
-  GemmProbT<T> g = g0;
-  if (g.k2 || g.a_tri || g.b_tri || g.c_lower || g.inplace) return -1;
-  if (g.n > kskinny::kMaxCols && g.m <= kskinny::kMaxCols) {
-    const ViewT<T> A = tr(g.B), B = tr(g.A);
-    g.A = A;
-    g.B = B;
-    g.C = tr(g.C);
-    const int t = g.m;
-    g.m = g.n;
-    g.n = t;
-  }
-  if (g.n > kskinny::kMaxCols || g.m <= 0 || g.n <= 0 || g.k <= 0) return -1;
-  if ((int64_t)g.m * g.k < ((int64_t)1 << 20)) return -1;
-  const bool rows = g.A.rs == 1 || g.A.rs == -1;
-  if (!rows && !(g.A.cs == 1 || g.A.cs == -1)) return -1;
+  GemmProbT<T> g;
+  const SkinnyRoute r = skinny_route(g0, &g);
+  if (!r.use) return -1;
   const kskinny::Args<T> a{g.A.p, g.A.rs, g.A.cs, g.B.p, g.B.rs, g.B.cs, g.C.p, g.C.rs, g.C.cs,
                            g.m, g.n, g.k, g.alpha, g.beta};
   ProfScope ps(ctx->prof, ctx->stream, K_SGEMM, 2.0 * g.m * g.n * (double)g.k,
@@ -113,13 +100,15 @@ int launch_skinny(const GemmProbT<T>& g0, const int* abort_flag, curfpContext* c
   cudaStream_t st = ctx->stream;
   auto go = [&](auto ncols) {
     constexpr int N = decltype(ncols)::value;
-    if (rows) kskinny::skinny_rows<T, N><<<grid, kskinny::kThreads, 0, st>>>(a, abort_flag);
+    if (r.rows) kskinny::skinny_rows<T, N><<<grid, kskinny::kThreads, 0, st>>>(a, abort_flag);
     else kskinny::skinny_cols<T, N><<<grid, kskinny::kThreads, 0, st>>>(a, abort_flag);
   };
-  if (g.n == 1) go(std::integral_constant<int, 1>{});
-  else if (g.n == 2) go(std::integral_constant<int, 2>{});
-  else if (g.n <= 4) go(std::integral_constant<int, 4>{});
-  else go(std::integral_constant<int, 8>{});
+  switch (r.inst) {
+    case 1: go(std::integral_constant<int, 1>{}); break;
+    case 2: go(std::integral_constant<int, 2>{}); break;
+    case 4: go(std::integral_constant<int, 4>{}); break;
+    default: go(std::integral_constant<int, 8>{}); break;
+  }
   ++ctx->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }

@@ -26,7 +26,6 @@ namespace rfp {
 namespace kskinny {
 
 constexpr int kThreads = 256;
-constexpr int kMaxCols = 8;
 
 template <typename T>
 struct Args {

@@ -27,36 +27,12 @@
 #include <cstdint>
 
 #include "rfp.h"
+#include "symv_layout.h"
 
 namespace rfp {
 namespace ksymv {
 
-constexpr int TB = 64;        // tile edge
-constexpr int S = 16;         // tiles per strip
 constexpr int kThreads = 256;
-
-// Layout of the partials for T = ceil(n / 64) tile rows.
-struct Parts {
-  int tiles;      // T
-  int strips;     // ceil(T / S): row_part stride per tile row
-  int64_t n_row;  // T * strips * 64 elements
-  int64_t n_col;  // T (T + 1) / 2 * 64 elements
-};
-RFP_HD Parts parts(int n) {
-  Parts p;
-  p.tiles = (n + TB - 1) / TB;
-  p.strips = (p.tiles + S - 1) / S;
-  p.n_row = (int64_t)p.tiles * p.strips * TB;
-  p.n_col = (int64_t)p.tiles * (p.tiles + 1) / 2 * TB;
-  return p;
-}
-// Strips over tile rows 0 .. I-1: sum_{i < I} (floor(i / S) + 1).
-RFP_HD int64_t strips_before(int64_t I) {
-  const int64_t q = I / S, r = I - q * S;
-  return I + S * q * (q - 1) / 2 + q * r;
-}
-// First col_part entry of tile column J: sum_{j < J} (T - j).
-RFP_HD int64_t col_base(int64_t J, int64_t T) { return J * T - J * (J - 1) / 2; }
 
 enum : int { kRowFast = 0, kColFast = 1, kSlow = 2 };
 
@@ -160,15 +136,8 @@ __global__ void __launch_bounds__(kThreads)
   const int n = g.n;
   const Parts P = parts(n);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  // (I, s) of this CTA: the largest I with strips_before(I) <= blockIdx.x
-  int lo = 0, hi = P.tiles - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) / 2;
-    if (strips_before(mid) <= (int64_t)blockIdx.x) lo = mid;
-    else hi = mid - 1;
-  }
-  const int I = lo;
-  const int s = (int)((int64_t)blockIdx.x - strips_before(I));
+  int I, s;
+  strip_of(blockIdx.x, P.tiles, I, s);
   const int Jb = s * S, Je = min(Jb + S, I + 1);
   const int64_t i0 = (int64_t)I * TB;
   E* row_part = part + ((int64_t)I * P.strips + s) * TB;
