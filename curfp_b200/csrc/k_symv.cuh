@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(kThreads)
         cp[threadIdx.x] = t;
       }
     }
-    cur = nxt;
+    if (J + 1 < Je) cur = nxt;
   }
   // row product of the strip: the 8 warps' lane sums, then the column-fast sums
   rbuf[w][lane] = racc_l[0];
