@@ -77,3 +77,26 @@ def test_dpftrs_few_rhs(curfp, orc, nrhs, tr, ul):
     curfp.dpftrs_raw(curfp._get_handle(), tr, ul, n, nrhs, F, X, n)
     got = host(X).T
     assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [300, 513, 1000])
+@pytest.mark.parametrize("nrhs", [2048, 2100])
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+def test_spftrs_many_rhs(curfp, orc, n, nrhs, tr, ul):
+    """Thousands of right-hand sides over triangles of at most 512 rows (the
+    recursive solve's leaves): one CTA per 64-column chunk walks the block
+    rows (a partial last chunk with 2100 columns); against the FP64 solve
+    with the same factor, and bitwise repeatable."""
+    F = factor(curfp, n, tr, ul, torch.float32, seed=n + nrhs + 5 * tr + 11 * ul)
+    rng = np.random.default_rng(n * nrhs)
+    Bh = rng.standard_normal((nrhs, n)).astype(np.float32)  # column-major n x nrhs
+    want = fp64_solve(orc, tr, ul, n, F, Bh.T.astype(np.float64))
+    h = curfp._get_handle()
+    X1 = torch.from_numpy(Bh).cuda()
+    X2 = X1.clone()
+    curfp.spftrs_raw(h, tr, ul, n, nrhs, F, X1, n)
+    curfp.spftrs_raw(h, tr, ul, n, nrhs, F, X2, n)
+    assert torch.equal(X1, X2)
+    got = host(X1).T.astype(np.float64)
+    assert np.abs(got - want).max() <= 2e-5 * np.abs(want).max()
