@@ -479,7 +479,7 @@ def run_ours(args, rank, world, local):
 
 
 CASES = ("ssfrk-bf16", "ssfrk-fp32", "chol-bf16", "chol-fp32", "solve", "refine", "pack",
-         "norms", "rank", "symv", "nll-fused")
+         "norms", "rank", "symv", "dsfrk", "nll-fused")
 
 
 def run_case(args):
@@ -558,6 +558,12 @@ def run_case(args):
         prof_on()
         for _ in range(reps):
             curfp.ssfmv(C, x, y)
+    elif case == "dsfrk":
+        A = torch.randn(n, k, device="cuda", dtype=torch.float64, generator=g) / k ** 0.5
+        C = torch.empty(nt, device="cuda", dtype=torch.float64)
+        prof_on()
+        for _ in range(reps):
+            curfp.dsfrk(A, C)
     elif case == "nll-fused":
         X = torch.randn(n, k, device="cuda", generator=g)
         y = torch.randn(n, device="cuda", generator=g)

@@ -272,9 +272,22 @@ __global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 && BM >= 128) ? 1 : 
 #pragma unroll
       for (int g = 0; g < GM; ++g)
         lds4(&sa[buf][kk][swz<BK>(g * (BM / GM) + tr * 4, kk)], a + g * 4);
+      if constexpr (sizeof(T) == 8) {
+        // FP64: column pairs 2 tc + 32 h, so that consecutive lanes read
+        // consecutive 16-byte pairs (groups of four doubles would put the
+        // lanes 32 bytes apart and conflict)
 #pragma unroll
-      for (int g = 0; g < GN; ++g)
-        lds4(&sb[buf][kk][swz<BK>(g * (BN / GN) + tc * 4, kk)], b + g * 4);
+        for (int h = 0; h < TN / 2; ++h) {
+          const double2 v =
+              *reinterpret_cast<const double2*>(&sb[buf][kk][swz<BK>(tc * 2 + 32 * h, kk)]);
+          b[2 * h] = v.x;
+          b[2 * h + 1] = v.y;
+        }
+      } else {
+#pragma unroll
+        for (int g = 0; g < GN; ++g)
+          lds4(&sb[buf][kk][swz<BK>(g * (BN / GN) + tc * 4, kk)], b + g * 4);
+      }
 #pragma unroll
       for (int i = 0; i < TM; ++i)
 #pragma unroll
@@ -292,7 +305,8 @@ __global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 && BM >= 128) ? 1 : 
     if (gi >= P.m) continue;
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
-      const int gj = n0 + (j / 4) * (BN / GN) + tc * 4 + (j % 4);
+      const int gj = sizeof(T) == 8 ? n0 + tc * 2 + 32 * (j / 2) + (j % 2)
+                                    : n0 + (j / 4) * (BN / GN) + tc * 4 + (j % 4);
       if (gj >= P.n) continue;
       if (P.c_lower && gj > gi) continue;
       T* c = P.C + (int64_t)gi * P.c_rs + (int64_t)gj * P.c_cs;
