@@ -43,6 +43,7 @@ SIGNATURES = {
                         ctypes.POINTER(_f), _p, _i],
     "curfpGetKernelLaunchCount": [_h, ctypes.POINTER(ctypes.c_longlong)],
     "curfpReleaseWorkspace": [_h],
+    "curfpDiagWaitTimeout": [_h, ctypes.POINTER(ctypes.c_int)],
     "curfpDsfrk": [_h, _i, _i, _i, _i, _i, ctypes.POINTER(_d), _p, _i, ctypes.POINTER(_d), _p],
     "curfpDsfr2k": [_h, _i, _i, _i, _i, _i, ctypes.POINTER(_d), _p, _i, _p, _i,
                     ctypes.POINTER(_d), _p],

@@ -210,6 +210,17 @@ curfpStatus_t curfpReleaseWorkspace(curfpHandle_t handle) {
   return ok ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
 }
 
+curfpStatus_t curfpDiagWaitTimeout(curfpHandle_t handle, int* err_code) {
+  if (!handle || !err_code) return CURFP_STATUS_INVALID_VALUE;
+  if (!reset_info(handle)) return CURFP_STATUS_EXECUTION_FAILED;
+  const int rc = rfp::wave_wait_selftest(handle);
+  int info = 0, err = 0;
+  if (!read_info(handle, &info, &err)) return CURFP_STATUS_EXECUTION_FAILED;
+  *err_code = err;
+  if (rc) return status_of(rc);
+  return err ? CURFP_STATUS_EXECUTION_FAILED : CURFP_STATUS_SUCCESS;
+}
+
 // src/curfp_handle.cpp:37-43
 curfpStatus_t curfpSetStream(curfpHandle_t handle, cudaStream_t stream) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;

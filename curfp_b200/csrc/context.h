@@ -76,6 +76,10 @@ int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, Vie
 // (cleared here on the stream); no allocation.
 int launch_trsm_wave_fixed(curfpContext* ctx, const int* abort_flag, View L, int n, View B,
                            int m, float alpha, const float* W, int* sync, size_t sync_words);
+// Bounded-wait self-test of the wavefront solve (exec_cuda.cu): launches a
+// solve whose first block row never runs; its dependents time out (~2 s) and
+// set error code 5 in ctx->d_info[1].
+int wave_wait_selftest(curfpContext* ctx);
 // Whether a contraction of this size goes to the tensor-core path.
 bool tc_worthwhile(int m, int n, int k);
 

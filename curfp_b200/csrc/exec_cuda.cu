@@ -314,6 +314,35 @@ int CudaExecT<T>::trsm_wave(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const
 template class CudaExecT<float>;
 template class CudaExecT<double>;
 
+// Bounded-wait self-test: a wavefront solve of three 64-row block rows in
+// which the CTA of block row 0 is never launched (the ticket counter starts
+// at 1), so block rows 1 and 2 wait on a flag that nothing sets.  Their
+// waits give up after ~2 s, set error code 5 in the handle's error word and
+// return; the caller reads the word.  All buffers are zeroed first.
+int wave_wait_selftest(curfpContext* ctx) {
+  constexpr int n = 3 * ktrsv::NB, m = 1, nblk = 3;
+  const size_t fl = (size_t)n * n + n * m + (size_t)nblk * kInvStride;
+  const size_t bytes = fl * sizeof(float) + (1 + nblk) * sizeof(int);
+  char* buf = static_cast<char*>(grow_buffer(ctx, &ctx->ws, &ctx->ws_bytes, bytes));
+  if (!buf) return 2;
+  if (cudaMemsetAsync(buf, 0, bytes, ctx->stream) != cudaSuccess) return 4;
+  float* Lp = reinterpret_cast<float*>(buf);
+  float* Bp = Lp + (size_t)n * n;
+  float* Wp = Bp + n * m;
+  int* sync = reinterpret_cast<int*>(Wp + (size_t)nblk * kInvStride);
+  static const int one = 1;
+  if (cudaMemcpyAsync(sync, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream) !=
+      cudaSuccess)
+    return 4;
+  constexpr int smem = ktrsv::smem_bytes<float, 8>();
+  static const bool attr = smem_attr(ktrsv::trsm_wave<float, 8>, ktrsv::smem_limit<float, 8>());
+  if (!attr) return 4;
+  ktrsv::trsm_wave<float, 8><<<nblk - 1, 256, smem, ctx->stream>>>(
+      View{Lp, n, 1}, n, View{Bp, 1, n}, m, 1.0f, Wp, sync, ctx->d_info + 1, nullptr);
+  ++ctx->launches;
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
 int launch_trsm_wave_fixed(curfpContext* ctx, const int* abort_flag, View L, int n, View B,
                            int m, float alpha, const float* W, int* sync, size_t sync_words) {
   if (n <= 0 || m <= 0) return 0;

@@ -140,6 +140,16 @@ def release_workspace() -> None:
     check(h._lib.curfpReleaseWorkspace(h.ptr))
 
 
+def diag_wait_timeout() -> tuple:
+    """Self-test of the kernels' bounded waits (~2 s): a wavefront solve whose
+    first block row never runs; returns (status, error code), which is
+    (CURFP_STATUS_EXECUTION_FAILED, 5) when the waits give up as designed."""
+    h = _get_handle()
+    code = ctypes.c_int(0)
+    st = h._lib.curfpDiagWaitTimeout(h.ptr, ctypes.byref(code))
+    return int(st), code.value
+
+
 KERNEL_CLASSES = ["sgemm", "tc_gemm", "tc_stage", "potrf_tile", "trtri", "lauum",
                   "pack", "diag", "symm_acc64", "trsv_wave", "norm"]
 

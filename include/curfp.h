@@ -367,6 +367,14 @@ curfpStatus_t curfpReleaseWorkspace(curfpHandle_t handle);
 /* Number of kernels launched through this handle since its creation. */
 curfpStatus_t curfpGetKernelLaunchCount(curfpHandle_t handle, long long *count);
 
+/* Self-test of the kernels' failure detection (no counterpart in the
+ * reference): launches a small wavefront solve whose first block row never
+ * runs, so the CTAs of the next rows wait on a flag that nothing sets.  Their
+ * waits are bounded: after ~2 s they record error code 5 in the handle's
+ * error word and return, and the call reports CURFP_STATUS_EXECUTION_FAILED
+ * with *err_code = 5.  The context stays usable.  Takes ~2 s. */
+curfpStatus_t curfpDiagWaitTimeout(curfpHandle_t handle, int *err_code);
+
 /* Optional kernel timing: when enabled, every kernel this handle launches is
  * bracketed by CUDA events on its stream and attributed to a kernel class
  * (0 SIMT GEMM, 1 tensor-core contraction, 2 tensor-core operand staging,
