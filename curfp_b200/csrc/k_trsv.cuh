@@ -222,7 +222,8 @@ __device__ __forceinline__ int wait_flag(const int* f, int* err) {
 // sync layout: sync[0] = ticket counter, sync[1 + b*nchunk + c] = flag of
 // block row b, chunk c (0 = not ready, 1 = ready, -1 = poisoned).
 // All zero at launch.  W: kInvStride elements per block row ([W_j | M_j]).
-// FP32: two CTAs per SM (102 KB of shared memory each); FP64: one (204 KB).
+// FP32: up to two CTAs per SM (104 KB of shared memory each; launches of at
+// most two chunks ask for one CTA per SM); FP64: one (204 KiB).
 template <typename T, int NC = 64>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     trsm_wave(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const T* __restrict__ W,
