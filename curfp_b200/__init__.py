@@ -28,7 +28,7 @@ __all__ = [
     "strttf_raw", "stfttr", "stfttr_raw", "ssfr2k", "ssfr2k_raw", "CurfpError",
     "NORM_MAX", "NORM_ONE", "NORM_FRO", "slansf", "slansf_raw", "spfcon", "spfcon_raw",
     "spftrf_rcond", "SIDE_LEFT", "SIDE_RIGHT", "ssfmm", "ssfmm_raw", "ssfmv", "ssfmv_raw",
-    "ssfr", "ssfr_raw", "ssfr2", "ssfr2_raw",
+    "ssfr", "ssfr_raw", "ssfr2", "ssfr2_raw", "set_math_mode", "get_math_mode",
 ]
 
 # Enum values of include/curfp.h (reference curfp/_ext.cpp:869-877).
@@ -64,6 +64,17 @@ class Handle:
         check(self._lib.curfpGetStream(self._h, ctypes.byref(s)))
         return int(s.value or 0)
 
+    def set_math_mode(self, mode: str) -> None:
+        """Contraction arithmetic of the FP32 routines on this handle:
+        "bf16x3" (default: split-BF16 tensor-core contractions) or "fp32"
+        (FP32 FMA on the SIMT cores)."""
+        check(self._lib.curfpSetMathMode(self._h, _MATH_MODES[_math_key(mode)]))
+
+    def get_math_mode(self) -> str:
+        m = ctypes.c_int(0)
+        check(self._lib.curfpGetMathMode(self._h, ctypes.byref(m)))
+        return {v: k for k, v in _MATH_MODES.items()}[m.value]
+
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
             self._lib.curfpDestroy(self._h)
@@ -82,6 +93,15 @@ class Handle:
         return False
 
 
+_MATH_MODES = {"fp32": 0, "bf16x3": 1}
+
+
+def _math_key(mode: str) -> str:
+    if mode not in _MATH_MODES:
+        raise ValueError(f"math mode must be one of {sorted(_MATH_MODES)}, got {mode!r}")
+    return mode
+
+
 _handles: dict = {}
 
 
@@ -90,6 +110,17 @@ def _get_handle() -> Handle:
     if dev not in _handles:
         _handles[dev] = Handle()
     return _handles[dev]
+
+
+def set_math_mode(mode: str) -> None:
+    """Contraction arithmetic of the FP32 routines on the current device's
+    handle: "bf16x3" (the default, split-BF16 tensor cores) or "fp32" (SIMT
+    FP32 FMA).  No counterpart in the reference."""
+    _get_handle().set_math_mode(mode)
+
+
+def get_math_mode() -> str:
+    return _get_handle().get_math_mode()
 
 
 def set_stream(stream) -> None:

@@ -14,6 +14,7 @@
 #include "k_pack.cuh"
 #include "k_refine.cuh"
 #include "k_symv.cuh"
+#include "status.cuh"
 
 using rfp::CudaExec;
 using rfp::Geometry;
@@ -31,29 +32,20 @@ inline curfpStatus_t status_of(int rc) {
   }
 }
 
+// Contraction arithmetic of a drop-in routine: the handle's math mode for
+// FP32 (curfpSetMathMode), SIMT FP64 for the D twins.
+template <typename T>
+inline int drop_math(curfpHandle_t h) {
+  return sizeof(T) == sizeof(float) ? h->math : 0;
+}
+
 inline int n1_of(int n, int lower) {
   return (n & 1) ? (lower ? n - n / 2 : n / 2) : n / 2;
 }
 
-__global__ void set_int2(int* p, int v0, int v1) { p[0] = v0; p[1] = v1; }
-
-// Reset the info word (INT_MAX = no failure) and the kernel error word.
-inline int reset_info(curfpHandle_t h) {
-  set_int2<<<1, 1, 0, h->stream>>>(h->d_info, INT_MAX, 0);
-  ++h->launches;
-  return ok_launch();
-}
-
-// Synchronise and read both words back.
+inline int reset_info(curfpHandle_t h) { return rfp::status::reset(h); }
 inline int read_info(curfpHandle_t h, int* info, int* err) {
-  int w[2] = {0, 0};
-  if (cudaMemcpyAsync(w, h->d_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream) !=
-          cudaSuccess ||
-      cudaStreamSynchronize(h->stream) != cudaSuccess)
-    return 0;
-  *info = w[0];
-  *err = w[1];
-  return 1;
+  return rfp::status::read(h, info, err);
 }
 
 // Launch the FP64-accumulated symmetric multiply; when the row blocks alone
@@ -151,18 +143,28 @@ curfpStatus_t curfpCreate(curfpHandle_t* handle) {
   curfpContext* ctx = new (std::nothrow) curfpContext();
   if (!ctx) return CURFP_STATUS_ALLOC_FAILED;
   if (cudaGetDevice(&ctx->device) != cudaSuccess ||
-      cudaMalloc(&ctx->d_info, 2 * sizeof(int)) != cudaSuccess) {
+      cudaMalloc(&ctx->d_info, 2 * sizeof(int)) != cudaSuccess ||
+      cudaMemset(ctx->d_info, 0, 2 * sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
+    if (ctx->d_info) cudaFree(ctx->d_info);
     delete ctx;
     return CURFP_STATUS_NOT_INITIALIZED;
   }
-  // Keep memory released by the stream-ordered workspace in the device pool
-  // (workspaces grow with the problem; re-mapping on every growth is slow).
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
-    uint64_t keep = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  // Workspaces come from a pool of the handle's own, which keeps memory
+  // released by a growing workspace (re-mapping on every growth is slow);
+  // the device's default pool is not touched.
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = ctx->device;
+  if (cudaMemPoolCreate(&ctx->pool, &props) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(ctx->d_info);
+    delete ctx;
+    return CURFP_STATUS_NOT_INITIALIZED;
   }
+  uint64_t keep = UINT64_MAX;
+  cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
   cudaGetLastError();
   *handle = ctx;
   return CURFP_STATUS_SUCCESS;
@@ -180,6 +182,8 @@ curfpStatus_t curfpDestroy(curfpHandle_t handle) {
   if (handle->tsv) cudaFree(handle->tsv);
   if (handle->wsg) cudaFree(handle->wsg);
   if (handle->d_info) cudaFree(handle->d_info);
+  if (handle->pool) cudaMemPoolDestroy(handle->pool);
+  cudaGetLastError();
   delete handle;
   return CURFP_STATUS_SUCCESS;
 }
@@ -203,9 +207,7 @@ curfpStatus_t curfpReleaseWorkspace(curfpHandle_t handle) {
     *bufs[i] = nullptr;
     *sizes[i] = 0;
   }
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, handle->device) == cudaSuccess)
-    ok &= cudaMemPoolTrimTo(pool, 0) == cudaSuccess;
+  ok &= cudaMemPoolTrimTo(handle->pool, 0) == cudaSuccess;
   cudaGetLastError();
   return ok ? CURFP_STATUS_SUCCESS : CURFP_STATUS_EXECUTION_FAILED;
 }
@@ -213,12 +215,14 @@ curfpStatus_t curfpReleaseWorkspace(curfpHandle_t handle) {
 curfpStatus_t curfpDiagWaitTimeout(curfpHandle_t handle, int* err_code) {
   if (!handle || !err_code) return CURFP_STATUS_INVALID_VALUE;
   if (!reset_info(handle)) return CURFP_STATUS_EXECUTION_FAILED;
-  const int rc = rfp::wave_wait_selftest(handle);
-  int info = 0, err = 0;
-  if (!read_info(handle, &info, &err)) return CURFP_STATUS_EXECUTION_FAILED;
-  *err_code = err;
-  if (rc) return status_of(rc);
-  return err ? CURFP_STATUS_EXECUTION_FAILED : CURFP_STATUS_SUCCESS;
+  // The error word is read and cleared by the same check that every routine
+  // with bounded waits runs before it returns (status.cuh), so the code
+  // reported here is the one a real solve would surface, and later calls on
+  // this handle do not inherit it.
+  rfp::status::WaitCheck wc(handle);
+  const int rc = wc.finish(rfp::wave_wait_selftest(handle));
+  *err_code = wc.err;
+  return status_of(rc);
 }
 
 // src/curfp_handle.cpp:37-43
@@ -260,16 +264,19 @@ static curfpStatus_t ssfrk_impl(curfpHandle_t handle, curfpOperation_t transr,
   if (lda < (trans == CURFP_OP_N ? nmax : (k > 1 ? k : 1)))
     return CURFP_STATUS_INVALID_VALUE;
   rfp::CudaExecT<T> ex(handle);
-  return status_of(rfp::plan::ssfrk(ex, transr == CURFP_OP_T, lower,
-                                    trans == CURFP_OP_T, n, k, *alpha, A, lda,
-                                    *beta, C, math));
+  rfp::status::WaitCheck wc(handle);
+  return status_of(wc.finish(rfp::plan::ssfrk(ex, transr == CURFP_OP_T, lower,
+                                              trans == CURFP_OP_T, n, k, *alpha, A, lda,
+                                              *beta, C, math)));
 }
 
 curfpStatus_t curfpSsfrk(curfpHandle_t handle, curfpOperation_t transr,
                          curfpFillMode_t uplo, curfpOperation_t trans, int n,
                          int k, const float* alpha, const float* A, int lda,
                          const float* beta, float* C) {
-  return ssfrk_impl(handle, transr, uplo, trans, n, k, alpha, A, lda, beta, C, 0);
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  return ssfrk_impl(handle, transr, uplo, trans, n, k, alpha, A, lda, beta, C,
+                    drop_math<float>(handle));
 }
 
 curfpStatus_t curfpSsfrkEx(curfpHandle_t handle, curfpOperation_t transr,
@@ -303,9 +310,10 @@ static curfpStatus_t sfr2k_impl(curfpHandle_t handle, curfpOperation_t transr,
   const int need = trans == CURFP_OP_N ? nmax : (k > 1 ? k : 1);
   if (lda < need || ldb < need) return CURFP_STATUS_INVALID_VALUE;
   rfp::CudaExecT<T> ex(handle);
-  return status_of(rfp::plan::ssfr2k(ex, transr == CURFP_OP_T, lower,
-                                     trans == CURFP_OP_T, n, k, *alpha, A, lda,
-                                     B, ldb, *beta, C));
+  rfp::status::WaitCheck wc(handle);
+  return status_of(wc.finish(rfp::plan::ssfr2k(ex, transr == CURFP_OP_T, lower,
+                                               trans == CURFP_OP_T, n, k, *alpha, A, lda,
+                                               B, ldb, *beta, C, drop_math<T>(handle))));
 }
 
 curfpStatus_t curfpSsfr2k(curfpHandle_t handle, curfpOperation_t transr,
@@ -342,7 +350,8 @@ static curfpStatus_t spftrf_impl(curfpHandle_t handle, curfpOperation_t transr,
 
 curfpStatus_t curfpSpftrf(curfpHandle_t handle, curfpOperation_t transr,
                           curfpFillMode_t uplo, int n, float* A, int* info) {
-  return spftrf_impl(handle, transr, uplo, n, A, info, 0);
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  return spftrf_impl(handle, transr, uplo, n, A, info, drop_math<float>(handle));
 }
 
 curfpStatus_t curfpSpftrfEx(curfpHandle_t handle, curfpOperation_t transr,
@@ -365,8 +374,9 @@ static curfpStatus_t pftrs_impl(curfpHandle_t handle, curfpOperation_t transr,
   const int n1 = n1_of(n, lower), nmax = n1 > n - n1 ? n1 : n - n1;
   if (ldb < nmax) return CURFP_STATUS_INVALID_VALUE;
   rfp::CudaExecT<T> ex(handle);
-  return status_of(rfp::plan::spftrs(ex, transr == CURFP_OP_T, lower, n, nrhs,
-                                     A, B, ldb));
+  rfp::status::WaitCheck wc(handle);
+  return status_of(wc.finish(rfp::plan::spftrs(ex, transr == CURFP_OP_T, lower, n, nrhs,
+                                               A, B, ldb, drop_math<T>(handle))));
 }
 
 curfpStatus_t curfpSpftrs(curfpHandle_t handle, curfpOperation_t transr,
@@ -393,7 +403,8 @@ static curfpStatus_t pftri_impl(curfpHandle_t handle, curfpOperation_t transr,
   if (!read_info(handle, &h, &err)) return CURFP_STATUS_EXECUTION_FAILED;
   if (h != INT_MAX) return CURFP_STATUS_EXECUTION_FAILED;
   rfp::CudaExecT<T> ex(handle);
-  return status_of(rfp::plan::spftri(ex, tr, lower, n, arf));
+  rfp::status::WaitCheck wc(handle);
+  return status_of(wc.finish(rfp::plan::spftri(ex, tr, lower, n, arf, drop_math<T>(handle))));
 }
 
 curfpStatus_t curfpSpftri(curfpHandle_t handle, curfpOperation_t transr,
@@ -688,9 +699,9 @@ curfpStatus_t curfpSsfrkBackward(curfpHandle_t handle, curfpOperation_t transr,
 
 // Cotangent of the stored elements of A from that of its Cholesky factor
 // (rfp::plan::spftrf_backward), packed to RFP with the diagonal halved.
-curfpStatus_t curfpSpftrfBackward(curfpHandle_t handle, curfpOperation_t transr,
-                                  curfpFillMode_t uplo, int n, const float* L,
-                                  const float* Lbar, float* Abar, curfpMath_t math) {
+static curfpStatus_t spftrf_backward_body(curfpHandle_t handle, curfpOperation_t transr,
+                                          curfpFillMode_t uplo, int n, const float* L,
+                                          const float* Lbar, float* Abar, curfpMath_t math) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (n < 0) return CURFP_STATUS_INVALID_VALUE;
   if (math != CURFP_MATH_FP32 && math != CURFP_MATH_SPLIT_BF16) return CURFP_STATUS_INVALID_VALUE;
@@ -709,10 +720,10 @@ curfpStatus_t curfpSpftrfBackward(curfpHandle_t handle, curfpOperation_t transr,
 
 // X = A^-1 B with A = L L^T:  Bbar := A^-1 Xbar and
 // Lbar := -tril(Bbar (L^T X)^T + X (L^T Bbar)^T) on the factor's stored elements.
-curfpStatus_t curfpSpftrsBackward(curfpHandle_t handle, curfpOperation_t transr,
-                                  curfpFillMode_t uplo, int n, int nrhs, const float* L,
-                                  const float* X, int ldx, const float* Xbar, int ldxbar,
-                                  float* Bbar, int ldbbar, float* Lbar) {
+static curfpStatus_t spftrs_backward_body(curfpHandle_t handle, curfpOperation_t transr,
+                                          curfpFillMode_t uplo, int n, int nrhs, const float* L,
+                                          const float* X, int ldx, const float* Xbar, int ldxbar,
+                                          float* Bbar, int ldbbar, float* Lbar) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (n < 0 || nrhs < 0) return CURFP_STATUS_INVALID_VALUE;
   if (n == 0) return CURFP_STATUS_SUCCESS;
@@ -754,10 +765,10 @@ curfpStatus_t curfpSpftrsBackward(curfpHandle_t handle, curfpOperation_t transr,
 }
 
 // Mixed-precision refinement around spftrs (see include/curfp.h).
-curfpStatus_t curfpSpftrsRefine(curfpHandle_t handle, curfpOperation_t transr,
-                                curfpFillMode_t uplo, int n, int nrhs, const float* Aorig,
-                                const float* factor, float* B, int ldb, int max_iter,
-                                int* iters) {
+static curfpStatus_t refine_body(curfpHandle_t handle, curfpOperation_t transr,
+                                 curfpFillMode_t uplo, int n, int nrhs, const float* Aorig,
+                                 const float* factor, float* B, int ldb, int max_iter,
+                                 int* iters) {
   if (iters) *iters = 0;
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
   if (n < 0 || nrhs < 0 || ldb < 1 || max_iter < 0) return CURFP_STATUS_INVALID_VALUE;
@@ -822,6 +833,55 @@ curfpStatus_t curfpSpftrsRefine(curfpHandle_t handle, curfpOperation_t transr,
       if (d <= 0x1p-22f * x) break;
     }
   }
+  return CURFP_STATUS_SUCCESS;
+}
+
+// The three entry points above, each under a check of the kernel error word
+// (status.cuh): a wait that ran out surfaces as EXECUTION_FAILED.
+curfpStatus_t curfpSpftrfBackward(curfpHandle_t handle, curfpOperation_t transr,
+                                  curfpFillMode_t uplo, int n, const float* L,
+                                  const float* Lbar, float* Abar, curfpMath_t math) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  return rfp::status::checked(handle, [&] {
+    return spftrf_backward_body(handle, transr, uplo, n, L, Lbar, Abar, math);
+  });
+}
+
+curfpStatus_t curfpSpftrsBackward(curfpHandle_t handle, curfpOperation_t transr,
+                                  curfpFillMode_t uplo, int n, int nrhs, const float* L,
+                                  const float* X, int ldx, const float* Xbar, int ldxbar,
+                                  float* Bbar, int ldbbar, float* Lbar) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  return rfp::status::checked(handle, [&] {
+    return spftrs_backward_body(handle, transr, uplo, n, nrhs, L, X, ldx, Xbar, ldxbar, Bbar,
+                                ldbbar, Lbar);
+  });
+}
+
+curfpStatus_t curfpSpftrsRefine(curfpHandle_t handle, curfpOperation_t transr,
+                                curfpFillMode_t uplo, int n, int nrhs, const float* Aorig,
+                                const float* factor, float* B, int ldb, int max_iter,
+                                int* iters) {
+  if (iters) *iters = 0;
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  return rfp::status::checked(handle, [&] {
+    return refine_body(handle, transr, uplo, n, nrhs, Aorig, factor, B, ldb, max_iter, iters);
+  });
+}
+
+// Math mode of the drop-in FP32 routines (curfpSsfrk, curfpSsfr2k,
+// curfpSpftrf, curfpSpftrs, curfpSpftri); include/curfp.h.
+curfpStatus_t curfpSetMathMode(curfpHandle_t handle, curfpMath_t math) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (math != CURFP_MATH_FP32 && math != CURFP_MATH_SPLIT_BF16) return CURFP_STATUS_INVALID_VALUE;
+  handle->math = (int)math;
+  return CURFP_STATUS_SUCCESS;
+}
+
+curfpStatus_t curfpGetMathMode(curfpHandle_t handle, curfpMath_t* math) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (!math) return CURFP_STATUS_INVALID_VALUE;
+  *math = (curfpMath_t)handle->math;
   return CURFP_STATUS_SUCCESS;
 }
 

@@ -4,8 +4,10 @@
 // (src/curfp_internal.h:11-14); this one holds what the native kernels need:
 // the stream, the device, one device-side info word (pivot failures, also used
 // as the abort flag that makes later kernels of a failed factorization return
-// immediately), a grow-only stream-ordered workspace and the staging buffers
-// of the split-BF16 path.
+// immediately), a kernel error word, grow-only stream-ordered workspaces and
+// the staging buffers of the split-BF16 path.  Workspaces come from the
+// handle's own memory pool (created with the handle, kept across calls), so
+// the device's default pool and its settings are left to the caller.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -17,6 +19,9 @@
 struct curfpContext {
   cudaStream_t stream = nullptr;
   int device = 0;
+  cudaMemPool_t pool = nullptr;  // the handle's workspace pool
+  int math = 1;            // contraction arithmetic of the drop-in routines (curfpSetMathMode)
+  long long wait_launches = 0;  // kernels with bounded waits launched (status.cuh)
   int* d_info = nullptr;   // [0]: INT_MAX = no pivot failure; [1]: kernel error code
   void* ws = nullptr;      // TRSM diagonal-block inverses and other scratch
   size_t ws_bytes = 0;
@@ -54,6 +59,8 @@ class CudaExecT : public ExecT<T> {
   int inplace_rows() const override { return 64; }
   int gemm_shared(ViewT<T> X, int rows, int k, const SharedTaskT<T>* t, int count,
                   int math) override;
+  int gemm_pair(ViewT<T> X, ViewT<T> Y, int rows, int k, const SharedTaskT<T>* t, int count,
+                int math) override;
   int trsm_wave(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const T* W) override;
   int mirror_lower(ViewT<T> D, int n) override;
 

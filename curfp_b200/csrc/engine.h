@@ -130,6 +130,31 @@ class ExecT {
     }
     return gemm(p, count);
   }
+  // Symmetric rank-2k blocks over two operand matrices X, Y (rows x k):
+  // C_t := alpha_t (X[a_row0:+m, :] Y[b_row0:+n, :]^T + Y[a_row0:+m, :]
+  // X[b_row0:+n, :]^T) + beta_t C_t.  The default lowers them to two-product
+  // gemm() problems; the CUDA executor runs large ones as two tensor-core
+  // contractions.
+  virtual int gemm_pair(ViewT<T> X, ViewT<T> Y, int rows, int k, const SharedTaskT<T>* t,
+                        int count, int math) {
+    (void)rows;
+    GemmProbT<T> p[kMaxBatch];
+    if (count > kMaxBatch) return 3;
+    for (int i = 0; i < count; ++i) {
+      GemmProbT<T>& g = p[i];
+      g.A = sub(X, t[i].a_row0, 0);
+      g.B = tr(sub(Y, t[i].b_row0, 0));
+      g.A2 = sub(Y, t[i].a_row0, 0);
+      g.B2 = tr(sub(X, t[i].b_row0, 0));
+      g.C = t[i].C;
+      g.m = t[i].m; g.n = t[i].n; g.k = k; g.k2 = k;
+      g.alpha = t[i].alpha; g.beta = t[i].beta;
+      g.c_lower = t[i].c_lower; g.inplace = 0;
+      g.a_tri = g.b_tri = g.a2_tri = g.b2_tri = 0;
+      g.math = math;
+    }
+    return gemm(p, count);
+  }
 };
 using Exec = ExecT<float>;
 
@@ -168,14 +193,14 @@ int ssfrk(ExecT<T>& ex, int transr, int lower, int trans, int n, int k,
 template <typename T>
 int ssfr2k(ExecT<T>& ex, int transr, int lower, int trans, int n, int k,
            Scalar<T> alpha, const T* A, int lda, const T* B, int ldb,
-           Scalar<T> beta, T* C);
+           Scalar<T> beta, T* C, int math = 0);
 template <typename T>
 int spftrf(ExecT<T>& ex, int transr, int lower, int n, T* A, int math = 0);
 template <typename T>
 int spftrs(ExecT<T>& ex, int transr, int lower, int n, int nrhs, const T* A,
            T* B, int ldb, int math = 0);
 template <typename T>
-int spftri(ExecT<T>& ex, int transr, int lower, int n, T* A);
+int spftri(ExecT<T>& ex, int transr, int lower, int n, T* A, int math = 0);
 // In place: the RFP factor L := L^-1 (the first half of spftri).
 template <typename T>
 int rfp_trtri(ExecT<T>& ex, int transr, int lower, int n, T* A, int math = 0);

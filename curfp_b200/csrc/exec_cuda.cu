@@ -24,10 +24,10 @@ void* grow_buffer(curfpContext* ctx, void** buf, size_t* cur, size_t bytes) {
   size_t want = bytes < 256 ? 256 : bytes;
   if (*cur && want < *cur + *cur / 2) want = *cur + *cur / 2;
   void* p = nullptr;
-  if (cudaMallocAsync(&p, want, ctx->stream) != cudaSuccess) {
+  if (cudaMallocFromPoolAsync(&p, want, ctx->pool, ctx->stream) != cudaSuccess) {
     cudaGetLastError();
     want = bytes;  // retry without the growth margin
-    if (cudaMallocAsync(&p, want, ctx->stream) != cudaSuccess) {
+    if (cudaMallocFromPoolAsync(&p, want, ctx->pool, ctx->stream) != cudaSuccess) {
       cudaGetLastError();
       *cur = 0;
       return nullptr;
@@ -150,6 +150,40 @@ int CudaExecT<float>::gemm_shared(View X, int rows, int k, const SharedTask* t, 
     orient(A, ar, B, br, tt[i]);  // shared operand: swapping keeps B == A
   }
   return tc_contract(ctx_, abort_, X, rows, View{nullptr, 0, 0}, rows, k, tt, count);
+}
+
+template <>
+int CudaExecT<double>::gemm_pair(ViewT<double> X, ViewT<double> Y, int rows, int k,
+                                 const SharedTaskT<double>* t, int count, int math) {
+  return ExecT<double>::gemm_pair(X, Y, rows, k, t, count, math);  // SIMT FP64 only
+}
+
+// Rank-2k blocks on the tensor cores: two split-BF16 contractions over all
+// blocks.  Launch 0 contracts (X, Y), launch 1 (Y, X).  A task whose C is
+// column-contiguous is written transposed (orient()): C^T = Y[b] X[a]^T +
+// X[b] Y[a]^T takes its two products from the launches in the other order,
+// which sums to the same result.  beta applies in launch 0 only.
+template <>
+int CudaExecT<float>::gemm_pair(View X, View Y, int rows, int k, const SharedTask* t, int count,
+                                int math) {
+  bool tc = math != 0 && count <= kMaxBatch;
+  for (int i = 0; tc && i < count; ++i)
+    tc = tc_worthwhile(t[i].m, t[i].n, k);
+  if (!tc) return Exec::gemm_pair(X, Y, rows, k, t, count, math);
+  SharedTask tt[kMaxBatch];
+  for (int pass = 0; pass < 2; ++pass) {
+    View P = pass ? Y : X, Q = pass ? X : Y;
+    for (int i = 0; i < count; ++i) {
+      tt[i] = t[i];
+      if (pass) tt[i].beta = 1.0f;
+      View a = P, b = Q;
+      int r0 = rows, r1 = rows;
+      orient(a, r0, b, r1, tt[i]);  // only the task's rows and C are used here
+    }
+    const int rc = tc_contract(ctx_, abort_, P, rows, Q, rows, k, tt, count);
+    if (rc) return rc;
+  }
+  return 0;
 }
 
 template <>
@@ -298,6 +332,7 @@ int launch_wave(curfpContext* ctx, const int* abort_flag, ViewT<T> L, int n, Vie
   ktrsv::trsm_wave<T, NC><<<nblk * nchunk, 256, smem_launch, ctx->stream>>>(
       L, n, B, m, alpha, W, sync, ctx->d_info + 1, abort_flag);
   ++ctx->launches;
+  ++ctx->wait_launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 }  // namespace
@@ -340,6 +375,7 @@ int wave_wait_selftest(curfpContext* ctx) {
   ktrsv::trsm_wave<float, 8><<<nblk - 1, 256, smem, ctx->stream>>>(
       View{Lp, n, 1}, n, View{Bp, 1, n}, m, 1.0f, Wp, sync, ctx->d_info + 1, nullptr);
   ++ctx->launches;
+  ++ctx->wait_launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
@@ -357,6 +393,7 @@ int launch_trsm_wave_fixed(curfpContext* ctx, const int* abort_flag, View L, int
   ktrsv::trsm_wave<float><<<nblk * nchunk, 256, ktrsv::SMEM, ctx->stream>>>(
       L, n, B, m, alpha, W, sync, ctx->d_info + 1, abort_flag);
   ++ctx->launches;
+  ++ctx->wait_launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 

@@ -15,6 +15,7 @@
 
 #include "../../include/curfp.h"
 #include "context.h"
+#include "status.cuh"
 #include "engine.h"
 #include "k_nll.cuh"
 
@@ -36,11 +37,10 @@ inline int grid_for(int64_t work) {
 
 }  // namespace
 
-curfpStatus_t curfpSgpnllBackward(curfpHandle_t handle, curfpOperation_t transr,
-                                  curfpFillMode_t uplo, int n, int d, float s, const float* L,
-                                  const float* X, int ldx, const float* alpha, const float* g,
-                                  float* Xbar, int ldxbar, double* sums, curfpMath_t math) {
-  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+static curfpStatus_t nll_body(curfpHandle_t handle, curfpOperation_t transr,
+                              curfpFillMode_t uplo, int n, int d, float s, const float* L,
+                              const float* X, int ldx, const float* alpha, const float* g,
+                              float* Xbar, int ldxbar, double* sums, curfpMath_t math) {
   if (n < 0 || d < 0 || ldx < (d > 1 ? d : 1) || ldxbar < (d > 1 ? d : 1))
     return CURFP_STATUS_INVALID_VALUE;
   if (math != CURFP_MATH_FP32 && math != CURFP_MATH_SPLIT_BF16) return CURFP_STATUS_INVALID_VALUE;
@@ -91,4 +91,16 @@ curfpStatus_t curfpSgpnllBackward(curfpHandle_t handle, curfpOperation_t transr,
   handle->launches += 3;
   return cudaGetLastError() == cudaSuccess ? CURFP_STATUS_SUCCESS
                                            : CURFP_STATUS_EXECUTION_FAILED;
+}
+
+// The body above under a check of the kernel error word (status.cuh).
+curfpStatus_t curfpSgpnllBackward(curfpHandle_t handle, curfpOperation_t transr,
+                                  curfpFillMode_t uplo, int n, int d, float s, const float* L,
+                                  const float* X, int ldx, const float* alpha, const float* g,
+                                  float* Xbar, int ldxbar, double* sums, curfpMath_t math) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  return rfp::status::checked(handle, [&] {
+    return nll_body(handle, transr, uplo, n, d, s, L, X, ldx, alpha, g, Xbar, ldxbar, sums,
+                    math);
+  });
 }

@@ -19,14 +19,18 @@
 // different streams, or from different handles) race on the array.
 //
 // The device address of the array is fetched once per device with
-// cudaGetSymbolAddress on the first call made with that device current; make
-// that first call before any stream capture.
+// cudaGetSymbolAddress on the first call with a handle of that device (the
+// handle's device is made current for the lookup); make that first call
+// before any stream capture.  Each call synchronises the handle's stream
+// once, to read the kernel error word: a wavefront wait that ran out is
+// reported as CURFP_STATUS_EXECUTION_FAILED.
 #include <cuda_runtime.h>
 
 #include <mutex>
 
 #include "../../include/curfp.h"
 #include "context.h"
+#include "status.cuh"
 
 namespace {
 
@@ -43,14 +47,26 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 float* g_addr[kMaxDevices] = {};
 
-// Device address of g_solve_scratch for the current device (nullptr on error).
-float* scratch_address() {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+// Device address of g_solve_scratch on device `dev` (the handle's device,
+// whatever device is current in the calling thread); nullptr on error.  The
+// lookup runs with `dev` current and restores the caller's device.
+float* scratch_address(int dev) {
+  if (dev < 0 || dev >= kMaxDevices) return nullptr;
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_addr[dev]) {
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    if (prev != dev && cudaSetDevice(dev) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
     void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_solve_scratch) != cudaSuccess) {
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_solve_scratch);
+    if (prev != dev) cudaSetDevice(prev);
+    if (e != cudaSuccess) {
       cudaGetLastError();
       return nullptr;
     }
@@ -92,10 +108,14 @@ extern "C" curfpStatus_t curfpSpftrsNoAlloc(curfpHandle_t handle, curfpOperation
   const int n1 = (n & 1) ? (lower ? n - n / 2 : n / 2) : n / 2;
   const int nmax = n1 > n - n1 ? n1 : n - n1;
   if (ldb < nmax) return CURFP_STATUS_INVALID_VALUE;
-  float* scratch = scratch_address();
+  float* scratch = scratch_address(handle->device);
   if (!scratch) return CURFP_STATUS_EXECUTION_FAILED;
   NoAllocExec ex(handle, scratch);
-  const int rc = rfp::plan::spftrs(ex, transr == CURFP_OP_T, lower, n, nrhs, A, B, ldb);
+  // A wavefront wait that runs out leaves B partly solved and sets the
+  // handle's kernel error word; the word is read back (one stream
+  // synchronisation, no allocation) and reported as EXECUTION_FAILED.
+  rfp::status::WaitCheck wc(handle);
+  const int rc = wc.finish(rfp::plan::spftrs(ex, transr == CURFP_OP_T, lower, n, nrhs, A, B, ldb));
   switch (rc) {
     case 0: return CURFP_STATUS_SUCCESS;
     case 3: return CURFP_STATUS_INVALID_VALUE;

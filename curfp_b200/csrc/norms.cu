@@ -7,6 +7,7 @@
 
 #include "../../include/curfp.h"
 #include "context.h"
+#include "status.cuh"
 #include "engine.h"
 #include "k_norm.cuh"
 
@@ -138,7 +139,8 @@ static curfpStatus_t pfcon_impl(curfpHandle_t handle, curfpOperation_t transr,
   Stats hs;
   auto solve = [&]() -> curfpStatus_t {
     rfp::CudaExecT<T> ex(handle);
-    const int rc = rfp::plan::spftrs(ex, tr, lower, n, 1, arf, x, n);
+    rfp::status::WaitCheck wc(handle);
+    const int rc = wc.finish(rfp::plan::spftrs(ex, tr, lower, n, 1, arf, x, n));
     return rc == 0 ? CURFP_STATUS_SUCCESS
                    : (rc == 2 ? CURFP_STATUS_ALLOC_FAILED : CURFP_STATUS_EXECUTION_FAILED);
   };

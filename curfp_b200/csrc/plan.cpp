@@ -170,9 +170,9 @@ int lauum_lower(ExecT<T>& ex, ViewT<T> L, int n, int math) {
   ViewT<T> L21 = sub(L, n1, 0);
   int rc = lauum_lower(ex, L, n1, math);
   if (rc) return rc;
-  GemmProbT<T> p = gemm_prob(tr(L21), L21, L, n1, n1, n2, 1.0f, 1.0f, math);
-  p.c_lower = 1;
-  if ((rc = ex.gemm(&p, 1))) return rc;
+  // L11 += L21^T L21 (lower): a SYRK whose one operand is L21^T (n1 x n2)
+  SharedTaskT<T> t{0, 0, n1, n1, L, 1.0f, 1.0f, 1};
+  if ((rc = ex.gemm_shared(tr(L21), n1, n2, &t, 1, math))) return rc;
   if ((rc = trmm(ex, 1, 1, 1, sub(L, n1, n1), L21, n2, n1, 1.0f, math)))
     return rc;
   return lauum_lower(ex, sub(L, n1, n1), n2, math);
@@ -206,32 +206,24 @@ int ssfrk(ExecT<T>& ex, int transr, int lower, int trans, int n, int k,
 template <typename T>
 int ssfr2k(ExecT<T>& ex, int transr, int lower, int trans, int n, int k,
            Scalar<T> alpha, const T* A, int lda, const T* B, int ldb,
-           Scalar<T> beta, T* C) {
+           Scalar<T> beta, T* C, int math) {
   Geometry g = geometry(n, transr, lower);
   ViewT<T> opA = trans ? ViewT<T>{const_cast<T*>(A), lda, 1}
                    : ViewT<T>{const_cast<T*>(A), 1, lda};
   ViewT<T> opB = trans ? ViewT<T>{const_cast<T*>(B), ldb, 1}
                    : ViewT<T>{const_cast<T*>(B), 1, ldb};
   if (alpha == 0.0f) k = 0;
-  ViewT<T> Ab[2] = {opA, sub(opA, g.n1, 0)};
-  ViewT<T> Bb[2] = {opB, sub(opB, g.n1, 0)};
-  ViewT<T> Cb[3] = {block_view(C, g.b11), block_view(C, g.b21),
-                block_view(C, g.b22)};
-  const int bi[3] = {0, 1, 1}, bj[3] = {0, 0, 1};
-  const int dm[3] = {g.n1, g.n2, g.n2}, dn[3] = {g.n1, g.n1, g.n2};
-  GemmProbT<T> p[3];
+  // The blocks of the reference's 2 SSYR2K + 2 SGEMM (src/curfp_ssfr2k.cpp:
+  // 193-229): T1 (lower), S, T2 (lower), each alpha (A_i B_j^T + B_i A_j^T).
+  ViewT<T> C11 = block_view(C, g.b11), C21 = block_view(C, g.b21),
+       C22 = block_view(C, g.b22);
+  SharedTaskT<T> t[3];
   int cnt = 0;
-  for (int b = 0; b < 3; ++b) {
-    if (dm[b] <= 0 || dn[b] <= 0) continue;
-    GemmProbT<T> q = gemm_prob(Ab[bi[b]], tr(Bb[bj[b]]), Cb[b], dm[b], dn[b], k,
-                           alpha, beta, 0);
-    q.A2 = Bb[bi[b]];
-    q.B2 = tr(Ab[bj[b]]);
-    q.k2 = k;
-    q.c_lower = (b != 1);
-    p[cnt++] = q;
-  }
-  return ex.gemm(p, cnt);
+  if (g.n1 > 0) t[cnt++] = SharedTaskT<T>{0, 0, g.n1, g.n1, C11, alpha, beta, 1};
+  if (g.n1 > 0 && g.n2 > 0)
+    t[cnt++] = SharedTaskT<T>{g.n1, 0, g.n2, g.n1, C21, alpha, beta, 0};
+  if (g.n2 > 0) t[cnt++] = SharedTaskT<T>{g.n1, g.n1, g.n2, g.n2, C22, alpha, beta, 1};
+  return ex.gemm_pair(opA, opB, n, k, t, cnt, math);
 }
 
 template <typename T>
@@ -293,22 +285,21 @@ int rfp_trtri(ExecT<T>& ex, int transr, int lower, int n, T* A, int math) {
 }
 
 template <typename T>
-int spftri(ExecT<T>& ex, int transr, int lower, int n, T* A) {
+int spftri(ExecT<T>& ex, int transr, int lower, int n, T* A, int math) {
   Geometry g = geometry(n, transr, lower);
   ViewT<T> V11 = block_view(A, g.b11), V21 = block_view(A, g.b21),
        V22 = block_view(A, g.b22);
   int rc;
-  if ((rc = rfp_trtri(ex, transr, lower, n, A, 0))) return rc;
+  if ((rc = rfp_trtri(ex, transr, lower, n, A, math))) return rc;
   // inv(A) = M^T M:  (11) = M11^T M11 + M21^T M21, (21) = M22^T M21,
   //                  (22) = M22^T M22
-  if ((rc = lauum_lower(ex, V11, g.n1))) return rc;
+  if ((rc = lauum_lower(ex, V11, g.n1, math))) return rc;
   if (g.n1 > 0 && g.n2 > 0) {
-    GemmProbT<T> p = gemm_prob(tr(V21), V21, V11, g.n1, g.n1, g.n2, 1.0f, 1.0f, 0);
-    p.c_lower = 1;
-    if ((rc = ex.gemm(&p, 1))) return rc;
-    if ((rc = trmm(ex, 1, 1, 1, V22, V21, g.n2, g.n1, 1.0f))) return rc;
+    SharedTaskT<T> t{0, 0, g.n1, g.n1, V11, 1.0f, 1.0f, 1};
+    if ((rc = ex.gemm_shared(tr(V21), g.n1, g.n2, &t, 1, math))) return rc;
+    if ((rc = trmm(ex, 1, 1, 1, V22, V21, g.n2, g.n1, 1.0f, math))) return rc;
   }
-  return lauum_lower(ex, V22, g.n2);
+  return lauum_lower(ex, V22, g.n2, math);
 }
 
 // ---------------------------------------------------------------------------
@@ -561,10 +552,10 @@ int rfp_symm_dbl(ExecT<T>& ex, int transr, int lower, int n, const T* G, ViewT<T
   template int ssfrk<T>(ExecT<T>&, int, int, int, int, int, Scalar<T>, const T*, int,         \
                         Scalar<T>, T*, int);                                                 \
   template int ssfr2k<T>(ExecT<T>&, int, int, int, int, int, Scalar<T>, const T*, int,        \
-                         const T*, int, Scalar<T>, T*);                                      \
+                         const T*, int, Scalar<T>, T*, int);                                 \
   template int spftrf<T>(ExecT<T>&, int, int, int, T*, int);                                  \
   template int spftrs<T>(ExecT<T>&, int, int, int, int, const T*, T*, int, int);              \
-  template int spftri<T>(ExecT<T>&, int, int, int, T*);                                       \
+  template int spftri<T>(ExecT<T>&, int, int, int, T*, int);                                  \
   template int rfp_trtri<T>(ExecT<T>&, int, int, int, T*, int);                               \
   template int rfp_trsm<T>(ExecT<T>&, int, int, int, const T*, int, ViewT<T>, int, Scalar<T>, \
                            int);                                                             \

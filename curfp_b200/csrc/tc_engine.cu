@@ -152,6 +152,7 @@ int tc_slab(curfpContext* ctx, const int* abort_flag, View A, int arows, View B,
   ProfScope ps(ctx->prof, ctx->stream, K_TC_GEMM, flops, 0);
   ktc::tc_gemm_kernel<<<grid, ktc::THREADS, ktc::SMEM_BYTES, ctx->stream>>>(mA, mB, b);
   ++ctx->launches;
+  ++ctx->wait_launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 

@@ -68,7 +68,9 @@ typedef enum {
 } curfpNormType_t;
 
 /* Opaque handle — reference include/curfp.h:58.  The context holds the
- * stream, the device, a device-side info word and a grow-only workspace. */
+ * stream, the device, a device-side info word, a kernel error word, the math
+ * mode of the drop-in routines and grow-only workspaces taken from a memory
+ * pool of the handle's own (the device's default pool is not touched). */
 typedef struct curfpContext *curfpHandle_t;
 
 /* Handle management — reference include/curfp.h:63-66
@@ -77,6 +79,37 @@ curfpStatus_t curfpCreate(curfpHandle_t *handle);
 curfpStatus_t curfpDestroy(curfpHandle_t handle);
 curfpStatus_t curfpSetStream(curfpHandle_t handle, cudaStream_t stream);
 curfpStatus_t curfpGetStream(curfpHandle_t handle, cudaStream_t *stream);
+
+/* Arithmetic of the contractions (SYRK / GEMM / TRSM and TRMM updates)
+ * inside the FP32 routines; set per handle with curfpSetMathMode, or per call
+ * through the *Ex entry points below.
+ *   CURFP_MATH_SPLIT_BF16 (the handle's default): contractions with
+ *     m, n, k >= 128 and m*n*k >= 6.7e7 run on the tcgen05 tensor cores; every
+ *     FP32 operand row is scaled by a power of two and split into three
+ *     integer BF16 digits, and the six digit products of weight >= 2^-16 are
+ *     accumulated exactly per 1024-deep chunk and summed in FP32.  Measured
+ *     against FP64 it is more accurate than FP32 FMA (about 2e-7 against
+ *     3e-6 relative on a rank-1024 update).  Diagonal blocks, triangular
+ *     leaves and smaller updates use FP32 FMA.
+ *   CURFP_MATH_FP32: every contraction in FP32 FMA on the SIMT cores (the
+ *     arithmetic of the reference's cuBLAS calls in their default math mode).
+ * The D-prefix routines always use FP64 FMA. */
+typedef enum {
+    CURFP_MATH_FP32       = 0,
+    CURFP_MATH_SPLIT_BF16 = 1
+} curfpMath_t;
+
+/* Math mode of curfpSsfrk, curfpSsfr2k, curfpSpftrf, curfpSpftrs and
+ * curfpSpftri on this handle (no counterpart in the reference, whose math
+ * is the one of its cuBLAS handle). */
+curfpStatus_t curfpSetMathMode(curfpHandle_t handle, curfpMath_t math);
+curfpStatus_t curfpGetMathMode(curfpHandle_t handle, curfpMath_t *math);
+
+/* Kernels that wait on other blocks (the wavefront solve, the tensor-core
+ * pipeline) give up after about 2 s and set the handle's kernel error word;
+ * a routine that launched such a kernel reads the word before it returns
+ * (one stream synchronisation) and reports CURFP_STATUS_EXECUTION_FAILED if
+ * it was set.  Routines that launched none return without synchronising. */
 
 /* C := alpha*op(A)*op(A)^T + beta*C, C n x n symmetric in RFP.
  * trans = N: A is n x k; trans = T: A is k x n (column-major, lda).
@@ -146,27 +179,14 @@ curfpStatus_t curfpDaddToDiagonal(curfpHandle_t handle,
                                   curfpFillMode_t uplo, int n, double value,
                                   double *arf);
 
-/* Arithmetic of the contractions inside ssfrk / spftrf (the precision form).
- *   CURFP_MATH_FP32:       SIMT FP32 FMA, the drop-in (same as curfpSsfrk /
- *                          curfpSpftrf).
- *   CURFP_MATH_SPLIT_BF16: large contractions (SYRK / GEMM updates) run on the
- *                          tcgen05 tensor cores with every FP32 operand split
- *                          into three BF16 terms (hi + mid + lo) and six BF16
- *                          products accumulated in FP32; diagonal blocks and
- *                          small updates stay FP32. */
-typedef enum {
-    CURFP_MATH_FP32       = 0,
-    CURFP_MATH_SPLIT_BF16 = 1
-} curfpMath_t;
-
-/* curfpSsfrk with a selectable contraction arithmetic. */
+/* curfpSsfrk with the contraction arithmetic given per call (curfpMath_t). */
 curfpStatus_t curfpSsfrkEx(curfpHandle_t handle, curfpOperation_t transr,
                            curfpFillMode_t uplo, curfpOperation_t trans,
                            int n, int k, const float *alpha, const float *A,
                            int lda, const float *beta, float *C,
                            curfpMath_t math);
 
-/* curfpSpftrf with a selectable contraction arithmetic. */
+/* curfpSpftrf with the contraction arithmetic given per call (curfpMath_t). */
 curfpStatus_t curfpSpftrfEx(curfpHandle_t handle, curfpOperation_t transr,
                             curfpFillMode_t uplo, int n, float *A, int *info,
                             curfpMath_t math);
