@@ -1,0 +1,176 @@
+"""The drop-in FP32 routines (ssfrk, ssfr2k, spftrf, spftrs, spftri) in both
+math modes of the handle, all 8 variants, at sizes whose contractions reach
+the tensor-core path (m, n, k >= 128 and m n k >= 6.7e7).
+
+* "bf16x3" (the default): large contractions run as exact split-BF16
+  tcgen05 products; the test checks that tc_gemm_kernel actually ran.
+* "fp32": every contraction in FP32 FMA on the SIMT cores; the test checks
+  that no tensor-core kernel ran.
+
+Accuracy against FP64 (torch float64 on the GPU, unpacked matrices), stated
+bounds: ssfrk / ssfr2k 2e-6 relative to max |C|; factor backward error
+||A - L L^T||_F / ||A||_F <= 2e-6; solve backward error
+max_j ||b_j - A x_j|| / (||A||_F ||x_j|| + ||b_j||) <= 2e-6; inverse residual
+||A Z - I||_F / sqrt(n) <= 1e-4 (cond ~ 45).  The default mode must be at
+least as accurate as the FP32 mode up to a factor 2 (checked on the factor)."""
+import pytest
+import torch
+
+from conftest import VARIANTS
+from helpers import TR, UL
+
+MODES = ["bf16x3", "fp32"]
+
+
+def dense_sym(curfp, C, tr, ul):
+    M = curfp.stfttr(C, transr=tr, uplo=ul).double()
+    return M + M.triu(1).T if ul == "U" else M + M.tril(-1).T
+
+
+def factor_L(curfp, F, tr, ul):
+    T = curfp.stfttr(F, transr=tr, uplo=ul).double()
+    return T.T if ul == "U" else T
+
+
+def stored_mask(n, ul):
+    m = torch.ones(n, n, device="cuda", dtype=torch.bool)
+    return m.triu() if ul == "U" else m.tril()
+
+
+class Mode:
+    """Runs a block with the current device handle in one math mode and
+    records which kernel classes ran inside it."""
+
+    def __init__(self, curfp, mode):
+        self.curfp, self.mode = curfp, mode
+
+    def __enter__(self):
+        from curfp_b200 import precision as P
+        self.prev = self.curfp.get_math_mode()
+        self.curfp.set_math_mode(self.mode)
+        P.profile_enable(True)
+        return self
+
+    def __exit__(self, *exc):
+        from curfp_b200 import precision as P
+        self.classes = P.profile_read()
+        P.profile_enable(False)
+        self.curfp.set_math_mode(self.prev)
+        return False
+
+    def check_engine(self):
+        tc = self.classes.get("tc_gemm", {}).get("launches", 0)
+        if self.mode == "bf16x3":
+            assert tc > 0, self.classes
+        else:
+            assert tc == 0, self.classes
+
+
+@pytest.mark.gpu
+def test_math_mode_api(curfp):
+    assert curfp.get_math_mode() == "bf16x3"  # the handle's default
+    curfp.set_math_mode("fp32")
+    assert curfp.get_math_mode() == "fp32"
+    curfp.set_math_mode("bf16x3")
+    with pytest.raises(ValueError):
+        curfp.set_math_mode("tf32")
+    with curfp.Handle() as h:
+        assert h._lib.curfpSetMathMode(h.ptr, 7) == 3
+        assert h._lib.curfpSetMathMode(None, 0) == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("n", [1537, 2048])
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+def test_pipeline_math_mode(curfp, mode, n, tr, ul):
+    T, U = TR[tr], UL[ul]
+    k = n // 2
+    g = torch.Generator(device="cuda").manual_seed(11 * n + 2 * tr + ul)
+    A = torch.randn(n, k, device="cuda", generator=g) / k ** 0.5
+    B = torch.randn(n, 64, device="cuda", generator=g)
+    C = torch.empty(n * (n + 1) // 2, device="cuda")
+    with Mode(curfp, mode) as m:
+        curfp.ssfrk(A, C, transr=T, uplo=U)
+        curfp.add_to_diagonal(C, 1.0, transr=T, uplo=U)
+        C0 = C.clone()
+        assert curfp.spftrf(C, transr=T, uplo=U) == 0
+        X = B.clone()
+        curfp.spftrs(C, X, transr=T, uplo=U)
+        Z = C.clone()
+        curfp.spftri(Z, transr=T, uplo=U)
+        torch.cuda.synchronize()
+    m.check_engine()
+    Ad = A.double()
+    S = dense_sym(curfp, C0, T, U)
+    full = Ad @ Ad.T + torch.eye(n, device="cuda", dtype=torch.float64)
+    mask = stored_mask(n, U)
+    e_frk = ((S - full)[mask].abs().max() / full[mask].abs().max()).item()
+    assert e_frk <= 2e-6, e_frk
+    L = factor_L(curfp, C, T, U)
+    e_fac = (torch.linalg.norm(S - L @ L.T) / torch.linalg.norm(S)).item()
+    assert e_fac <= 2e-6, e_fac
+    R = B.double() - S @ X.double()
+    nS = torch.linalg.norm(S)
+    e_sol = (R.norm(dim=0) / (nS * X.double().norm(dim=0) + B.double().norm(dim=0))).max().item()
+    assert e_sol <= 2e-6, e_sol
+    Zs = dense_sym(curfp, Z, T, U)
+    P = S @ Zs
+    P.diagonal().sub_(1.0)
+    e_inv = (torch.linalg.norm(P) / n ** 0.5).item()
+    assert e_inv <= 1e-4, e_inv
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [2048, 3001])
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+def test_spftrf_default_mode_not_worse_than_fp32(curfp, n, tr, ul):
+    T, U = TR[tr], UL[ul]
+    k = n // 4
+    g = torch.Generator(device="cuda").manual_seed(5 * n + tr + 7 * ul)
+    A = torch.randn(n, k, device="cuda", generator=g) / k ** 0.5
+    C = torch.empty(n * (n + 1) // 2, device="cuda")
+    curfp.ssfrk(A, C, transr=T, uplo=U)
+    curfp.add_to_diagonal(C, 0.1, transr=T, uplo=U)
+    S = dense_sym(curfp, C, T, U)
+    errs = {}
+    for mode in MODES:
+        F = C.clone()
+        with Mode(curfp, mode) as m:
+            assert curfp.spftrf(F, transr=T, uplo=U) == 0
+        m.check_engine()
+        L = factor_L(curfp, F, T, U)
+        errs[mode] = (torch.linalg.norm(S - L @ L.T) / torch.linalg.norm(S)).item()
+    assert errs["bf16x3"] <= 2.0 * errs["fp32"] + 1e-8, errs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("trans", ["N", "T"])
+@pytest.mark.parametrize("tr,ul", VARIANTS)
+def test_ssfr2k_math_mode(curfp, mode, trans, tr, ul):
+    """C := alpha (op(A) op(B)^T + op(B) op(A)^T) + beta C at n = 1500,
+    k = 700 (the tensor-core path runs the rank-2k blocks as two split-BF16
+    contractions, beta applied once)."""
+    T, U = TR[tr], UL[ul]
+    n, k = 1500, 700
+    g = torch.Generator(device="cuda").manual_seed(n + 3 * tr + ul + (trans == "T"))
+    Aop = torch.randn(n, k, device="cuda", generator=g) / k ** 0.5
+    Bop = torch.randn(n, k, device="cuda", generator=g) / k ** 0.5
+    C0 = torch.randn(n * (n + 1) // 2, device="cuda", generator=g)
+    C = C0.clone()
+    # trans = T: A (n, k) row-major; trans = N: A column-major n x k = (k, n) row-major
+    Ain = Aop.contiguous() if trans == "T" else Aop.t().contiguous()
+    Bin = Bop.contiguous() if trans == "T" else Bop.t().contiguous()
+    with Mode(curfp, mode) as m:
+        curfp.ssfr2k(Ain, Bin, C, alpha=0.5, beta=-1.5, transr=T, uplo=U, trans=trans)
+        torch.cuda.synchronize()
+    m.check_engine()
+    Ad, Bd = Aop.double(), Bop.double()
+    want = 0.5 * (Ad @ Bd.T + Bd @ Ad.T)
+    D = curfp.stfttr(C, transr=T, uplo=U).double()
+    D0 = curfp.stfttr(C0, transr=T, uplo=U).double()
+    mask = stored_mask(n, U)
+    err = (D - (want - 1.5 * D0))[mask].abs().max().item()
+    scale = (want.abs() + 1.5 * D0.abs())[mask].max().item()
+    assert err / scale <= 2e-6, err / scale
