@@ -1,31 +1,25 @@
 #!/usr/bin/env python
-"""Scale workloads of the RFP path on one GPU, one JSON line per result.
+"""Scale workloads of the RFP path on one GPU (helpers of tests/test_scale_gpu.py).
 
-Run as a script (pytest does not collect it):
+C2   plain FP32 drop-in at n in {32767, 32768}, k = 1024, all 8 variants:
+     ssfrk, spftrf, spftrs (64 RHS) and spftri through the C ABI, beside the
+     reference's own GPU build (oracle/_ref/libcurfp_ref.so, cuBLAS/cuSOLVER)
+     on the same input, with FP64 checks of both: ||C - L L^T||_F / ||C||_F,
+     solve backward error, inverse residual, ours-vs-reference differences.
+C3   precision form at n = 65536, k = 2048, 256 RHS, per shift lambda:
+     split-BF16 ssfrk + spftrf + FP64-residual refined spftrs against the
+     FP32 (SIMT) form and the drop-in, errors against the exact FP64 solution.
+C5   n = 131072, k = 4096, lambda = 1e-2: split-BF16 ssfrk + spftrf + refined
+     spftrs (64 RHS), then the fused GP NLL forward + backward (X = A, s = 1,
+     sigma2 = lambda), with the loss and gradient against exact FP64 values.
+next the routines beyond the Cholesky path at n = 32768 (slansf, spfcon,
+     ssfmv, ssfmm with 64 RHS, ssfr, ssfr2) and the FP64 twins at n = 16384
+     (dsfrk k = 512, dpftrf, dpftrs with 64 RHS, dpftri), beside the
+     reference build.
 
-  python tests/scale_configs.py c2 [--n 32768 32767] [--variants all|TU]
-      Plain FP32 drop-in at n in {32767, 32768}, k = 1024, all 8 variants:
-      ssfrk, spftrf, spftrs (64 RHS) and spftri through the C ABI, per-op
-      ms / TFLOP/s / algorithmic GB/s, beside the reference's own GPU build
-      (oracle/_ref/libcurfp_ref.so, cuBLAS/cuSOLVER) on the same input, with
-      FP64 checks of both: ||C - L L^T||_F / ||C||_F, solve backward error,
-      inverse residual, and ours-vs-reference differences.
-  python tests/scale_configs.py lapack [--n 32768 32767]
-      Host LAPACK (scipy/OpenBLAS, all threads) ssfrk / spftrf / spftrs /
-      spftri at the same sizes, transr=T uplo=U, one run each.
-  python tests/scale_configs.py c3 [--lam 0.1 0.001]
-      Precision form at n = 65536, k = 2048, 256 RHS, per shift lambda:
-      split-BF16 ssfrk + spftrf + FP64-residual refined spftrs against the
-      plain FP32 form, errors against the exact FP64 solution.
-  python tests/scale_configs.py next [--next-n 32768] [--next-nd 16384]
-      The routines beyond the Cholesky path at n = 32768 (slansf, spfcon,
-      ssfmv, ssfmm with 64 RHS, ssfr, ssfr2) and the FP64 twins at n = 16384
-      (dsfrk k = 512, dpftrf, dpftrs with 64 RHS, dpftri), each beside the
-      reference build.
-  python tests/scale_configs.py c5
-      n = 131072, k = 4096, lambda = 1e-2: split-BF16 ssfrk + spftrf + refined
-      spftrs (64 RHS), then the fused GP NLL forward + backward (X = A, s = 1,
-      sigma2 = lambda), with the loss and gradient against exact FP64 values.
+Each run_* function returns one result dict per case (timings, errors); the
+tests assert the stated bounds on it and, when CURFP_SCALE_LOG names a file,
+append it there as a JSON line (the numbers summarised under profiles/).
 
 The FP64 oracle of C3 / C5 is exact and needs no n x n factorization: for
 C = A A^T + lam I with A (n x k, its FP32 values, n > k) the Woodbury
@@ -36,13 +30,13 @@ cond_2(C) = ||C||_2 / lam, log det C = (n-k) log lam + sum log(s_i + lam),
 tr C^-1 = (n-k)/lam + sum 1/(s_i + lam).  Inputs are seeded numpy
 default_rng draws: A ~ N(0,1)/sqrt(k) (n x k float32), B ~ N(0,1).
 Timing: CUDA events on the default stream (the library handle's stream),
-`--warmup` untimed runs then the median of `--reps`; the input of each
-in-place routine is restored (untimed) before every run.
+`warmup` untimed runs then the median of `reps`; the input of each in-place
+routine is restored (untimed) before every run.
 """
 from __future__ import annotations
 
-import argparse
 import ctypes
+import os
 import json
 import math
 import statistics
@@ -73,33 +67,42 @@ def chol_flops(n: int) -> float:
     return n ** 3 / 3.0 + n ** 2 / 2.0 + n / 6.0
 
 
-def emit(d: dict, out) -> None:
-    line = json.dumps(d)
-    print(line, flush=True)
+def emit(d: dict) -> None:
+    """Append a result to the file named by CURFP_SCALE_LOG (if set)."""
+    out = os.environ.get("CURFP_SCALE_LOG")
     if out:
         with open(out, "a") as f:
-            f.write(line + "\n")
+            f.write(json.dumps(d) + "\n")
 
 
 class Ours:
-    """This library through its C ABI (the drop-in boundary)."""
+    """This library through its C ABI (the drop-in boundary).  math=None runs
+    the drop-in entry points in the handle's math mode; 0 / 1 select the
+    arithmetic per call through the *Ex entry points."""
 
     def __init__(self):
         self.h = curfp._get_handle()
         self.lib = self.h._lib
 
-    def ssfrk(self, tr, ul, n, k, A, C, math=0):
+    def ssfrk(self, tr, ul, n, k, A, C, math=None):
         a, b = ctypes.c_float(1.0), ctypes.c_float(0.0)
-        st = self.lib.curfpSsfrkEx(self.h.ptr, tr, ul, 1, n, k, ctypes.byref(a), vp(A), k,
-                                   ctypes.byref(b), vp(C), math)
+        if math is None:
+            st = self.lib.curfpSsfrk(self.h.ptr, tr, ul, 1, n, k, ctypes.byref(a), vp(A), k,
+                                     ctypes.byref(b), vp(C))
+        else:
+            st = self.lib.curfpSsfrkEx(self.h.ptr, tr, ul, 1, n, k, ctypes.byref(a), vp(A), k,
+                                       ctypes.byref(b), vp(C), math)
         assert st == 0, st
 
     def add_diag(self, tr, ul, n, v, C):
         assert self.lib.curfpSaddToDiagonal(self.h.ptr, tr, ul, n, ctypes.c_float(v), vp(C)) == 0
 
-    def spftrf(self, tr, ul, n, C, math=0):
+    def spftrf(self, tr, ul, n, C, math=None):
         info = ctypes.c_int(0)
-        st = self.lib.curfpSpftrfEx(self.h.ptr, tr, ul, n, vp(C), ctypes.byref(info), math)
+        if math is None:
+            st = self.lib.curfpSpftrf(self.h.ptr, tr, ul, n, vp(C), ctypes.byref(info))
+        else:
+            st = self.lib.curfpSpftrfEx(self.h.ptr, tr, ul, n, vp(C), ctypes.byref(info), math)
         assert st == 0 and info.value == 0, (st, info.value)
 
     def spftrs(self, tr, ul, n, nrhs, F, X):
@@ -131,6 +134,21 @@ class Ours:
 
     def release(self):
         assert self.lib.curfpReleaseWorkspace(self.h.ptr) == 0
+
+    def mode(self, m: str):
+        """Context manager: the handle's math mode set to m ("bf16x3" /
+        "fp32") inside the block."""
+        ours = self
+
+        class _M:
+            def __enter__(self_):
+                self_.prev = ours.h.get_math_mode()
+                ours.h.set_math_mode(m)
+
+            def __exit__(self_, *exc):
+                ours.h.set_math_mode(self_.prev)
+                return False
+        return _M()
 
 
 def cuda_ms(fn, prep=None, warmup=2, reps=5):
@@ -278,139 +296,93 @@ def rel_diff(a, b) -> float:
 # C2: plain FP32 at scale, all variants, beside the reference build
 # ---------------------------------------------------------------------------
 
-def run_c2(args):
+def run_c2(n, tr, ul, mode="bf16x3", warmup=2, reps=5, with_ref=True) -> dict:
+    """One C2 case: the drop-in routines in the handle math `mode` beside the
+    reference build (when present) on the same input; timings are medians of
+    `reps` runs after `warmup` (reps = 1, warmup = 0: one run each)."""
     from helpers import REF_LIB, RefLib
     ours = Ours()
-    ref = RefLib() if REF_LIB.exists() else None
+    ref = RefLib() if (with_ref and REF_LIB.exists()) else None
     k, nrhs, shift = 1024, 64, 1.0
-    variants = VARIANTS if args.variants == "all" else [
-        (int(args.variants[0] == "T"), int(args.variants[1] == "U"))]
-    for n in args.n:
-        A = gen_A(n, k, seed=n)
-        B0 = gen_B(n, nrhs, seed=n + 1)
-        orc = GramOracle(A, shift)  # only for ||C||_2 of the exact matrix
-        nt = n * (n + 1) // 2
-        f = {"ssfrk": n * (n + 1) * float(k), "spftrf": chol_flops(n),
-             "spftrs": 2.0 * n * n * nrhs, "spftri": 2.0 * n ** 3 / 3.0}
-        by = {"ssfrk": 4.0 * n * k + 4.0 * nt, "spftrf": 8.0 * nt,
-              "spftrs": 8.0 * nt + 16.0 * n * nrhs, "spftri": 8.0 * nt}
-        for tr, ul in variants:
-            res = {"config": "C2", "n": n, "k": k, "nrhs": nrhs, "shift": shift,
-                   "variant": NAME(tr, ul), "transr": "NT"[tr], "uplo": "LU"[ul],
-                   "timing": f"warmup {args.warmup}, median of {args.reps}",
-                   "ours": {}, "reference": {}, "errors": {}}
-            C0 = torch.empty(nt, device="cuda")
-            ms = cuda_ms(lambda: ours.ssfrk(tr, ul, n, k, A, C0), None, args.warmup, args.reps)
-            res["ours"]["ssfrk"] = rate(ms, f["ssfrk"], by["ssfrk"])
-            ours.add_diag(tr, ul, n, shift, C0)
-            F = torch.empty_like(C0)
-            X = torch.empty_like(B0)
-            Z = torch.empty_like(C0)
-            ms = cuda_ms(lambda: ours.spftrf(tr, ul, n, F), lambda: F.copy_(C0),
-                         args.warmup, args.reps)
-            res["ours"]["spftrf"] = rate(ms, f["spftrf"], by["spftrf"])
-            ms = cuda_ms(lambda: ours.spftrs(tr, ul, n, nrhs, F, X), lambda: X.copy_(B0),
-                         args.warmup, args.reps)
-            res["ours"]["spftrs"] = rate(ms, f["spftrs"], by["spftrs"])
-            ms = cuda_ms(lambda: ours.spftri(tr, ul, n, Z), lambda: Z.copy_(F),
-                         args.warmup, args.reps)
-            res["ours"]["spftri"] = rate(ms, f["spftri"], by["spftri"])
-            t = res["ours"]
-            t["chol_solve_tflops"] = round((f["spftrf"] + f["spftrs"]) /
-                                           ((t["spftrf"]["ms"] + t["spftrs"]["ms"]) * 1e-3) / 1e12, 3)
-            if ref is not None:
-                Cr = torch.empty(nt, device="cuda")
-                ms = cuda_ms(lambda: ref.ssfrk(tr, ul, 1, n, k, 1.0, A, k, 0.0, Cr), None,
-                             args.warmup, args.reps)
-                res["reference"]["ssfrk"] = rate(ms, f["ssfrk"], by["ssfrk"])
-                ours.add_diag(tr, ul, n, shift, Cr)
-                res["errors"]["ssfrk_maxabs_ours_vs_ref"] = float((Cr - C0).abs().max())
-                del Cr
-                Fr = torch.empty_like(C0)
-                Xr = torch.empty_like(B0)
-                Zr = torch.empty_like(C0)
+    A = gen_A(n, k, seed=n)
+    B0 = gen_B(n, nrhs, seed=n + 1)
+    orc = GramOracle(A, shift)  # only for ||C||_2 of the exact matrix
+    nt = n * (n + 1) // 2
+    f = {"ssfrk": n * (n + 1) * float(k), "spftrf": chol_flops(n),
+         "spftrs": 2.0 * n * n * nrhs, "spftri": 2.0 * n ** 3 / 3.0}
+    by = {"ssfrk": 4.0 * n * k + 4.0 * nt, "spftrf": 8.0 * nt,
+          "spftrs": 8.0 * nt + 16.0 * n * nrhs, "spftri": 8.0 * nt}
+    res = {"config": "C2", "n": n, "k": k, "nrhs": nrhs, "shift": shift,
+           "variant": NAME(tr, ul), "transr": "NT"[tr], "uplo": "LU"[ul], "math": mode,
+           "timing": f"warmup {warmup}, median of {reps}",
+           "ours": {}, "reference": {}, "errors": {}}
+    C0 = torch.empty(nt, device="cuda")
+    F = torch.empty_like(C0)
+    X = torch.empty_like(B0)
+    Z = torch.empty_like(C0)
+    with ours.mode(mode):
+        ms = cuda_ms(lambda: ours.ssfrk(tr, ul, n, k, A, C0), None, warmup, reps)
+        res["ours"]["ssfrk"] = rate(ms, f["ssfrk"], by["ssfrk"])
+        ours.add_diag(tr, ul, n, shift, C0)
+        ms = cuda_ms(lambda: ours.spftrf(tr, ul, n, F), lambda: F.copy_(C0), warmup, reps)
+        res["ours"]["spftrf"] = rate(ms, f["spftrf"], by["spftrf"])
+        ms = cuda_ms(lambda: ours.spftrs(tr, ul, n, nrhs, F, X), lambda: X.copy_(B0),
+                     warmup, reps)
+        res["ours"]["spftrs"] = rate(ms, f["spftrs"], by["spftrs"])
+        ms = cuda_ms(lambda: ours.spftri(tr, ul, n, Z), lambda: Z.copy_(F), warmup, reps)
+        res["ours"]["spftri"] = rate(ms, f["spftri"], by["spftri"])
+    t = res["ours"]
+    t["chol_solve_tflops"] = round((f["spftrf"] + f["spftrs"]) /
+                                   ((t["spftrf"]["ms"] + t["spftrs"]["ms"]) * 1e-3) / 1e12, 3)
+    if ref is not None:
+        Cr = torch.empty(nt, device="cuda")
+        ms = cuda_ms(lambda: ref.ssfrk(tr, ul, 1, n, k, 1.0, A, k, 0.0, Cr), None, warmup, reps)
+        res["reference"]["ssfrk"] = rate(ms, f["ssfrk"], by["ssfrk"])
+        ours.add_diag(tr, ul, n, shift, Cr)
+        res["errors"]["ssfrk_maxabs_ours_vs_ref"] = float((Cr - C0).abs().max())
+        del Cr
+        Fr = torch.empty_like(C0)
+        Xr = torch.empty_like(B0)
+        Zr = torch.empty_like(C0)
+        infos = []
 
-                def rf():
-                    st, info = ref.spftrf(tr, ul, n, Fr)
-                    assert st == 0 and info == 0, (st, info)
-                ms = cuda_ms(rf, lambda: Fr.copy_(C0), args.warmup, args.reps)
-                res["reference"]["spftrf"] = rate(ms, f["spftrf"], by["spftrf"])
-                ms = cuda_ms(lambda: ref.spftrs(tr, ul, n, nrhs, Fr, Xr, n), lambda: Xr.copy_(B0),
-                             args.warmup, args.reps)
-                res["reference"]["spftrs"] = rate(ms, f["spftrs"], by["spftrs"])
-                ms = cuda_ms(lambda: ref.spftri(tr, ul, n, Zr), lambda: Zr.copy_(Fr),
-                             args.warmup, args.reps)
-                res["reference"]["spftri"] = rate(ms, f["spftri"], by["spftri"])
-                t = res["reference"]
-                t["chol_solve_tflops"] = round(
-                    (f["spftrf"] + f["spftrs"]) /
-                    ((t["spftrf"]["ms"] + t["spftrs"]["ms"]) * 1e-3) / 1e12, 3)
-                e = res["errors"]
-                e["factor_rel_diff_ours_vs_ref"] = rel_diff(F, Fr)
-                e["solve_rel_diff_ours_vs_ref"] = rel_diff(X, Xr)
-                e["inverse_rel_diff_ours_vs_ref"] = rel_diff(Z, Zr)
-            # FP64 checks on the stored FP32 matrix C0 (the input of both arms)
-            S = dense_sym(ours, tr, ul, n, C0)
-            e = res["errors"]
-            arms = [("ours", F, X, Z)] + ([("reference", Fr, Xr, Zr)] if ref is not None else [])
-            for name, Fa, Xa, Za in arms:
-                T = dense_tri(ours, tr, ul, n, Fa)
-                e[f"{name}_factor_backward"] = factor_berr(S, T, ul)
-                del T
-                e[f"{name}_solve_backward"] = solve_berr_dense(S, orc.norm2, B0, Xa)
-                Zs = dense_sym(ours, tr, ul, n, Za)
-                e[f"{name}_inverse_residual"] = inverse_res(S, Zs)
-                del Zs
-            del S, F, X, Z, C0
-            if ref is not None:
-                del Fr, Xr, Zr
-            torch.cuda.empty_cache()
-            emit(res, args.out)
-        del A, B0, orc
-        torch.cuda.empty_cache()
-
-
-# ---------------------------------------------------------------------------
-# Host LAPACK at the C2 sizes
-# ---------------------------------------------------------------------------
-
-def run_lapack(args):
-    from scipy.linalg import lapack as la
-
-    from oracle import port
-    k, nrhs, shift = 1024, 64, 1.0
-    for n in args.n:
-        rng = np.random.default_rng(n)
-        A = np.asfortranarray(rng.standard_normal((n, k), dtype=np.float32) /
-                              np.float32(math.sqrt(k)))
-        B = np.asfortranarray(np.random.default_rng(n + 1).standard_normal(
-            (n, nrhs), dtype=np.float32))
-        out = {"config": "C2-host-LAPACK", "n": n, "k": k, "nrhs": nrhs, "variant": "TU",
-               "cores": port.threads(),
-               "library": f"scipy {__import__('scipy').__version__} LAPACK (OpenBLAS)",
-               "timing": "one run each", "ops": {}}
-        t0 = time.perf_counter()
-        C = la.ssfrk(n, k, 1.0, A, 0.0, np.zeros(n * (n + 1) // 2, np.float32),
-                     transr="T", uplo="U", trans="N")
-        t1 = time.perf_counter()
-        C[port.diag_indices(n, "T", "U")] += np.float32(shift)
-        t2 = time.perf_counter()
-        F, info = la.spftrf(n, C, transr="T", uplo="U")
-        t3 = time.perf_counter()
-        assert info == 0, info
-        X, info = la.spftrs(n, F, B, transr="T", uplo="U")
-        t4 = time.perf_counter()
-        Z, info = la.spftri(n, F, transr="T", uplo="U")
-        t5 = time.perf_counter()
-        o = out["ops"]
-        o["ssfrk"] = rate((t1 - t0) * 1e3, n * (n + 1) * float(k))
-        o["spftrf"] = rate((t3 - t2) * 1e3, chol_flops(n))
-        o["spftrs"] = rate((t4 - t3) * 1e3, 2.0 * n * n * nrhs)
-        o["spftri"] = rate((t5 - t4) * 1e3, 2.0 * n ** 3 / 3.0)
-        out["chol_solve_tflops"] = round((chol_flops(n) + 2.0 * n * n * nrhs) /
-                                         (t4 - t2) / 1e12, 4)
-        emit(out, args.out)
-        del A, B, C, F, X, Z
+        def rf():
+            st, info = ref.spftrf(tr, ul, n, Fr)
+            assert st == 0, st
+            infos.append(info)
+        ms = cuda_ms(rf, lambda: Fr.copy_(C0), warmup, reps)
+        res["reference"]["spftrf"] = rate(ms, f["spftrf"], by["spftrf"])
+        res["reference_info"] = infos[-1]
+        ms = cuda_ms(lambda: ref.spftrs(tr, ul, n, nrhs, Fr, Xr, n), lambda: Xr.copy_(B0),
+                     warmup, reps)
+        res["reference"]["spftrs"] = rate(ms, f["spftrs"], by["spftrs"])
+        ms = cuda_ms(lambda: ref.spftri(tr, ul, n, Zr), lambda: Zr.copy_(Fr), warmup, reps)
+        res["reference"]["spftri"] = rate(ms, f["spftri"], by["spftri"])
+        t = res["reference"]
+        t["chol_solve_tflops"] = round(
+            (f["spftrf"] + f["spftrs"]) /
+            ((t["spftrf"]["ms"] + t["spftrs"]["ms"]) * 1e-3) / 1e12, 3)
+        e = res["errors"]
+        e["factor_rel_diff_ours_vs_ref"] = rel_diff(F, Fr)
+        e["solve_rel_diff_ours_vs_ref"] = rel_diff(X, Xr)
+        e["inverse_rel_diff_ours_vs_ref"] = rel_diff(Z, Zr)
+    # FP64 checks on the stored FP32 matrix C0 (the input of both arms)
+    S = dense_sym(ours, tr, ul, n, C0)
+    e = res["errors"]
+    arms = [("ours", F, X, Z)] + ([("reference", Fr, Xr, Zr)] if ref is not None else [])
+    for name, Fa, Xa, Za in arms:
+        T = dense_tri(ours, tr, ul, n, Fa)
+        e[f"{name}_factor_backward"] = factor_berr(S, T, ul)
+        del T
+        e[f"{name}_solve_backward"] = solve_berr_dense(S, orc.norm2, B0, Xa)
+        Zs = dense_sym(ours, tr, ul, n, Za)
+        e[f"{name}_inverse_residual"] = inverse_res(S, Zs)
+        del Zs
+    del S, F, X, Z, C0, A, B0, orc
+    if ref is not None:
+        del Fr, Xr, Zr
+    torch.cuda.empty_cache()
+    return res
 
 
 # ---------------------------------------------------------------------------
@@ -426,7 +398,13 @@ def breakdown(fn) -> dict:
     return {k: round(v["ms"], 2) for k, v in r.items()}
 
 
-def run_c3(args):
+def run_c3(lam, n=65536, k=2048, warmup=2, reps=5, max_iter=3) -> dict:
+    """One C3 case (shift lam): the FP32 (SIMT) form, the drop-in in its
+    default math mode, and the precision form (split-BF16 factor + FP64
+    refined solve), each against the exact FP64 solution."""
+    from types import SimpleNamespace
+    args = SimpleNamespace(c3_n=n, c3_k=k, lam=[lam], warmup=warmup, reps=reps,
+                           max_iter=max_iter)
     ours = Ours()
     n, k, nrhs = args.c3_n, args.c3_k, 256
     tr, ul = 1, 1
@@ -440,7 +418,7 @@ def run_c3(args):
                "cond2_exact": orc.cond2, "norm2_exact": orc.norm2,
                "timing": f"warmup {args.warmup}, median of {args.reps}",
                "metric": "Cholesky+solve TFLOP/s = (n^3/3 + n^2/2 + n/6 + 2 n^2 nrhs) / t"}
-        for form, math_ in (("plain_fp32", 0), ("split_bf16", 1)):
+        for form, math_ in (("plain_fp32", 0), ("drop_in_default", None), ("split_bf16", 1)):
             C = torch.empty(nt, device="cuda")
             ms_s = cuda_ms(lambda: ours.ssfrk(tr, ul, n, k, A, C, math_), None,
                            args.warmup, args.reps)
@@ -450,16 +428,17 @@ def run_c3(args):
             ms_f = cuda_ms(lambda: ours.spftrf(tr, ul, n, F, math_), lambda: F.copy_(C),
                            args.warmup, args.reps)
             iters = []
-            if math_ == 0:
-                ms_x = cuda_ms(lambda: ours.spftrs(tr, ul, n, nrhs, F, X), lambda: X.copy_(B0),
-                               args.warmup, args.reps)
+            if math_ != 1:
+                with ours.mode("fp32" if math_ == 0 else "bf16x3"):
+                    ms_x = cuda_ms(lambda: ours.spftrs(tr, ul, n, nrhs, F, X),
+                                   lambda: X.copy_(B0), args.warmup, args.reps)
             else:
                 ms_x = cuda_ms(lambda: iters.append(
                     ours.refine(tr, ul, n, nrhs, C, F, X, args.max_iter)),
                     lambda: X.copy_(B0), args.warmup, args.reps)
             d = {"ssfrk": rate(ms_s, n * (n + 1) * float(k)),
                  "spftrf": rate(ms_f, chol_flops(n)),
-                 "spftrs" if math_ == 0 else "spftrs_refined": rate(ms_x, 2.0 * n * n * nrhs),
+                 "spftrs" if math_ != 1 else "spftrs_refined": rate(ms_x, 2.0 * n * n * nrhs),
                  "chol_solve": rate(ms_f + ms_x, fl)}
             if iters:
                 d["refine_corrections"] = iters[-1]
@@ -474,9 +453,9 @@ def run_c3(args):
             ours.release()
         res["precision_over_plain"] = round(res["split_bf16"]["chol_solve"]["tflops"] /
                                             res["plain_fp32"]["chol_solve"]["tflops"], 3)
-        emit(res, args.out)
         del orc
         torch.cuda.empty_cache()
+    return res
 
 
 def conditioning(ours: Ours, tr, ul, n, C, F) -> dict:
@@ -545,7 +524,13 @@ def rfp_offsets(tr, ul, n, rows):
 # C5: n = 131072 precision pipeline + fused NLL fwd/bwd
 # ---------------------------------------------------------------------------
 
-def run_c5(args):
+def run_c5(n=131072, k=4096, warmup=1, reps=3, max_iter=3, nll=True, nll_warmup=1,
+           nll_reps=3) -> dict:
+    """The C5 pipeline (split-BF16 ssfrk + spftrf + refined spftrs) and,
+    with nll, the fused GP NLL forward + backward, against exact FP64."""
+    from types import SimpleNamespace
+    args = SimpleNamespace(c5_n=n, c5_k=k, warmup=warmup, reps=reps, max_iter=max_iter,
+                           nll_warmup=nll_warmup, nll_reps=nll_reps)
     ours = Ours()
     n, k, nrhs, lam = args.c5_n, args.c5_k, 64, 1e-2
     tr, ul = 1, 1
@@ -582,9 +567,12 @@ def run_c5(args):
     del C, F, X
     torch.cuda.empty_cache()
     ours.release()
-    if not args.no_nll:
+    if nll:
         res["nll"] = nll_c5(orc, A, lam, args)
-    emit(res, args.out)
+    del A, B0, orc
+    torch.cuda.empty_cache()
+    ours.release()
+    return res
 
 
 def nll_c5(orc: GramOracle, A, lam, args) -> dict:
@@ -622,8 +610,12 @@ def nll_c5(orc: GramOracle, A, lam, args) -> dict:
 # symmetric multiplies, rank updates, and the FP64 twins
 # ---------------------------------------------------------------------------
 
-def run_next(args):
+def run_next(n=32768, nd=16384, warmup=2, reps=5) -> dict:
+    """The routines beyond the Cholesky path beside the reference build."""
+    from types import SimpleNamespace
+
     from helpers import REF_LIB, RefLib
+    args = SimpleNamespace(next_n=n, next_nd=nd, warmup=warmup, reps=reps)
     ours = Ours()
     ref = RefLib() if REF_LIB.exists() else None
     lib, h = ours.lib, ours.h.ptr
@@ -709,7 +701,9 @@ def run_next(args):
          (lambda: ref.dpftri(tr, ul, nd, Zd)) if ref else None, flops=2.0 * nd ** 3 / 3.0,
          prep=lambda: Zd.copy_(Fd))
     res["fp64_n"] = nd
-    emit(res, args.out)
+    del Ad, Cd, Fd, Bd, Xd, Zd, x, y, Bm, Ym
+    torch.cuda.empty_cache()
+    return res
 
 
 def nll_exact(orc: GramOracle, y):
@@ -725,33 +719,3 @@ def nll_exact(orc: GramOracle, y):
     gs64 = 0.5 * (orc.trace_ata_cinv() - float(ata @ ata))
     gv64 = 0.5 * (orc.trace_inv() - float(alpha @ alpha))
     return loss64, gx64, gs64, gv64
-
-
-def main():
-    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("what", choices=["c2", "lapack", "c3", "c5", "next"])
-    ap.add_argument("--next-n", type=int, default=32768)
-    ap.add_argument("--next-nd", type=int, default=16384)
-    ap.add_argument("--n", type=int, nargs="+", default=[32768, 32767])
-    ap.add_argument("--variants", default="all")
-    ap.add_argument("--lam", type=float, nargs="+", default=[0.1, 0.001])
-    ap.add_argument("--c3-n", type=int, default=65536)
-    ap.add_argument("--c3-k", type=int, default=2048)
-    ap.add_argument("--c5-n", type=int, default=131072)
-    ap.add_argument("--c5-k", type=int, default=4096)
-    ap.add_argument("--warmup", type=int, default=2)
-    ap.add_argument("--reps", type=int, default=5)
-    ap.add_argument("--nll-warmup", type=int, default=1)
-    ap.add_argument("--nll-reps", type=int, default=3)
-    ap.add_argument("--max-iter", type=int, default=3)
-    ap.add_argument("--no-nll", action="store_true")
-    ap.add_argument("--out", default=None, help="also append the JSON lines to this file")
-    args = ap.parse_args()
-    if args.what != "lapack":
-        torch.cuda.init()
-    {"c2": run_c2, "lapack": run_lapack, "c3": run_c3, "c5": run_c5,
-     "next": run_next}[args.what](args)
-
-
-if __name__ == "__main__":
-    main()

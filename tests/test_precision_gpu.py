@@ -51,7 +51,7 @@ def test_ssfrk_bf16x3_k_split(curfp, tr, ul):
     (n = 16384, k = 36864: 4.9 GiB) runs as two k-slabs; C accumulates across
     them with beta applied once.  Checked on 256 sampled rows in FP64."""
     from curfp_b200 import precision as P
-    from scale_configs import rfp_offsets
+    from scale_lib import rfp_offsets
     n, k = 16384, 36864
     g = torch.Generator(device="cuda").manual_seed(k)
     A = torch.randn(n, k, device="cuda", generator=g) / k ** 0.5

@@ -1,4 +1,4 @@
-"""The FP64 checkers of tests/scale_configs.py on CPU: the RFP row gather
+"""The FP64 checkers of tests/scale_lib.py on CPU: the RFP row gather
 against the oracle's dense expansion, and the Woodbury (Gram-matrix) oracle
 of C = A A^T + lam I -- solve, residual, norms, log-determinant, traces and
 the GP NLL loss and gradients -- against dense FP64 computations and torch
@@ -8,7 +8,7 @@ import pytest
 import torch
 
 from conftest import VARIANTS
-from scale_configs import GramOracle, nll_exact, rfp_offsets, solve_errors
+from scale_lib import GramOracle, nll_exact, rfp_offsets, solve_errors
 
 
 @pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 8, 9, 64, 65])
