@@ -4,10 +4,14 @@ Workload (per GPU): n = 32768, transr='T', uplo='U', C = A A^T + 1.0 I with
 A ~ N(0,1)/sqrt(k), k = 1024, 64 right-hand sides B ~ N(0,1) -- synthetic and
 seeded, built on the device by the library's own ssfrk.
 One step = Cholesky of a fresh copy of C + solve of the 64 right-hand sides:
-  headline (--math bf16x3, default): curfpSpftrfEx(split-BF16 tensor-core
-      updates) + curfpSpftrsRefine(FP64-residual refinement, one correction);
-  also measured and reported beside it: the plain FP32 drop-in
-      (curfpSpftrf + curfpSpftrs).
+  headline (--math bf16x3, default): the precision form, curfpSpftrfEx
+      (split-BF16 tensor-core updates) + curfpSpftrsRefine (FP64-residual
+      refinement, one correction);
+  reported beside it on the same workload:
+    other_form: the plain FP32 form, every contraction in FP32 FMA on the
+      SIMT cores (curfpSetMathMode(CURFP_MATH_FP32), curfpSpftrf + curfpSpftrs);
+    drop_in: the drop-in entry points in the handle's default math mode
+      (split-BF16 contractions, curfpSpftrf + curfpSpftrs, no refinement).
 Metric: Cholesky+solve TFLOP/s = (n^3/3 + n^2/2 + n/6 + 2 n^2 nrhs) / time.
 The RFP matrix (2.1 GB) is larger than L2 (126 MB): no extra L2 flush.
 
@@ -22,9 +26,13 @@ The RFP matrix (2.1 GB) is larger than L2 (126 MB): no extra L2 flush.
 
 --impl reference times the reference's algorithm on the host cores: LAPACK's
 RFP routines (spftrf/spftrs via scipy/OpenBLAS, all threads), which the
-reference's GPU code translates call for call; each step is a bounded sample
-(n = 8192) of the same workload.  N > 1 GPUs run independent replicas (the
-path has no cross-GPU exchange); value = total flops / max-over-ranks time.
+reference's GPU code translates call for call, on the same workload (n =
+32768, k = 1024, 64 RHS; about 6 s per step on 16 cores).  Its line also
+carries `reference_gpu_build`: the reference's own GPU library (its
+unmodified sources compiled into oracle/_ref, cuBLAS/cuSOLVER) timed on the
+same workload on the GPU, when that library and a GPU are present.  N > 1
+GPUs run independent replicas (the path has no cross-GPU exchange); value =
+total flops / max-over-ranks time.
 """
 from __future__ import annotations
 
@@ -42,7 +50,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "RFP Cholesky+solve TFLOP/s at n=32768 (spftrf + spftrs 64 RHS), split-BF16 vs plain FP32"
-CPU_SAMPLE_N = 8192
+CPU_SAMPLE_N = 32768
+TRAFFIC_PROFILE = "profiles/tc_gemm_kernel-ssfrk-bf16-n16384-k8192-dram.txt"
 
 
 def chol_solve_flops(n: int, nrhs: int) -> float:
@@ -142,15 +151,16 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
-def profiled_traffic():
-    """DRAM bytes per tc_gemm_kernel launch of this step, from the ncu capture
-    summarised in profiles/tc_gemm_kernel-bench-n32768-traffic.txt (None if
-    the summary is absent)."""
+def profiled_bytes_per_flop():
+    """DRAM bytes per FP32-equivalent flop of tc_gemm_kernel, from the small
+    ncu capture summarised in TRAFFIC_PROFILE (None if absent).  It is not
+    measured in this run: the roofline's traffic is this ratio scaled to the
+    run's average flops per launch, and says so."""
     import re
-    f = ROOT / "profiles" / "tc_gemm_kernel-bench-n32768-traffic.txt"
+    f = ROOT / TRAFFIC_PROFILE
     if not f.exists():
         return None
-    m = re.search(r"traffic_bytes_per_launch\s+([0-9.eE+]+)", f.read_text())
+    m = re.search(r"dram_bytes_per_flop\s+([0-9.eE+-]+)", f.read_text())
     return float(m.group(1)) if m else None
 
 
@@ -162,48 +172,154 @@ def measured_peaks() -> dict:
     return {"bf16_tflops": 1590.0, "hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def cpu_baseline(n_sample: int = CPU_SAMPLE_N, nrhs: int = 64, reps: int = 2) -> dict:
-    """LAPACK (scipy/OpenBLAS) spftrf + spftrs on the host at n_sample."""
-    import numpy as np
+class HostLapack:
+    """The workload on the host: C = A A^T + 1.0 I built once by LAPACK ssfrk
+    (A n x k, seeded), then per step a fresh copy of C is factored (spftrf)
+    and 64 right-hand sides are solved (spftrs), all host threads
+    (scipy/OpenBLAS)."""
 
-    from oracle import port
-    rng = np.random.default_rng(0)
-    k = max(1, n_sample // 32)
-    A = (rng.standard_normal((n_sample, k)) / np.sqrt(k)).astype(np.float32)
-    B = rng.standard_normal((n_sample, nrhs)).astype(np.float32)
-    best = None
-    for _ in range(reps):
-        r = port.cholesky_solve(A, B, 1.0)
-        t = r["spftrf"] + r["spftrs"]
-        best = t if best is None else min(best, t)
-    val = chol_solve_flops(n_sample, nrhs) / best / 1e12
-    return {"value": round(val, 5), "unit": "TFLOP/s", "cores": port.threads(), "kind": "port",
-            "sample": f"LAPACK spftrf+spftrs (scipy {__import__('scipy').__version__}, OpenBLAS) "
-                      f"at n={n_sample}, nrhs={nrhs}, transr=T uplo=U, C=AA^T+I (k={k}), "
-                      f"best of {reps}"}
+    def __init__(self, n: int, k: int, nrhs: int):
+        import numpy as np
+        from scipy.linalg import lapack as la
+
+        from oracle import port
+        self.la, self.port = la, port
+        rng = np.random.default_rng(0)
+        A = np.asfortranarray(rng.standard_normal((n, k), dtype=np.float32) /
+                              np.float32(k ** 0.5))
+        self.B = np.asfortranarray(rng.standard_normal((n, nrhs), dtype=np.float32))
+        self.C = la.ssfrk(n, k, 1.0, A, 0.0, np.zeros(n * (n + 1) // 2, np.float32),
+                          transr="T", uplo="U", trans="N")
+        self.C[port.diag_indices(n, "T", "U")] += np.float32(1.0)
+        self.n, self.k, self.nrhs = n, k, nrhs
+
+    def step(self) -> float:
+        """Seconds of one spftrf + spftrs (the copy of C is not timed)."""
+        import time
+        C = self.C.copy()
+        t0 = time.perf_counter()
+        F, info = self.la.spftrf(self.n, C, transr="T", uplo="U", overwrite_a=1)
+        X, info2 = self.la.spftrs(self.n, F, self.B, transr="T", uplo="U")
+        t1 = time.perf_counter()
+        if info != 0 or info2 != 0:
+            raise RuntimeError(f"LAPACK failed: spftrf info={info} spftrs info={info2}")
+        return t1 - t0
+
+    def describe(self, reps: int) -> str:
+        import scipy
+        return (f"LAPACK spftrf+spftrs (scipy {scipy.__version__}, OpenBLAS) at n={self.n}, "
+                f"nrhs={self.nrhs}, transr=T uplo=U, C=AA^T+I (k={self.k}), "
+                f"{reps} step(s), {self.port.threads()} threads")
+
+
+def cpu_baseline(n: int = CPU_SAMPLE_N, k: int = 1024, nrhs: int = 64, reps: int = 2) -> dict:
+    """LAPACK (scipy/OpenBLAS) spftrf + spftrs on the host at the workload's
+    size, best of reps steps (about 6 s each at n = 32768 on 16 cores)."""
+    h = HostLapack(n, k, nrhs)
+    best = min(h.step() for _ in range(reps))
+    val = chol_solve_flops(n, nrhs) / best / 1e12
+    return {"value": round(val, 5), "unit": "TFLOP/s", "cores": h.port.threads(), "kind": "port",
+            "sample": h.describe(reps) + ", best step"}
+
+
+def tu_diag_offsets(n: int, device):
+    """Flat offsets of the diagonal in RFP transr='T', uplo='U' (LAPACK's
+    layout): n even, with h = n/2, the leading block's diagonal at
+    h(h+1) + i(h+1) and the trailing block's at h^2 + i(h+1); n odd, with
+    n1 = n//2 and n2 = n - n1, at n2^2 + i(n2+1) and n1 n2 + i(n2+1)."""
+    import torch
+    i = torch.arange(n, device=device, dtype=torch.int64)
+    if n % 2 == 0:
+        h = n // 2
+        return torch.where(i < h, h * (h + 1) + i * (h + 1), h * h + (i - h) * (h + 1))
+    n1 = n // 2
+    n2 = n - n1
+    return torch.where(i < n1, n2 * n2 + i * (n2 + 1), n1 * n2 + (i - n1) * (n2 + 1))
+
+
+def reference_gpu_build(n: int, k: int, nrhs: int, steps: int, warmup: int):
+    """The reference's own GPU library (oracle/_ref/libcurfp_ref.so, its
+    unmodified sources: cuBLAS/cuSOLVER) on the workload: curfpSpftrf +
+    curfpSpftrs per step on a fresh copy of C, CUDA events.  None when the
+    library or a GPU is absent.  Nothing of this repository's library runs
+    here (the input is built by the reference's own curfpSsfrk)."""
+    lib_path = ROOT / "oracle" / "_ref" / "libcurfp_ref.so"
+    try:
+        import torch
+        if not lib_path.exists() or not torch.cuda.is_available():
+            return None
+    except Exception:
+        return None
+    lib = ctypes.CDLL(str(lib_path))
+    h = ctypes.c_void_p()
+    assert lib.curfpCreate(ctypes.byref(h)) == 0
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    A = torch.randn(n, k, device="cuda", generator=g) / k ** 0.5
+    B0 = torch.randn(n, nrhs, device="cuda", generator=g)
+    nt = n * (n + 1) // 2
+    C0 = torch.empty(nt, device="cuda")
+    a, b = ctypes.c_float(1.0), ctypes.c_float(0.0)
+    # trans = T: A (n, k) row-major is the column-major k x n operand
+    assert lib.curfpSsfrk(h, 1, 1, 1, n, k, ctypes.byref(a), ctypes.c_void_p(A.data_ptr()), k,
+                          ctypes.byref(b), ctypes.c_void_p(C0.data_ptr())) == 0
+    C0[tu_diag_offsets(n, "cuda")] += 1.0
+    del A
+    C = torch.empty_like(C0)
+    X = torch.empty(nrhs, n, device="cuda")
+    Bc = B0.t().contiguous()
+    info = ctypes.c_int(0)
+
+    def step():
+        assert lib.curfpSpftrf(h, 1, 1, n, ctypes.c_void_p(C.data_ptr()), ctypes.byref(info)) == 0
+        assert lib.curfpSpftrs(h, 1, 1, n, nrhs, ctypes.c_void_p(C.data_ptr()),
+                               ctypes.c_void_p(X.data_ptr()), n) == 0
+
+    def prep():
+        C.copy_(C0)
+        X.copy_(Bc)
+
+    for _ in range(warmup):
+        prep()
+        step()
+    times = timed_steps(step, prep, steps, 1)
+    ms = sum(times) / len(times)
+    lib.curfpDestroy(h)
+    del C, C0, X, Bc, B0
+    torch.cuda.empty_cache()
+    return {"value": round(chol_solve_flops(n, nrhs) / (ms * 1e-3) / 1e12, 4), "unit": "TFLOP/s",
+            "ms_per_step": round(ms, 3), "steps": steps, "warmup": warmup,
+            "form": "reference curfp GPU build (unmodified sources, cuBLAS/cuSOLVER): "
+                    "curfpSpftrf + curfpSpftrs, FP32"}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    ns = args.cpu_n
+    host = HostLapack(args.cpu_n, args.k, args.nrhs)
     for _ in range(max(0, args.warmup)):
-        cpu_baseline(ns, reps=1)
-    vals = [cpu_baseline(ns, reps=1)["value"] for _ in range(args.steps)]
-    cb = cpu_baseline(ns, reps=1)
-    v = statistics.median(vals)
-    ms = chol_solve_flops(ns, args.nrhs) / (v * 1e12) * 1e3
-    cb["value"] = v
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "TFLOP/s",
+        host.step()
+    secs = [host.step() for _ in range(args.steps)]
+    ms = statistics.median(secs) * 1e3
+    v = chol_solve_flops(args.cpu_n, args.nrhs) / (ms * 1e-3) / 1e12
+    cb = {"value": round(v, 5), "unit": "TFLOP/s", "cores": host.port.threads(), "kind": "port",
+          "sample": host.describe(args.steps) + ", median step"}
+    del host
+    rgb = None
+    if not args.no_ref_gpu:
+        rgb = reference_gpu_build(args.n, args.k, args.nrhs, max(1, min(args.steps, 10)),
+                                  max(1, min(args.warmup, 3)))
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 5), "unit": "TFLOP/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"RFP Cholesky+solve on host LAPACK, sample n={ns}, "
-                                   f"nrhs={args.nrhs}, transr=T, uplo=U",
-                       "n": ns, "nrhs": args.nrhs, "parallelism": "host"},
+            "config": {"workload": f"RFP Cholesky+solve on host LAPACK, n={args.cpu_n}, "
+                                   f"k={args.k}, nrhs={args.nrhs}, transr=T, uplo=U",
+                       "n": args.cpu_n, "k": args.k, "nrhs": args.nrhs, "parallelism": "host",
+                       "same_config": args.cpu_n == args.n},
             "cpu_baseline": cb,
-            "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+            "e2e": {"value": round(v, 5), "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "reference_gpu_build": rgb}
     print(json.dumps(line), flush=True)
 
 
@@ -221,6 +337,14 @@ class Lib:
         st = self.lib.curfpSpftrfEx(self.h.ptr, 1, 1, n, ctypes.c_void_p(C.data_ptr()),
                                     ctypes.byref(self.info), math)
         assert st == 0 and self.info.value == 0, (st, self.info.value)
+
+    def spftrf_dropin(self, n, C):
+        st = self.lib.curfpSpftrf(self.h.ptr, 1, 1, n, ctypes.c_void_p(C.data_ptr()),
+                                  ctypes.byref(self.info))
+        assert st == 0 and self.info.value == 0, (st, self.info.value)
+
+    def set_mode(self, math):
+        assert self.lib.curfpSetMathMode(self.h.ptr, math) == 0
 
     def spftrs(self, n, nrhs, F, X):
         assert self.lib.curfpSpftrs(self.h.ptr, 1, 1, n, nrhs, ctypes.c_void_p(F.data_ptr()),
@@ -345,11 +469,17 @@ def run_ours(args, rank, world, local):
         L.spftrf(n, C, 1)
         L.refine(n, nrhs, C0, C, X, args.max_iter)
 
-    def step_plain():
-        L.spftrf(n, C, 0)
+    def step_plain():  # the drop-in entry points; FP32 SIMT once set_mode(0)
+        L.spftrf_dropin(n, C)
         L.spftrs(n, nrhs, C, X)
 
+    def residual():
+        """max_j ||b_j - A x_j|| / ||b_j|| with A x summed in FP64."""
+        r = B0.double() - P.ssfmm_acc64(C0, X.t().contiguous()).double()
+        return (torch.linalg.norm(r, dim=0) / torch.linalg.norm(B0.double(), dim=0)).max().item()
+
     step_head = step_prec if math_head else step_plain
+    L.set_mode(1 if math_head else 0)
     for _ in range(args.warmup):
         prep()
         step_head()
@@ -367,27 +497,40 @@ def run_ours(args, rank, world, local):
     ms_step = total_ms / args.steps
     value = world * args.steps * flops / (total_ms * 1e-3) / 1e12
 
-    # Accuracy of the measured step (FP64 backward errors, one solve).
+    # Accuracy of the measured step (FP64 residual of one solve).
     prep()
     step_head()
     torch.cuda.synchronize()
-    res = B0.double() - P.ssfmm_acc64(C0, X.t().contiguous()).double()
-    berr_solve = (torch.linalg.norm(res, dim=0) /
-                  torch.linalg.norm(B0.double(), dim=0)).max().item()
+    berr_solve = residual()
 
-    # The other form, same workload, for the ratio the metric names.
-    other = {}
+    def timed_form(step, mode):
+        L.set_mode(mode)
+        prep()
+        step()
+        t = timed_steps(step, prep, max(1, args.steps // 2), world)
+        ms_ = max_over_ranks(sum(t), world) / len(t)
+        prep()
+        step()
+        torch.cuda.synchronize()
+        return {"value": round(flops / (ms_ * 1e-3) / 1e12, 4), "unit": "TFLOP/s",
+                "ms_per_step": round(ms_, 3), "steps": len(t),
+                "solve_rel_residual_fp64": residual()}
+
+    # The other form, same workload, for the ratio the metric names, and the
+    # drop-in entry points in the handle's default math mode.
+    other, drop_in = {}, None
     if not args.no_other:
-        step_other = step_plain if math_head else step_prec
-        for _ in range(1):
-            prep()
-            step_other()
-        t_other = timed_steps(step_other, prep, max(1, args.steps // 2), world)
-        ms_other = max_over_ranks(sum(t_other), world) / len(t_other)
-        other = {"value": round(flops / (ms_other * 1e-3) / 1e12, 4), "unit": "TFLOP/s",
-                 "ms_per_step": round(ms_other, 3),
-                 "form": "plain FP32 (curfpSpftrf + curfpSpftrs)" if math_head
-                 else "split-BF16 (curfpSpftrfEx + curfpSpftrsRefine)"}
+        if math_head:
+            other = timed_form(step_plain, 0)
+            other["form"] = ("plain FP32: every contraction in FP32 FMA on the SIMT cores "
+                             "(curfpSetMathMode(CURFP_MATH_FP32); curfpSpftrf + curfpSpftrs)")
+            drop_in = timed_form(step_plain, 1)
+            drop_in["form"] = ("drop-in entry points in the handle's default math mode "
+                               "(split-BF16 contractions): curfpSpftrf + curfpSpftrs")
+        else:
+            other = timed_form(step_prec, 1)
+            other["form"] = "split-BF16 (curfpSpftrfEx + curfpSpftrsRefine)"
+    L.set_mode(1 if math_head else 0)  # the headline's mode for the passes below
 
     # Live per-kernel-class timing over the same steps (a second pass with the
     # library's event bracketing on; the headline number above has it off).
@@ -406,9 +549,16 @@ def run_ours(args, rank, world, local):
             # six BF16 tensor products per FP32 product: the tensor roofline in
             # FP32-equivalent flops is the BF16 peak / 6
             peak = peaks["bf16_tflops"] / 6.0
+            bpf = profiled_bytes_per_flop()
+            per_launch = prof[dom]["flops"] / max(1, prof[dom]["launches"])
             roof = {"kernel": "tc_gemm_kernel (split-BF16 tcgen05)", "bound": "tensor",
                     "achieved": round(ach, 2), "peak": round(peak, 2), "unit": "TFLOP/s",
-                    "frac": round(ach / peak, 4), "traffic": profiled_traffic(),
+                    "frac": round(ach / peak, 4),
+                    "traffic": round(bpf * per_launch, -3) if bpf is not None else None,
+                    "traffic_source": (f"not measured in this run: DRAM bytes per flop from the "
+                                       f"ncu capture in {TRAFFIC_PROFILE}, scaled to this run's "
+                                       f"average {per_launch:.3e} flops per launch"),
+                    "algorithmic_flops_per_launch": round(per_launch, -6),
                     "note": f"FP32-equivalent flops; peak = {peaks['source']} bf16 "
                             f"{peaks['bf16_tflops']} TFLOP/s / 6 products",
                     "share_of_step": round(prof[dom]["ms"] / sum(t for t in times), 3)}
@@ -448,9 +598,10 @@ def run_ours(args, rank, world, local):
                "unit": "TFLOP/s", "h2d_bytes_per_step": nt * 4 + n * nrhs * 4,
                "d2h_bytes_per_step": n * nrhs * 4}
 
+    L.set_mode(1)
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cb = cpu_baseline(args.cpu_n)
+        cb = cpu_baseline(args.cpu_n, args.k, args.nrhs)
     fb = None
     if not args.no_nll:
         fb = nll_fwd_bwd(local)
@@ -468,7 +619,8 @@ def run_ours(args, rank, world, local):
                            "refine_max_iter": args.max_iter if math_head else 0,
                            "parallelism": f"replicas x{world}",
                            "l2": "inputs (2.1 GB RFP) larger than L2, no flush"},
-                "other_form": other, "solve_rel_residual_fp64": berr_solve,
+                "other_form": other, "drop_in": drop_in,
+                "solve_rel_residual_fp64": berr_solve,
                 "gpu_launches": launches, "kernels": kernels,
                 "roofline": roof, "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cb,
                 "fwd_bwd": fb}
@@ -595,7 +747,9 @@ def main():
     ap.add_argument("--no-nll", action="store_true")
     ap.add_argument("--case", choices=CASES, default=None)
     ap.add_argument("--cpu-n", type=int, default=CPU_SAMPLE_N,
-                    help="host LAPACK sample size (cpu_baseline and --impl reference)")
+                    help="host LAPACK size (cpu_baseline and --impl reference)")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="--impl reference: skip the reference GPU build timing")
     args = ap.parse_args()
     if args.case:
         run_case(args)

@@ -33,7 +33,7 @@ def _worker(rank, world, port, outdir):
     assert (r, w) == (rank, world)
     bench.barrier(w)
     m = bench.max_over_ranks(float(rank + 1), w)
-    args = SimpleNamespace(steps=1, warmup=0, nrhs=8, cpu_n=256)
+    args = SimpleNamespace(steps=1, warmup=0, nrhs=8, cpu_n=256, n=256, k=32, no_ref_gpu=True)
     buf = io.StringIO()
     with redirect_stdout(buf):
         bench.run_reference(args, r, w)
