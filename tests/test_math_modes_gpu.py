@@ -159,11 +159,14 @@ def test_ssfr2k_math_mode(curfp, mode, trans, tr, ul):
     Bop = torch.randn(n, k, device="cuda", generator=g) / k ** 0.5
     C0 = torch.randn(n * (n + 1) // 2, device="cuda", generator=g)
     C = C0.clone()
-    # trans = T: A (n, k) row-major; trans = N: A column-major n x k = (k, n) row-major
+    # trans = T: A (n, k) row-major; trans = N: A column-major n x k, whose
+    # memory is the (k, n) row-major tensor, with k and lda = n given
+    # explicitly as the reference's wrapper expects for that layout
     Ain = Aop.contiguous() if trans == "T" else Aop.t().contiguous()
     Bin = Bop.contiguous() if trans == "T" else Bop.t().contiguous()
+    kw = {} if trans == "T" else {"k": k, "lda": n, "ldb": n}
     with Mode(curfp, mode) as m:
-        curfp.ssfr2k(Ain, Bin, C, alpha=0.5, beta=-1.5, transr=T, uplo=U, trans=trans)
+        curfp.ssfr2k(Ain, Bin, C, alpha=0.5, beta=-1.5, transr=T, uplo=U, trans=trans, **kw)
         torch.cuda.synchronize()
     m.check_engine()
     Ad, Bd = Aop.double(), Bop.double()
