@@ -697,8 +697,11 @@ curfpStatus_t curfpSsfrkBackward(curfpHandle_t handle, curfpOperation_t transr,
                                            *alpha, 0.0f));
 }
 
-// Cotangent of the stored elements of A from that of its Cholesky factor
-// (rfp::plan::spftrf_backward), packed to RFP with the diagonal halved.
+// Cotangent of the stored elements of A from that of its Cholesky factor,
+// computed in place in Abar by the blocked RFP adjoint
+// (rfp::plan::spftrf_adjoint): only L and the cotangent are held, plus the
+// solves' diagonal-block inverses (n/64 records of 32 KB).  Abar may alias
+// Lbar; it must not alias L, which is read throughout.
 static curfpStatus_t spftrf_backward_body(curfpHandle_t handle, curfpOperation_t transr,
                                           curfpFillMode_t uplo, int n, const float* L,
                                           const float* Lbar, float* Abar, curfpMath_t math) {
@@ -706,16 +709,14 @@ static curfpStatus_t spftrf_backward_body(curfpHandle_t handle, curfpOperation_t
   if (n < 0) return CURFP_STATUS_INVALID_VALUE;
   if (math != CURFP_MATH_FP32 && math != CURFP_MATH_SPLIT_BF16) return CURFP_STATUS_INVALID_VALUE;
   if (n == 0) return CURFP_STATUS_SUCCESS;
+  if (!L || !Lbar || !Abar || Abar == L) return CURFP_STATUS_INVALID_VALUE;
   const int tr = transr == CURFP_OP_T, lower = uplo == CURFP_FILL_MODE_LOWER;
-  const int64_t ldd = n;
-  float* D = static_cast<float*>(rfp::grow_buffer(handle, &handle->wsg, &handle->wsg_bytes,
-                                                  (size_t)n * n * sizeof(float)));
-  if (!D) return CURFP_STATUS_ALLOC_FAILED;
+  if (Abar != Lbar &&
+      cudaMemcpyAsync(Abar, Lbar, (size_t)n * (n + 1) / 2 * sizeof(float),
+                      cudaMemcpyDeviceToDevice, handle->stream) != cudaSuccess)
+    return CURFP_STATUS_EXECUTION_FAILED;
   CudaExec ex(handle);
-  rfp::View S{};
-  int rc = rfp::plan::spftrf_backward(ex, tr, lower, n, L, Lbar, D, ldd, &S, (int)math);
-  if (rc) return status_of(rc);
-  return pack_strided(handle, tr, lower, n, S.p, Abar, S.rs, S.cs, 1, 0.5f);
+  return status_of(rfp::plan::spftrf_adjoint(ex, tr, lower, n, L, Abar, (int)math));
 }
 
 // X = A^-1 B with A = L L^T:  Bbar := A^-1 Xbar and

@@ -37,7 +37,7 @@ struct curfpContext {
   rfp::Profiler prof;      // optional per-class event timing
   void* tsv = nullptr;     // wavefront solve flags / tickets
   size_t tsv_bytes = 0;
-  void* wsg = nullptr;     // dense n x n scratch of the Cholesky adjoint
+  void* wsg = nullptr;     // adjoint scratch (solve adjoint n x 2nrhs, NLL gradient)
   size_t wsg_bytes = 0;
 };
 
@@ -62,7 +62,7 @@ class CudaExecT : public ExecT<T> {
   int gemm_pair(ViewT<T> X, ViewT<T> Y, int rows, int k, const SharedTaskT<T>* t, int count,
                 int math) override;
   int trsm_wave(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const T* W) override;
-  int mirror_lower(ViewT<T> D, int n) override;
+  int potrf_adj_tile(ViewT<T> L, ViewT<T> G, int n) override;
 
  protected:
   curfpContext* ctx_;

@@ -68,6 +68,7 @@ constexpr int kTrsmLeaf = 64;    // TRSM diagonal blocks (inverted, then multipl
 // wavefront solve uses it).
 constexpr int kInvStride = 2 * kTrsmLeaf * kTrsmLeaf;
 constexpr int kTriTile = 64;     // trtri / lauum tiles
+constexpr int kAdjTile = 64;     // Cholesky-adjoint diagonal tiles
 constexpr int kTrmmLeaf = 64;    // TRMM leaves (masked in-place multiply)
 constexpr int kTrsvMaxRhs = 512; // wavefront solve for at most this many RHS
 constexpr int kTrsvMaxRhsTc = 64;  // ... when the updates may use the tensor cores
@@ -106,9 +107,11 @@ class ExecT {
     (void)L; (void)n; (void)B; (void)m; (void)alpha; (void)W;
     return kNotSupported;
   }
-  // D(j,i) := D(i,j) for i > j (n x n view): the stored lower triangle is
-  // mirrored into the upper one.
-  virtual int mirror_lower(ViewT<T> D, int n) = 0;
+  // Adjoint of the Cholesky factorization of one diagonal tile
+  // (n <= kAdjTile): L is the factor (lower triangle read), G holds the
+  // cotangent of L's stored lower elements on entry and that of the factored
+  // matrix's stored lower elements on exit (lower triangle, in place).
+  virtual int potrf_adj_tile(ViewT<T> L, ViewT<T> G, int n) = 0;
   // Contractions sharing one operand matrix.  The default lowers them to
   // gemm(); the CUDA executor stages X once for the tensor-core path.
   virtual int gemm_shared(ViewT<T> X, int rows, int k, const SharedTaskT<T>* t, int count,
@@ -214,31 +217,23 @@ int rfp_trsm(ExecT<T>& ex, int transr, int lower, int n, const T* L, int trans, 
 // B := L^T B (B dense n x m).
 template <typename T>
 int rfp_trmm_t(ExecT<T>& ex, int transr, int lower, int n, const T* L, ViewT<T> B, int m);
-// D(i,j) := (L^T Lbar)(i,j) for i >= j (D dense n x n view; upper part
-// untouched); L and Lbar in RFP with the same variant.
-template <typename T>
-int rfp_ltl(ExecT<T>& ex, int transr, int lower, int n, const T* L, const T* Lbar,
-            ViewT<T> D);
 // Lower triangle of the logical matrix C (RFP): C := alpha (A1 B1 + A2 B2)
 // + beta C with A1, A2 n x k and B1, B2 k x n dense views.
 template <typename T>
 int rfp_gemm_lower2(ExecT<T>& ex, int transr, int lower, int n, T* C, ViewT<T> A1, ViewT<T> B1,
                     ViewT<T> A2, ViewT<T> B2, int k, Scalar<T> alpha, Scalar<T> beta);
-// L^T X = B for the lower triangle of X only (diagonal included): reads the
-// lower triangle of B and overwrites it with that of X; above the diagonal B
-// may hold anything and is left undefined.  n^3/3 flops instead of n^3.
+// Adjoint of the Cholesky factorization, in place on the lower triangle
+// (recursive blocked algorithm; no scratch beyond the solves' diagonal-block
+// inverses).  L is the factor; G holds the cotangent of L's stored lower
+// elements on entry and, on exit, the cotangent of the factored matrix's
+// stored lower elements (an off-diagonal stored element stands for two
+// entries of the symmetric matrix).
 template <typename T>
-int trsm_lt_lowerout(ExecT<T>& ex, ViewT<T> L, int n, ViewT<T> B, int math = 0);
-// Adjoint of the Cholesky factorization.  Given the factor L and the cotangent
-// Lbar of its stored lower triangle (both RFP, same variant), leaves in the
-// view S (n x n, dense, anything may alias nothing) the lower triangle of
-// S = L^-T Q L^-1 with Q the symmetric matrix whose lower triangle is that of
-// L^T Lbar.  The cotangent of the stored triangle of A is then S(p,q) for
-// p > q and S(p,p)/2 on the diagonal.  D is an n x n column-major scratch;
-// S is returned as a view into D.
+int potrf_adj_lower(ExecT<T>& ex, ViewT<T> L, ViewT<T> G, int n, int math = 0);
+// The same for RFP arrays of the same variant: L the factor, G the cotangent
+// (overwritten in place).
 template <typename T>
-int spftrf_backward(ExecT<T>& ex, int transr, int lower, int n, const T* L,
-                    const T* Lbar, T* D, int64_t ldd, ViewT<T>* S, int math = 0);
+int spftrf_adjoint(ExecT<T>& ex, int transr, int lower, int n, const T* L, T* G, int math = 0);
 // Y := alpha A X + beta Y for the symmetric matrix A held in the RFP array
 // (any variant); X, Y dense n x m views.  alpha == 0 reads neither A nor X.
 template <typename T>

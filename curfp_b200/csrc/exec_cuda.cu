@@ -248,12 +248,14 @@ bool smem_attr(K kernel, int bytes) {
 }  // namespace
 
 template <typename T>
-int CudaExecT<T>::mirror_lower(ViewT<T> D, int n) {
-  if (n <= 1) return 0;
-  const int t = (n + ktile::MTS - 1) / ktile::MTS;
-  ProfScope ps(ctx_->prof, ctx_->stream, K_PACK, 0, (double)sizeof(T) * n * (double)(n - 1));
-  ktile::mirror_lower<T>
-      <<<t * (t + 1) / 2, dim3(ktile::MTS, ktile::MTY), 0, ctx_->stream>>>(D, n);
+int CudaExecT<T>::potrf_adj_tile(ViewT<T> L, ViewT<T> G, int n) {
+  if (n <= 0) return 0;
+  if (n > ktile::T) return 3;
+  ProfScope ps(ctx_->prof, ctx_->stream, K_POTRF, 2.0 * n * (double)n * n / 3.0, 0);
+  constexpr int smem = ktile::adj_smem<T>();
+  static const bool attr = smem_attr(ktile::potrf_adj_tile<T>, smem);
+  if (!attr) return 4;
+  ktile::potrf_adj_tile<T><<<1, ktile::ADJ_THREADS, smem, ctx_->stream>>>(L, G, n);
   ++ctx_->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }

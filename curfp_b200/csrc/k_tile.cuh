@@ -1,7 +1,8 @@
 // k_tile.cuh — single-CTA kernels on small triangular tiles held in shared
 // memory: the diagonal Cholesky tile (the only place pivots are checked), the
-// inverses of diagonal blocks used by the blocked TRSM, and the in-place
-// inverse / L^T L tiles of the blocked spftri.
+// inverses of diagonal blocks used by the blocked TRSM, the in-place
+// inverse / L^T L tiles of the blocked spftri and the diagonal tiles of the
+// Cholesky adjoint.
 #pragma once
 #include <climits>
 #include <cstdint>
@@ -363,35 +364,53 @@ __global__ void __launch_bounds__(256) lauum_tile(ViewT<E> L, int n) {
   }
 }
 
-constexpr int MTS = 32, MTY = 8;  // mirror tile edge, thread rows
-
-// D(q,p) := D(p,q) for p > q on an n x n view: one 32 x 32 tile of the lower
-// tile triangle per CTA, read along the view's contiguous dimension and
-// written transposed through shared memory, so both sides coalesce.
+// Adjoint of the Cholesky factorization of one diagonal tile (n <= T), in
+// place on G's lower triangle.  Column j = n-1 .. 0 reverses the forward
+// step that produced column j of L (l = L(j,j), v = L(j+1:, j)) once the
+// trailing block's cotangent G(j+1:, j+1:) is final:
+//   w = (tril(G_t) + tril(G_t)^T) v      (G_t's diagonal counted twice)
+//   G(j+1:, j) = (G(j+1:, j) - w) / l
+//   G(j, j)    = (G(j, j) - G(j+1:, j)^T v) / (2 l)
+// Four threads share a row of w (strided k, shuffle sum); warp 0 forms the
+// diagonal dot product.  Two block barriers per column.
+constexpr int ADJ_THREADS = 256;
 template <typename E>
-__global__ void __launch_bounds__(MTS * MTY) mirror_lower(ViewT<E> D, int n) {
-  __shared__ E tile[MTS][MTS + 1];
-  const int lt = blockIdx.x;
-  int tp = (int)((sqrt(8.0 * (double)lt + 1.0) - 1.0) * 0.5);
-  while ((tp + 1) * (tp + 2) / 2 <= lt) ++tp;
-  while (tp * (tp + 1) / 2 > lt) --tp;
-  const int tq = lt - tp * (tp + 1) / 2;
-  const int p0 = tp * MTS, q0 = tq * MTS;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const bool pc = (D.rs == 1 || D.rs == -1);
-#pragma unroll
-  for (int r = 0; r < MTS / MTY; ++r) {
-    const int lp = pc ? tx : ty + r * MTY, lq = pc ? ty + r * MTY : tx;
-    const int p = p0 + lp, q = q0 + lq;
-    if (p < n && p > q) tile[lp][lq] = D.p[(int64_t)p * D.rs + (int64_t)q * D.cs];
-  }
+constexpr int adj_smem() { return 2 * T * LD * (int)sizeof(E); }
+
+template <typename E>
+__global__ void __launch_bounds__(ADJ_THREADS) potrf_adj_tile(ViewT<E> L, ViewT<E> G, int n) {
+  extern __shared__ __align__(16) unsigned char adj_raw[];
+  E* Ls = reinterpret_cast<E*>(adj_raw);
+  E* Gs = Ls + T * LD;
+  load_lower<LD>(L, n, Ls);
+  load_lower<LD>(G, n, Gs);
   __syncthreads();
+  const int tid = threadIdx.x, r = tid >> 2, sl = tid & 3;
+  for (int j = n - 1; j >= 0; --j) {
+    const E l = Ls[j * LD + j];
+    const int p = j + 1 + r;
+    E w = E(0);
+    if (p < n) {
+      for (int q = j + 1 + sl; q < n; q += 4) {
+        const E g = q < p ? Gs[p * LD + q] : (q > p ? Gs[q * LD + p] : E(2) * Gs[p * LD + p]);
+        w += g * Ls[q * LD + j];
+      }
+    }
+    w += __shfl_xor_sync(0xffffffffu, w, 1);
+    w += __shfl_xor_sync(0xffffffffu, w, 2);
+    // column j is not read above (q, p > j), so it is updated in place
+    if (p < n && sl == 0) Gs[p * LD + j] = (Gs[p * LD + j] - w) / l;
+    __syncthreads();
+    if (tid < 32) {
+      E d = E(0);
+      for (int i = j + 1 + tid; i < n; i += 32) d += Gs[i * LD + j] * Ls[i * LD + j];
 #pragma unroll
-  for (int r = 0; r < MTS / MTY; ++r) {
-    const int lq = pc ? tx : ty + r * MTY, lp = pc ? ty + r * MTY : tx;
-    const int p = p0 + lp, q = q0 + lq;
-    if (p < n && p > q) D.p[(int64_t)q * D.rs + (int64_t)p * D.cs] = tile[lp][lq];
+      for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+      if (tid == 0) Gs[j * LD + j] = (Gs[j * LD + j] - d) / (E(2) * l);
+    }
+    __syncthreads();
   }
+  store_lower<LD>(G, n, Gs);
 }
 
 }  // namespace ktile

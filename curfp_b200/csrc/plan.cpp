@@ -363,43 +363,6 @@ int rfp_trmm_t(ExecT<T>& ex, int transr, int lower, int n, const T* L, ViewT<T> 
 }
 
 template <typename T>
-int rfp_ltl(ExecT<T>& ex, int transr, int lower, int n, const T* L, const T* Lbar,
-            ViewT<T> D) {
-  Blocks<T> a = blocks(transr, lower, n, L), c = blocks(transr, lower, n, Lbar);
-  const int n1 = a.g.n1, n2 = a.g.n2;
-  GemmProbT<T> p[3];
-  int cnt = 0;
-  // (L^T Lbar) lower blocks:
-  //   11: tril(L11^T Lbar11) + L21^T Lbar21     21: L22^T Lbar21
-  //   22: tril(L22^T Lbar22)
-  if (n1 > 0) {
-    GemmProbT<T> q = gemm_prob(tr(a.V11), c.V11, D, n1, n1, n1, 1.0f, 0.0f, 0);
-    q.a_tri = 2;  // L11^T is upper
-    q.b_tri = 1;  // Lbar11 is lower
-    if (n2 > 0) {
-      q.A2 = tr(a.V21);
-      q.B2 = c.V21;
-      q.k2 = n2;
-    }
-    q.c_lower = 1;
-    p[cnt++] = q;
-  }
-  if (n1 > 0 && n2 > 0) {
-    GemmProbT<T> q = gemm_prob(tr(a.V22), c.V21, sub(D, n1, 0), n2, n1, n2, 1.0f, 0.0f, 0);
-    q.a_tri = 2;
-    p[cnt++] = q;
-  }
-  if (n2 > 0) {
-    GemmProbT<T> q = gemm_prob(tr(a.V22), c.V22, sub(D, n1, n1), n2, n2, n2, 1.0f, 0.0f, 0);
-    q.a_tri = 2;
-    q.b_tri = 1;
-    q.c_lower = 1;
-    p[cnt++] = q;
-  }
-  return ex.gemm(p, cnt);
-}
-
-template <typename T>
 int rfp_gemm_lower2(ExecT<T>& ex, int transr, int lower, int n, T* C, ViewT<T> A1, ViewT<T> B1,
                     ViewT<T> A2, ViewT<T> B2, int k, Scalar<T> alpha, Scalar<T> beta) {
   Blocks<T> c = blocks(transr, lower, n, C);
@@ -422,58 +385,57 @@ int rfp_gemm_lower2(ExecT<T>& ex, int transr, int lower, int n, T* C, ViewT<T> A
   return ex.gemm(p, cnt);
 }
 
-template <typename T>
-int trsm_lt_lowerout(ExecT<T>& ex, ViewT<T> L, int n, ViewT<T> B, int math) {
-  if (n <= 0) return 0;
-  if (n <= kWaveLeaf) return trsm(ex, 1, 1, 1, L, B, n, n, 1.0f, math);
-  // L = [L11 0; L21 L22]:  L22^T X22 = B22 (lower part), L22^T X21 = B21,
-  // L11^T X11 = B11 - L21^T X21 (lower part).
-  const int n1 = split(n, kTriTile), n2 = n - n1;
-  ViewT<T> L11 = L, L21 = sub(L, n1, 0), L22 = sub(L, n1, n1);
-  ViewT<T> B11 = B, B21 = sub(B, n1, 0), B22 = sub(B, n1, n1);
-  int rc;
-  if ((rc = trsm_lt_lowerout(ex, L22, n2, B22, math))) return rc;
-  if ((rc = trsm(ex, 1, 1, 1, L22, B21, n2, n1, 1.0f, math))) return rc;
-  GemmProbT<T> p = gemm_prob(tr(L21), B21, B11, n1, n1, n2, -1.0f, 1.0f, math);
-  p.c_lower = 1;
-  if ((rc = ex.gemm(&p, 1))) return rc;
-  return trsm_lt_lowerout(ex, L11, n1, B11, math);
-}
-
 namespace {
-// trsm_lt_lowerout with L the logical factor of an RFP array.
+// One panel step of the blocked Cholesky adjoint.  With the trailing block's
+// adjoint G22 final (stored lower triangle of the cotangent of
+// S = A22 - L21 L21^T):
+//   G21 -= (tril(G22) + tril(G22)^T) L21     (S's diagonal counted twice)
+//   G21 := G21 L11^{-1}                       (cotangent of A21 = L21 L11^T)
+//   G11 -= tril(G21^T L21)                    (L11's share through L21)
 template <typename T>
-int rfp_trsm_lowerout(ExecT<T>& ex, int transr, int lower, int n, const T* L, ViewT<T> B,
-                      int math) {
-  Blocks<T> b = blocks(transr, lower, n, L);
-  const int n1 = b.g.n1, n2 = b.g.n2;
-  ViewT<T> B11 = B, B21 = sub(B, n1, 0), B22 = sub(B, n1, n1);
+int adj_panel(ExecT<T>& ex, ViewT<T> L11, ViewT<T> L21, ViewT<T> G11, ViewT<T> G21,
+              ViewT<T> G22, int n1, int n2, int math) {
+  GemmProbT<T> p = gemm_prob(G22, L21, G21, n2, n1, n2, -1.0f, 1.0f, math);
+  p.a_tri = 1;          // lower(G22), diagonal included
+  p.A2 = tr(G22);
+  p.B2 = L21;
+  p.k2 = n2;
+  p.a2_tri = 2;         // lower(G22)^T, diagonal included again
   int rc;
-  if ((rc = trsm_lt_lowerout(ex, b.V22, n2, B22, math))) return rc;
-  if (n1 > 0 && n2 > 0) {
-    if ((rc = trsm(ex, 1, 1, 1, b.V22, B21, n2, n1, 1.0f, math))) return rc;
-    GemmProbT<T> p = gemm_prob(tr(b.V21), B21, B11, n1, n1, n2, -1.0f, 1.0f, math);
-    p.c_lower = 1;
-    if ((rc = ex.gemm(&p, 1))) return rc;
-  }
-  return trsm_lt_lowerout(ex, b.V11, n1, B11, math);
+  if ((rc = ex.gemm(&p, 1))) return rc;
+  if ((rc = trsm(ex, 0, 1, 0, L11, G21, n2, n1, 1.0f, math))) return rc;
+  GemmProbT<T> q = gemm_prob(tr(G21), L21, G11, n1, n1, n2, -1.0f, 1.0f, math);
+  q.c_lower = 1;
+  return ex.gemm(&q, 1);
 }
 }  // namespace
 
 template <typename T>
-int spftrf_backward(ExecT<T>& ex, int transr, int lower, int n, const T* L,
-                    const T* Lbar, T* D, int64_t ldd, ViewT<T>* S, int math) {
-  ViewT<T> Dv{D, 1, ldd};
+int potrf_adj_lower(ExecT<T>& ex, ViewT<T> L, ViewT<T> G, int n, int math) {
+  if (n <= 0) return 0;
+  if (n <= kAdjTile) return ex.potrf_adj_tile(L, G, n);
+  const int n1 = split(n, kAdjTile), n2 = n - n1;
   int rc;
-  // lower(Q) = lower(L^T Lbar); Q symmetric
-  if ((rc = rfp_ltl(ex, transr, lower, n, L, Lbar, Dv))) return rc;
-  if ((rc = ex.mirror_lower(Dv, n))) return rc;
-  // Z = L^-T Q, then S = L^-T Z^T (= Z L^-1, symmetric): lower part only
-  if ((rc = rfp_trsm(ex, transr, lower, n, L, 1, Dv, n, 1.0f, math))) return rc;
-  ViewT<T> St = tr(Dv);
-  if ((rc = rfp_trsm_lowerout(ex, transr, lower, n, L, St, math))) return rc;
-  *S = St;
-  return 0;
+  if ((rc = potrf_adj_lower(ex, sub(L, n1, n1), sub(G, n1, n1), n2, math))) return rc;
+  if ((rc = adj_panel(ex, L, sub(L, n1, 0), G, sub(G, n1, 0), sub(G, n1, n1), n1, n2, math)))
+    return rc;
+  return potrf_adj_lower(ex, L, G, n1, math);
+}
+
+// The RFP factor's three logical blocks follow the forward decomposition
+// (src/curfp_spftrf.cpp:254-282: POTRF T1, TRSM S, SYRK T2, POTRF T2), so the
+// adjoint runs the same panel step once on the blocks, between the two
+// diagonal-block adjoints taken in reverse order.
+template <typename T>
+int spftrf_adjoint(ExecT<T>& ex, int transr, int lower, int n, const T* L, T* G, int math) {
+  Blocks<T> b = blocks(transr, lower, n, L), c = blocks(transr, lower, n, (const T*)G);
+  const int n1 = b.g.n1, n2 = b.g.n2;
+  int rc;
+  if ((rc = potrf_adj_lower(ex, b.V22, c.V22, n2, math))) return rc;
+  if (n1 > 0 && n2 > 0 &&
+      (rc = adj_panel(ex, b.V11, b.V21, c.V11, c.V21, c.V22, n1, n2, math)))
+    return rc;
+  return potrf_adj_lower(ex, b.V11, c.V11, n1, math);
 }
 
 namespace {
@@ -560,12 +522,10 @@ int rfp_symm_dbl(ExecT<T>& ex, int transr, int lower, int n, const T* G, ViewT<T
   template int rfp_trsm<T>(ExecT<T>&, int, int, int, const T*, int, ViewT<T>, int, Scalar<T>, \
                            int);                                                             \
   template int rfp_trmm_t<T>(ExecT<T>&, int, int, int, const T*, ViewT<T>, int);              \
-  template int rfp_ltl<T>(ExecT<T>&, int, int, int, const T*, const T*, ViewT<T>);            \
   template int rfp_gemm_lower2<T>(ExecT<T>&, int, int, int, T*, ViewT<T>, ViewT<T>, ViewT<T>, \
                                   ViewT<T>, int, Scalar<T>, Scalar<T>);                      \
-  template int trsm_lt_lowerout<T>(ExecT<T>&, ViewT<T>, int, ViewT<T>, int);                  \
-  template int spftrf_backward<T>(ExecT<T>&, int, int, int, const T*, const T*, T*, int64_t,  \
-                                  ViewT<T>*, int);                                           \
+  template int potrf_adj_lower<T>(ExecT<T>&, ViewT<T>, ViewT<T>, int, int);                 \
+  template int spftrf_adjoint<T>(ExecT<T>&, int, int, int, const T*, T*, int);                \
   template int rfp_symm<T>(ExecT<T>&, int, int, int, const T*, ViewT<T>, ViewT<T>, int,       \
                            Scalar<T>, Scalar<T>);                                            \
   template int rfp_symm_dbl<T>(ExecT<T>&, int, int, int, const T*, ViewT<T>, ViewT<T>, int,   \

@@ -244,9 +244,11 @@ curfpStatus_t curfpSsfrkBackward(curfpHandle_t handle, curfpOperation_t transr,
 
 /* Adjoint of curfpSpftrf: L is the factor (as curfpSpftrf leaves it), Lbar
  * the cotangent of its stored elements; Abar receives the cotangent of the
- * stored elements of A (Abar may alias L or Lbar).  Uses n*n floats of
- * handle-owned scratch; math selects the arithmetic of its triangular
- * solves (CURFP_MATH_SPLIT_BF16: split-BF16 tensor-core updates). */
+ * stored elements of A.  Computed in RFP layout by a recursive blocked
+ * algorithm, in place in Abar (which may alias Lbar, not L): no n x n
+ * scratch, only the solves' diagonal-block inverses.  math selects the
+ * arithmetic of its triangular solves (CURFP_MATH_SPLIT_BF16: split-BF16
+ * tensor-core updates where large). */
 curfpStatus_t curfpSpftrfBackward(curfpHandle_t handle, curfpOperation_t transr,
                                   curfpFillMode_t uplo, int n, const float *L,
                                   const float *Lbar, float *Abar,

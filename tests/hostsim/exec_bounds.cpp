@@ -150,9 +150,11 @@ class BoundsExec : public Exec {
     check("trsm_wave W", View{const_cast<float*>(W), 1, kInvStride}, kInvStride, nblk, 0);
     return 0;
   }
-  int mirror_lower(View D, int n) override {
+  int potrf_adj_tile(View L, View G, int n) override {
     ++calls;
-    check("mirror_lower", D, n, n, 0);
+    if (n > kAdjTile) return 3;
+    check("potrf_adj_tile L", L, n, n, 1);
+    check("potrf_adj_tile G", G, n, n, 1);
     return 0;
   }
 };
@@ -166,6 +168,8 @@ extern "C" {
 //   op 2 spftrs (k right-hand sides, ldb = n)            op 3 spftri
 //   op 4 L X = B and op 5 L^T X = B on the RFP factor (B n x k row-major)
 //   op 6 in-place RFP triangular inverse
+//   op 7 Cholesky adjoint (a second RFP array holds the cotangent)
+//   op 8 ssfr2k (trans = T, A and B row-major n x k)
 // Returns the planner's status; out[0..2] = calls, range checks, violations.
 // msg (256 bytes) receives the first violation.
 int hs_bounds(int op, int transr, int lower, int n, int k, int math, int64_t* out, char* msg) {
@@ -193,6 +197,17 @@ int hs_bounds(int op, int transr, int lower, int n, int k, int math, int64_t* ou
       break;
     }
     case 6: rc = plan::rfp_trtri(ex, transr, lower, n, C, math); break;
+    case 7: {
+      float* G = ex.add("cotangent", nt);
+      rc = plan::spftrf_adjoint(ex, transr, lower, n, C, G, math);
+      break;
+    }
+    case 8: {
+      float* A = ex.add("A", (size_t)n * k);
+      float* B = ex.add("B", (size_t)n * k);
+      rc = plan::ssfr2k(ex, transr, lower, 1, n, k, 1.0f, A, k, B, k, 0.0f, C, math);
+      break;
+    }
     default: break;
   }
   out[0] = ex.calls;

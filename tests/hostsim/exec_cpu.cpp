@@ -156,9 +156,32 @@ class CpuExec : public Exec {
     return 0;
   }
 
-  int mirror_lower(View D, int n) override {
-    for (int q = 0; q < n; ++q)
-      for (int p = q + 1; p < n; ++p) at(D, q, p) = at(D, p, q);
+  // Same column recurrence as the GPU tile kernel, in FP64.
+  int potrf_adj_tile(View L, View G, int n) override {
+    if (n > kAdjTile) return 3;
+    std::vector<double> l((size_t)n * n, 0.0), g((size_t)n * n, 0.0);
+    for (int p = 0; p < n; ++p)
+      for (int q = 0; q <= p; ++q) {
+        l[(size_t)p * n + q] = at(L, p, q);
+        g[(size_t)p * n + q] = at(G, p, q);
+      }
+    for (int j = n - 1; j >= 0; --j) {
+      const double lj = l[(size_t)j * n + j];
+      for (int p = j + 1; p < n; ++p) {
+        double w = 0.0;
+        for (int q = j + 1; q < n; ++q) {
+          const double gv = q < p ? g[(size_t)p * n + q]
+                                  : (q > p ? g[(size_t)q * n + p] : 2.0 * g[(size_t)p * n + p]);
+          w += gv * l[(size_t)q * n + j];
+        }
+        g[(size_t)p * n + j] = (g[(size_t)p * n + j] - w) / lj;
+      }
+      double d = 0.0;
+      for (int p = j + 1; p < n; ++p) d += g[(size_t)p * n + j] * l[(size_t)p * n + j];
+      g[(size_t)j * n + j] = (g[(size_t)j * n + j] - d) / (2.0 * lj);
+    }
+    for (int p = 0; p < n; ++p)
+      for (int q = 0; q <= p; ++q) at(G, p, q) = (float)g[(size_t)p * n + q];
     return 0;
   }
 
@@ -205,18 +228,14 @@ int hs_spftri(int transr, int lower, int n, float* A) {
   return plan::spftri(ex, transr, lower, n, A);
 }
 
-// Lower triangle of S = L^-T Q L^-1 (Cholesky adjoint) written to S[p*n+q]
-// (row-major, p >= q).
-int hs_spftrf_backward(int transr, int lower, int n, const float* L, const float* Lbar,
-                       float* S, int math) {
+// Cholesky adjoint in RFP (same planning as curfpSpftrfBackward): G holds
+// the factor's cotangent on entry and the matrix's on exit (RFP, in place).
+int hs_spftrf_backward(int transr, int lower, int n, const float* L, float* G, int math,
+                       long* calls) {
   CpuExec ex;
-  std::vector<float> D((size_t)n * n, 0.0f);
-  View Sv{};
-  int rc = plan::spftrf_backward(ex, transr, lower, n, L, Lbar, D.data(), n, &Sv, math);
-  if (rc) return rc;
-  for (int p = 0; p < n; ++p)
-    for (int q = 0; q <= p; ++q) S[(size_t)p * n + q] = at(Sv, p, q);
-  return 0;
+  int rc = plan::spftrf_adjoint(ex, transr, lower, n, L, G, math);
+  if (calls) *calls = ex.gemm_calls;
+  return rc;
 }
 
 // Same arithmetic as curfpSsfrkBackward.

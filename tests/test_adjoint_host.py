@@ -53,36 +53,46 @@ def test_chol_adjoint_formula_vs_fd():
     assert abs(fd - np.sum(G * E)) <= 1e-7 * max(1.0, abs(fd))
 
 
+def from_rfp(orc, tr, ul, n, arf):
+    """Logical lower triangle (float64) of an RFP array."""
+    dense = orc.stfttr(tr, ul, n, np.asarray(arf, np.float64))
+    return np.tril(dense.T if ul == 1 else dense)
+
+
+def run_adjoint(orc, hostsim, tr, ul, L, Lbar):
+    n = L.shape[0]
+    G = to_rfp(orc, tr, ul, Lbar)
+    calls = ctypes.c_long(0)
+    assert hostsim.hs_spftrf_backward(tr, 1 - ul, n, fp(to_rfp(orc, tr, ul, L)), fp(G), 0,
+                                      ctypes.byref(calls)) == 0
+    return from_rfp(orc, tr, ul, n, G), calls.value
+
+
 @pytest.mark.parametrize("n", [1, 2, 3, 5, 8, 17, 64, 65, 130, 257])
 @pytest.mark.parametrize("tr,ul", VARIANTS)
 def test_spftrf_backward_host(orc, hostsim, n, tr, ul):
+    """The blocked in-place RFP adjoint (tiles of 64, panel steps between
+    them) against the closed form."""
     rng = np.random.default_rng(1000 + 8 * n + 2 * tr + ul)
     L = np.linalg.cholesky(spd(rng, n)).astype(np.float32).astype(np.float64)
     Lbar = np.tril(rng.standard_normal((n, n))).astype(np.float32).astype(np.float64)
-    S = np.zeros((n, n), np.float32)
-    assert hostsim.hs_spftrf_backward(tr, 1 - ul, n, fp(to_rfp(orc, tr, ul, L)),
-                                      fp(to_rfp(orc, tr, ul, Lbar)), fp(S), 0) == 0
-    G = np.tril(S.astype(np.float64))
-    G[np.diag_indices_from(G)] *= 0.5
+    G, _ = run_adjoint(orc, hostsim, tr, ul, L, Lbar)
     Ge = chol_adjoint_stored(L, Lbar)
     assert np.linalg.norm(G - Ge) <= 2e-5 * np.linalg.norm(Ge)
 
 
-@pytest.mark.parametrize("tr,ul", [(0, 0), (1, 1)])
+@pytest.mark.parametrize("tr,ul", [(0, 0), (1, 1), (0, 1), (1, 0)])
 def test_spftrf_backward_host_recursive(orc, hostsim, tr, ul):
-    """n above the solve leaf: the lower-triangle-only solve recurses."""
+    """n well above the tile: several levels of panel steps, each with its
+    solve and masked two-product update."""
     n = 600
     rng = np.random.default_rng(5 + tr + ul)
     L = np.linalg.cholesky(spd(rng, n)).astype(np.float32).astype(np.float64)
     Lbar = np.tril(rng.standard_normal((n, n))).astype(np.float32).astype(np.float64)
-    S = np.zeros((n, n), np.float32)
-    assert hostsim.hs_spftrf_backward(tr, 1 - ul, n, fp(to_rfp(orc, tr, ul, L)),
-                                      fp(to_rfp(orc, tr, ul, Lbar)), fp(S), 0) == 0
-    G = np.tril(S.astype(np.float64))
-    G[np.diag_indices_from(G)] *= 0.5
+    G, calls = run_adjoint(orc, hostsim, tr, ul, L, Lbar)
     Ge = chol_adjoint_stored(L, Lbar)
+    assert calls > 0
     assert np.linalg.norm(G - Ge) <= 2e-5 * np.linalg.norm(Ge)
-
 
 def test_ssfrk_adjoint_formula_vs_fd(orc):
     """<Cbar, ssfrk(A)> over stored elements, differentiated w.r.t. A."""

@@ -11,7 +11,8 @@ import pytest
 
 from conftest import VARIANTS
 
-OPS = {"ssfrk": 0, "spftrf": 1, "spftrs": 2, "spftri": 3, "trsm_n": 4, "trsm_t": 5, "trtri": 6}
+OPS = {"ssfrk": 0, "spftrf": 1, "spftrs": 2, "spftri": 3, "trsm_n": 4, "trsm_t": 5, "trtri": 6,
+       "adjoint": 7, "ssfr2k": 8}
 
 
 def bounds(hs, op, tr, ul, n, k, math):
@@ -26,7 +27,7 @@ def bounds(hs, op, tr, ul, n, k, math):
 @pytest.mark.parametrize("tr,ul", VARIANTS)
 @pytest.mark.parametrize("op", list(OPS))
 def test_views_in_bounds_large_n(hostsim, op, tr, ul, n, k):
-    for math in ((0, 1) if op in ("spftrf", "ssfrk", "trtri") else (0,)):
+    for math in ((0, 1) if op in ("spftrf", "ssfrk", "trtri", "adjoint", "ssfr2k") else (0,)):
         rc, (calls, checks, bad), msg = bounds(hostsim, op, tr, ul, n, k, math)
         assert rc == 0, (rc, msg)
         assert calls > 0 and checks > 0

@@ -96,3 +96,38 @@ def test_next_ops_vs_reference_build(curfp):
         a, b = o["spfcon"]["rcond_ours"], o["spfcon"]["rcond_reference"]
         assert abs(a - b) <= 1e-3 * abs(b), (a, b)
     torch.cuda.empty_cache()
+
+
+@pytest.mark.gpu
+def test_c5_cholesky_adjoint_in_rfp(curfp):
+    """curfpSpftrfBackward at n = 131072 (34.4 GB per RFP array): the factor
+    and the cotangent (updated in place) are the only n-squared arrays.  With
+    Lbar = L (f = 1/2 tr A) the result is 1/2 on the diagonal and 0
+    elsewhere: max |Abar - 1/2 I| <= 1e-4."""
+    import ctypes
+    n, k, lam = 131072, 4096, 1e-2
+    A = S.gen_A(n, k, seed=131072)
+    L = torch.empty(n * (n + 1) // 2, device="cuda")
+    curfp.ssfrk(A, L)
+    del A
+    curfp.add_to_diagonal(L, lam)
+    assert curfp.spftrf(L) == 0
+    G = L.clone()
+    h = curfp._get_handle()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    st = h._lib.curfpSpftrfBackward(h.ptr, 1, 1, n, ctypes.c_void_p(L.data_ptr()),
+                                    ctypes.c_void_p(G.data_ptr()), ctypes.c_void_p(G.data_ptr()), 1)
+    e1.record()
+    torch.cuda.synchronize()
+    assert st == 0, st
+    d = curfp.rfp_diag_indices(n)
+    G[d] -= 0.5
+    err = G.abs().max().item()
+    S.emit({"config": "C5-adjoint", "n": n, "k": k, "lambda": lam,
+            "spftrf_backward_ms": round(e0.elapsed_time(e1), 1), "max_abs_err_vs_half_I": err,
+            "peak_mem_gb": round(torch.cuda.max_memory_allocated() / 1e9, 1)})
+    del L, G
+    torch.cuda.empty_cache()
+    assert err <= 1e-4, err
