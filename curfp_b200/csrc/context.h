@@ -79,6 +79,12 @@ void* grow_buffer(curfpContext* ctx, void** buf, size_t* cur, size_t bytes);
 // (brows x k) FP32 views; B.p == nullptr means B is A.
 int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, View B,
                 int brows, int k, const SharedTask* tasks, int count);
+// The same with triangular operand masks (0 full, 1 keep column <= row,
+// 2 keep column >= row, columns counted over the whole k range): masked
+// elements are staged as zeros and never read.  B.p must be set.
+int tc_contract_masked(curfpContext* ctx, const int* abort_flag, View A, int arows, int amask,
+                       View B, int brows, int bmask, int k, const SharedTask* tasks,
+                       int count);
 // The wavefront solve with a caller-provided flag buffer of sync_words words
 // (cleared here on the stream); no allocation.
 int launch_trsm_wave_fixed(curfpContext* ctx, const int* abort_flag, View L, int n, View B,

@@ -118,15 +118,17 @@ int launch_skinny(const GemmProbT<T>& g0, const int* abort_flag, curfpContext* c
 // Output written through a column-contiguous view keeps the tensor-core
 // epilogue's warp-wide stores coalesced: C = A B^T is computed as
 // C^T = B A^T when C's contiguous dimension is its column index.
-static void orient(View& A, int& arows, View& B, int& brows, SharedTask& t) {
+// Returns whether it swapped the operands.
+static bool orient(View& A, int& arows, View& B, int& brows, SharedTask& t) {
   const bool col_contig = (t.C.cs == 1 || t.C.cs == -1) && !(t.C.rs == 1 || t.C.rs == -1);
-  if (!col_contig) return;
+  if (!col_contig) return false;
   View tv = A; A = B; B = tv;
   int tr_ = arows; arows = brows; brows = tr_;
   int x = t.a_row0; t.a_row0 = t.b_row0; t.b_row0 = x;
   x = t.m; t.m = t.n; t.n = x;
   t.C = tr(t.C);
   t.c_lower = t.c_lower ? 2 : 0;  // 2 = upper mask after transposition
+  return true;
 }
 
 template <>
@@ -215,14 +217,29 @@ int CudaExecT<float>::gemm(const GemmProb* p, int count) {
     const int rc = launch_skinny<float>(p[0], abort_, ctx_);
     if (rc >= 0) return rc;
   }
-  if (count == 1 && p[0].math && !p[0].inplace && !p[0].a_tri && !p[0].b_tri && p[0].k2 == 0 &&
-      tc_worthwhile(p[0].m, p[0].n, p[0].k)) {
+  // One problem, one or two products, on the tensor cores: the A operands
+  // may be triangular (lower / upper, staged with zeros), the B operands
+  // full; the second product accumulates with beta = 1.
+  if (count == 1 && p[0].math && !p[0].inplace && p[0].b_tri == 0 && p[0].b2_tri == 0 &&
+      p[0].a_tri <= 2 && p[0].a2_tri <= 2 && tc_worthwhile(p[0].m, p[0].n, p[0].k) &&
+      (p[0].k2 == 0 || tc_worthwhile(p[0].m, p[0].n, p[0].k2))) {
     const GemmProb& g = p[0];
-    View A = g.A, Bt = tr(g.B);  // A: m x k, Bt: n x k
-    int ar = g.m, br = g.n;
-    SharedTask t{0, 0, g.m, g.n, g.C, g.alpha, g.beta, g.c_lower};
-    orient(A, ar, Bt, br, t);
-    return tc_contract(ctx_, abort_, A, ar, Bt, br, g.k, &t, 1);
+    for (int prod = 0; prod < (g.k2 ? 2 : 1); ++prod) {
+      View A = prod ? g.A2 : g.A, Bt = tr(prod ? g.B2 : g.B);  // A: m x k, Bt: n x k
+      int ar = g.m, br = g.n;
+      int amask = prod ? g.a2_tri : g.a_tri, bmask = 0;
+      SharedTask t{0, 0, g.m, g.n, g.C, g.alpha, prod ? 1.0f : g.beta, g.c_lower};
+      if (orient(A, ar, Bt, br, t)) {  // operands swapped: the mask moves with A
+        bmask = amask;
+        amask = 0;
+      }
+      const int rc = (amask || bmask)
+                         ? tc_contract_masked(ctx_, abort_, A, ar, amask, Bt, br, bmask,
+                                              prod ? g.k2 : g.k, &t, 1)
+                         : tc_contract(ctx_, abort_, A, ar, Bt, br, prod ? g.k2 : g.k, &t, 1);
+      if (rc) return rc;
+    }
+    return 0;
   }
   // Tile choice: 128 x 128 when it fills the machine, else 64 x 64.
   int64_t t128 = 0;

@@ -429,8 +429,18 @@ __global__ void __launch_bounds__(THREADS, 1)
 // s_i >= max_k |X_ik| (1 for an all-zero row), for rows < rows_pad (padding
 // rows get 1).  One block of 256 threads per 32 rows; the warp runs along
 // the contiguous dimension of X.
+// Triangular operand mask of the staging kernels: element (r, c) of the
+// staged operand (c counted from column koff of the full operand) is kept
+// when mask == 0, when mask == 1 and c + koff <= r (lower, diagonal
+// included), or when mask == 2 and c + koff >= r (upper, diagonal
+// included); masked elements are staged as zeros and never read.
+__device__ __forceinline__ bool keep_elem(int mask, int r, int c, int koff) {
+  return mask == 0 || (mask == 1 ? c + koff <= r : c + koff >= r);
+}
+
 __global__ void __launch_bounds__(256) rowscale_kernel(View X, int rows, int k,
-                                                       float* scale, int rows_pad) {
+                                                       float* scale, int rows_pad, int mask,
+                                                       int koff) {
   __shared__ float red[8][33];
   const int r0 = blockIdx.x * 32;
   const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
@@ -449,7 +459,7 @@ __global__ void __launch_bounds__(256) rowscale_kernel(View X, int rows, int k,
 #pragma unroll
           for (int u = 0; u < 8; ++u) {
             const int cc = c + 32 * u;
-            v[u] = cc < k ? fabsf(row[(int64_t)cc * X.cs]) : 0.f;
+            v[u] = (cc < k && keep_elem(mask, r, cc, koff)) ? fabsf(row[(int64_t)cc * X.cs]) : 0.f;
           }
 #pragma unroll
           for (int u = 0; u < 8; ++u) m[j] = fmaxf(m[j], v[u]);
@@ -473,7 +483,7 @@ __global__ void __launch_bounds__(256) rowscale_kernel(View X, int rows, int k,
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
           const int cc = c + 8 * u;
-          v[u] = cc < k ? fabsf(row[(int64_t)cc * X.cs]) : 0.f;
+          v[u] = (cc < k && keep_elem(mask, r, cc, koff)) ? fabsf(row[(int64_t)cc * X.cs]) : 0.f;
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u) m[0] = fmaxf(m[0], v[u]);
@@ -509,7 +519,8 @@ __global__ void __launch_bounds__(256) rowscale_kernel(View X, int rows, int k,
 __global__ void __launch_bounds__(256) digits_kernel(View X, int rows, int k,
                                                      const float* __restrict__ scale,
                                                      __nv_bfloat16* out, int rows_pad,
-                                                     int k_pad, int nplanes) {
+                                                     int k_pad, int nplanes, int mask,
+                                                     int koff) {
   __shared__ float t[32][65];
   const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 64;
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -520,7 +531,9 @@ __global__ void __launch_bounds__(256) digits_kernel(View X, int rows, int k,
     if (kcont) { lc = tx + 32 * (r & 1); lr = ty + 8 * (r >> 1); }
     else       { lr = tx; lc = ty + 8 * r; }
     const int gr = r0 + lr, gc = c0 + lc;
-    t[lr][lc] = (gr < rows && gc < k) ? X.p[(int64_t)gr * X.rs + (int64_t)gc * X.cs] : 0.f;
+    t[lr][lc] = (gr < rows && gc < k && keep_elem(mask, gr, gc, koff))
+                    ? X.p[(int64_t)gr * X.rs + (int64_t)gc * X.cs]
+                    : 0.f;
   }
   __syncthreads();
   const int64_t plane = (int64_t)rows_pad * k_pad;

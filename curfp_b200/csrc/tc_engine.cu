@@ -49,7 +49,7 @@ struct Staged {
 // Stage X (rows x k) as row scales + `planes` BF16 digit planes in a context
 // staging buffer (two kernels: row maxima, then digits).
 int stage(curfpContext* ctx, void** buf, size_t* cur, View X, int rows, int k, int planes,
-          Staged* out) {
+          int mask, int koff, Staged* out) {
   out->rows_pad = (int)(round_up(rows, ktc::BN) + ktc::BN);
   out->k_pad = (int)round_up(k, 64);
   out->planes = planes;
@@ -63,10 +63,11 @@ int stage(curfpContext* ctx, void** buf, size_t* cur, View X, int rows, int k, i
   ProfScope ps(ctx->prof, ctx->stream, K_TC_STAGE, 0,
                (double)rows * k * 8.0 + (double)out->rows_pad * out->k_pad * 2.0 * planes);
   ktc::rowscale_kernel<<<out->rows_pad / 32, 256, 0, ctx->stream>>>(X, rows, k, out->scale,
-                                                                   out->rows_pad);
+                                                                   out->rows_pad, mask, koff);
   dim3 grid(out->k_pad / 64, out->rows_pad / 32);
   ktc::digits_kernel<<<grid, dim3(32, 8), 0, ctx->stream>>>(X, rows, k, out->scale, out->p,
-                                                            out->rows_pad, out->k_pad, planes);
+                                                            out->rows_pad, out->k_pad, planes,
+                                                            mask, koff);
   ctx->launches += 2;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
@@ -92,16 +93,17 @@ bool tc_worthwhile(int m, int n, int k) {
 
 namespace {
 
-int tc_slab(curfpContext* ctx, const int* abort_flag, View A, int arows, View B, int brows,
-            int k, const SharedTask* tasks, int count) {
+int tc_slab(curfpContext* ctx, const int* abort_flag, View A, int arows, int amask, View B,
+            int brows, int bmask, int k, int koff, const SharedTask* tasks, int count) {
   // The A side reads planes h, m, l'; the B side also m'.  A shared operand
   // is staged once with all four.
   Staged sa, sb;
   int rc = stage(ctx, &ctx->stage, &ctx->stage_bytes, A, arows, k,
-                 B.p ? ktc::PLANES_A : ktc::PLANES, &sa);
+                 B.p ? ktc::PLANES_A : ktc::PLANES, amask, koff, &sa);
   if (rc) return rc;
   if (B.p) {
-    if ((rc = stage(ctx, &ctx->stage2, &ctx->stage2_bytes, B, brows, k, ktc::PLANES, &sb)))
+    if ((rc = stage(ctx, &ctx->stage2, &ctx->stage2_bytes, B, brows, k, ktc::PLANES, bmask,
+                    koff, &sb)))
       return rc;
   } else {
     sb = sa;
@@ -165,14 +167,22 @@ int tc_slab(curfpContext* ctx, const int* abort_flag, View A, int arows, View B,
 // planes) at the cost of one extra read-modify-write of C per slab.
 int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, View B,
                 int brows, int k, const SharedTask* tasks, int count) {
+  return tc_contract_masked(ctx, abort_flag, A, arows, 0, B, brows, 0, k, tasks, count);
+}
+
+int tc_contract_masked(curfpContext* ctx, const int* abort_flag, View A, int arows, int amask,
+                       View B, int brows, int bmask, int k, const SharedTask* tasks,
+                       int count) {
   if (count <= 0 || k <= 0) return 0;
+  if (!B.p && amask) return 3;  // a shared operand is staged once, unmasked
   if (count > ktc::MAX_TASKS) return 3;
   const int rows = B.p && brows > arows ? brows : arows;
   const size_t per_k = (size_t)(round_up(rows, ktc::BN) + ktc::BN) * ktc::PLANES *
                        sizeof(__nv_bfloat16);
   int64_t kc = (int64_t)(kStageBudget / per_k) / kStageSlab * kStageSlab;
   if (kc < kStageSlab) kc = kStageSlab;
-  if (kc >= k) return tc_slab(ctx, abort_flag, A, arows, B, brows, k, tasks, count);
+  if (kc >= k)
+    return tc_slab(ctx, abort_flag, A, arows, amask, B, brows, bmask, k, 0, tasks, count);
   const int64_t nslab = (k + kc - 1) / kc;  // balanced slabs
   kc = round_up((k + nslab - 1) / nslab, kStageSlab);
   SharedTask t[ktc::MAX_TASKS];
@@ -181,7 +191,7 @@ int tc_contract(curfpContext* ctx, const int* abort_flag, View A, int arows, Vie
     const int kk = (int)(k - k0 < kc ? k - k0 : kc);
     const View As = sub(A, 0, k0);
     const View Bs = B.p ? sub(B, 0, k0) : B;
-    int rc = tc_slab(ctx, abort_flag, As, arows, Bs, brows, kk, t, count);
+    int rc = tc_slab(ctx, abort_flag, As, arows, amask, Bs, brows, bmask, kk, (int)k0, t, count);
     if (rc) return rc;
     for (int i = 0; i < count; ++i) t[i].beta = 1.0f;
   }
