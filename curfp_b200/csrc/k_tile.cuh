@@ -6,6 +6,7 @@
 #pragma once
 #include <climits>
 #include <cstdint>
+#include <type_traits>
 
 #include "engine.h"
 
@@ -100,6 +101,10 @@ __global__ void __launch_bounds__(256) potrf_tile(ViewT<E> L, int n, int info_ba
   E* dyn = reinterpret_cast<E*>(dyn_raw);
   E (*s)[PLD] = reinterpret_cast<E (*)[PLD]>(dyn);
   E* rdiag = dyn + PT * PLD;           // 32 reciprocals of the current diagonal block
+  E* col = rdiag + 32;                 // the current column of the diagonal block
+  // 16-byte vectors of E (the two 32-element buffers are 16-byte aligned)
+  using Vec = typename std::conditional<sizeof(E) == 4, float4, double2>::type;
+  constexpr int VW = 16 / (int)sizeof(E);
   __shared__ int fail_sh;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   load_lower<PLD>(L, n, dyn);
@@ -128,9 +133,19 @@ __global__ void __launch_bounds__(256) potrf_tile(ViewT<E> L, int n, int info_ba
         const E r = rsqrt_nr(d);
         a[j] = (lane == j) ? d * r : (lane > j ? a[j] * r : a[j]);
         if (lane == j) rdiag[j] = r;
+        // the scaled column goes through shared memory once and comes back
+        // as 16-byte broadcast reads (instead of one shuffle per row)
+        col[lane] = a[j];
+        __syncwarp();
         E lk[32];
 #pragma unroll
-        for (int k = j + 1; k < 32; ++k) lk[k] = __shfl_sync(0xffffffffu, a[j], k);
+        for (int k4 = (j + 1) / VW; k4 < 32 / VW; ++k4) {
+          const Vec v = reinterpret_cast<const Vec*>(col)[k4];
+          const E* pv = reinterpret_cast<const E*>(&v);
+#pragma unroll
+          for (int t = 0; t < VW; ++t) lk[VW * k4 + t] = pv[t];
+        }
+        __syncwarp();
 #pragma unroll
         for (int k = j + 1; k < 32; ++k)
           if (lane >= k) a[k] = fma(-a[j], lk[k], a[k]);

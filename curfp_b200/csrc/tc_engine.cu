@@ -91,6 +91,12 @@ bool tc_worthwhile(int m, int n, int k) {
   return m >= 128 && n >= 128 && k >= 128 && (double)m * n * k >= 6.7e7;
 }
 
+bool tc_single_slab(int rows, int k) {
+  const size_t per_k = (size_t)(round_up(rows, ktc::BN) + ktc::BN) * ktc::PLANES *
+                       sizeof(__nv_bfloat16);
+  return (size_t)k * per_k <= kStageBudget;
+}
+
 namespace {
 
 int tc_slab(curfpContext* ctx, const int* abort_flag, View A, int arows, int amask, View B,
