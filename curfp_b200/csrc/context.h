@@ -54,6 +54,9 @@ class CudaExecT : public ExecT<T> {
   ~CudaExecT() override;
   int gemm(const GemmProbT<T>* p, int count) override;
   int potrf_tile(ViewT<T> L, int n, int info_base) override;
+  // 256-row tiles in FP32 (one CTA of 512 threads, 148 KB of shared memory),
+  // 128 in FP64.
+  int potrf_tile_rows() const override { return sizeof(T) == 4 ? 256 : 128; }
   int trtri_blocks(ViewT<T> L, int n, int nb, T* W) override;
   int trtri_tile(ViewT<T> L, int n) override;
   int lauum_tile(ViewT<T> L, int n) override;

@@ -61,7 +61,7 @@ template <typename T>
 using Scalar = typename Id<T>::type;
 
 // Block sizes of the recursive algorithms.
-constexpr int kPotrfTile = 128;  // diagonal Cholesky tiles
+constexpr int kPotrfTile = 128;  // diagonal Cholesky tiles (executors may take larger ones)
 constexpr int kTrsmLeaf = 64;    // TRSM diagonal blocks (inverted, then multiplied)
 // Workspace record per 64-row TRSM block: [W_b | M_b], 64 x 64 each
 // (W_b = inv(L_bb); M_b = W_b L_{b,b-1}, written by executors whose
@@ -83,10 +83,13 @@ class ExecT {
   virtual ~ExecT() {}
   // Independent problems, executed as one launch where possible.
   virtual int gemm(const GemmProbT<T>* p, int count) = 0;
-  // In-place Cholesky of the lower triangle of L (n <= kPotrfTile).  On the
-  // first non-positive (or NaN) pivot at local column j the device info word
-  // becomes min(info, info_base + j + 1) and the tile stops.
+  // In-place Cholesky of the lower triangle of L (n <= potrf_tile_rows()).
+  // On the first non-positive (or NaN) pivot at local column j the device
+  // info word becomes min(info, info_base + j + 1) and the tile stops.
   virtual int potrf_tile(ViewT<T> L, int n, int info_base) = 0;
+  // Largest diagonal tile potrf_tile takes (a multiple of kPotrfTile); the
+  // recursive Cholesky splits down to it.
+  virtual int potrf_tile_rows() const { return kPotrfTile; }
   // Inverses of the diagonal nb x nb blocks of lower L (n x n): block b is
   // written to W + b*nb*nb, column-major with ld nb, zeros above the diagonal.
   // (W: nblk records of kInvStride floats, see kInvStride)

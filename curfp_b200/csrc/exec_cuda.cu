@@ -281,16 +281,27 @@ int CudaExecT<T>::potrf_adj_tile(ViewT<T> L, ViewT<T> G, int n) {
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
+namespace {
+template <typename T, int NT, int THR>
+int launch_potrf(curfpContext* ctx, ViewT<T> L, int n, int info_base) {
+  constexpr int smem = ktile::potrf_smem<T, NT>();
+  static const bool attr = smem_attr(ktile::potrf_tile<T, NT, THR>, smem);
+  if (!attr) return 4;
+  ktile::potrf_tile<T, NT, THR><<<1, THR, smem, ctx->stream>>>(L, n, info_base, ctx->d_info);
+  ++ctx->launches;
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+}  // namespace
+
 template <typename T>
 int CudaExecT<T>::potrf_tile(ViewT<T> L, int n, int info_base) {
   if (n <= 0) return 0;
+  if (n > potrf_tile_rows()) return 3;
   ProfScope ps(ctx_->prof, ctx_->stream, K_POTRF, (double)n * n * n / 3.0, 0);
-  constexpr int smem = ktile::potrf_smem<T>();
-  static const bool attr = smem_attr(ktile::potrf_tile<T>, smem);
-  if (!attr) return 4;
-  ktile::potrf_tile<T><<<1, 256, smem, ctx_->stream>>>(L, n, info_base, ctx_->d_info);
-  ++ctx_->launches;
-  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+  if (n <= ktile::PT) return launch_potrf<T, ktile::PT, 256>(ctx_, L, n, info_base);
+  if constexpr (sizeof(T) == 4)
+    return launch_potrf<T, ktile::PT_BIG, 512>(ctx_, L, n, info_base);
+  return 3;
 }
 
 template <typename T>

@@ -65,23 +65,41 @@ constexpr int LD = T + 1;    // padded shared-memory leading dimension
 
 static_assert(T == kTrsmLeaf && T == kTriTile, "tile kernels assume one tile size");
 
-// Lower-triangular Cholesky of an n x n tile (n <= 128), one CTA of 256
-// threads, the tile in shared memory.  Blocked by 32 columns:
-//   (1) warp 0 factors the 32 x 32 diagonal block in registers (lane = row,
-//       pivots broadcast with warp shuffles, warp-uniform control flow, no
-//       block barrier inside);
+// Lower-triangular Cholesky of an n x n tile (n <= NT, NT = 128 or 256), one
+// CTA of THR threads, the tile's lower triangle in shared memory.  Blocked
+// by 32 columns:
+//   (1) warp 0 factors the 32 x 32 diagonal block in registers (lane = row;
+//       each column is broadcast through shared memory as 16-byte reads;
+//       warp-uniform control flow, no block barrier inside);
 //   (2) the rows below solve against it (one thread per row, forward
 //       substitution with broadcast reads of the factor);
-//   (3) all threads apply the rank-32 update to the trailing triangle.
+//   (3) all threads apply the rank-32 update to the trailing triangle in
+//       4 x 4 register blocks.
+// Shared-memory layout, panel-blocked: panel p (columns 32p .. 32p+31) holds
+// rows 32p .. NT-1 with a row stride of 33, so consecutive rows of a column
+// fall in consecutive banks and only the lower triangle is stored (NT = 256
+// in FP32: 148 KB).
 // On a pivot that is not > 0 (or NaN) the device info word becomes
 // min(info, info_base + column + 1), the partially factored tile is written
 // back and the kernel returns (LAPACK xPOTRF semantics).
-constexpr int PT = 128;          // potrf tile (== kPotrfTile)
-constexpr int PLD = PT + 1;
-template <typename E>
-constexpr int potrf_smem() { return (PT * PLD + 64) * (int)sizeof(E); }
-constexpr int POTRF_SMEM = potrf_smem<float>();
+constexpr int PT = 128;           // potrf tile of the FP64 executor and the CPU planner tests
+constexpr int PT_BIG = 256;       // potrf tile of the FP32 executor
+constexpr int PLDP = 33;          // row stride inside a panel
+template <int NT>
+__host__ __device__ constexpr int panel_off(int p) {
+  return PLDP * (p * NT - 16 * p * (p - 1));
+}
+template <int NT>
+__device__ __forceinline__ int pidx(int i, int j) {
+  const int p = j >> 5;
+  return panel_off<NT>(p) + (i - 32 * p) * PLDP + (j & 31);
+}
+template <typename E, int NT>
+constexpr int potrf_smem() { return (panel_off<NT>(NT / 32) + 64) * (int)sizeof(E); }
+constexpr int POTRF_SMEM = potrf_smem<float, PT>();
 static_assert(PT == kPotrfTile, "potrf tile size");
+template <typename E>
+constexpr int potrf_threads(int nt) { return nt == PT_BIG ? 512 : 256; }
 
 // 1/sqrt(d): the hardware estimate refined by one Newton-Raphson step for
 // y = x^-1/2 (y <- y (3 - d y^2) / 2).
@@ -94,33 +112,53 @@ __device__ __forceinline__ double rsqrt_nr(double d) {
   return r * fma(-0.5 * d * r, r, 1.5);
 }
 
-template <typename E>
-__global__ void __launch_bounds__(256) potrf_tile(ViewT<E> L, int n, int info_base, int* info) {
+template <typename E, int NT, int THR>
+__global__ void __launch_bounds__(THR) potrf_tile(ViewT<E> L, int n, int info_base, int* info) {
   if (info && *info != INT_MAX) return;
   extern __shared__ __align__(16) unsigned char dyn_raw[];
-  E* dyn = reinterpret_cast<E*>(dyn_raw);
-  E (*s)[PLD] = reinterpret_cast<E (*)[PLD]>(dyn);
-  E* rdiag = dyn + PT * PLD;           // 32 reciprocals of the current diagonal block
-  E* col = rdiag + 32;                 // the current column of the diagonal block
+  E* s = reinterpret_cast<E*>(dyn_raw);
+  E* rdiag = s + panel_off<NT>(NT / 32);  // 32 reciprocals of the current diagonal block
+  E* col = rdiag + 32;                     // the current column of the diagonal block
   // 16-byte vectors of E (the two 32-element buffers are 16-byte aligned)
   using Vec = typename std::conditional<sizeof(E) == 4, float4, double2>::type;
   constexpr int VW = 16 / (int)sizeof(E);
+  static_assert((panel_off<NT>(NT / 32) * (int)sizeof(E)) % 16 == 0, "buffer alignment");
   __shared__ int fail_sh;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  load_lower<PLD>(L, n, dyn);
+  constexpr int NW = THR / 32;
+  // Load the lower triangle; the warp runs along the view's contiguous
+  // dimension with NT / 32 loads in flight per lane.
+  {
+    const bool rcont = (L.cs == 1 || L.cs == -1);
+    for (int a = warp; a < n; a += NW) {
+      E v[NT / 32];
+#pragma unroll
+      for (int q = 0; q < NT / 32; ++q) {
+        const int b = lane + 32 * q;
+        const int i = rcont ? a : b, j = rcont ? b : a;
+        v[q] = (b < n && i >= j) ? L.p[(int64_t)i * L.rs + (int64_t)j * L.cs] : E(0);
+      }
+#pragma unroll
+      for (int q = 0; q < NT / 32; ++q) {
+        const int b = lane + 32 * q;
+        const int i = rcont ? a : b, j = rcont ? b : a;
+        if (b < n && i >= j) s[pidx<NT>(i, j)] = v[q];
+      }
+    }
+  }
   if (tid == 0) fail_sh = 0;
   __syncthreads();
   for (int c0 = 0; c0 < n; c0 += 32) {
     const int w = min(32, n - c0);
+    const int pb = panel_off<NT>(c0 >> 5);  // this panel's base; row r at pb + (r - c0) * 33
     // (1) diagonal block in registers
     if (warp == 0) {
       E a[32];
 #pragma unroll
-      for (int k = 0; k < 32; ++k) a[k] = (lane < w && k < w) ? s[c0 + lane][c0 + k] : E(0);
+      for (int k = 0; k < 32; ++k) a[k] = (lane < w && k < w) ? s[pb + lane * PLDP + k] : E(0);
       int fail = 0;
       // The exit tests are warp-uniform (w is, and the pivot test goes
-      // through a vote), so the loop body runs without divergence handling;
-      // the shuffles of one step are issued together before their FMAs.
+      // through a vote), so the loop body runs without divergence handling.
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
         if (j >= w) break;
@@ -153,7 +191,7 @@ __global__ void __launch_bounds__(256) potrf_tile(ViewT<E> L, int n, int info_ba
       if (lane < w) {
 #pragma unroll
         for (int k = 0; k < 32; ++k)
-          if (k <= lane && k < w) s[c0 + lane][c0 + k] = a[k];
+          if (k <= lane && k < w) s[pb + lane * PLDP + k] = a[k];
       }
       if (lane == 0 && fail) fail_sh = fail;
     }
@@ -161,14 +199,15 @@ __global__ void __launch_bounds__(256) potrf_tile(ViewT<E> L, int n, int info_ba
     if (fail_sh) break;
     const int r1 = c0 + w;
     // (2) rows below: X L_blk^T = A_r
-    for (int r = r1 + tid; r < n; r += 256) {
+    for (int r = r1 + tid; r < n; r += THR) {
       E x[32];
+      E* row = s + pb + (r - c0) * PLDP;
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
         if (j < w) {
-          E v = s[r][c0 + j];
+          E v = row[j];
 #pragma unroll
-          for (int k = 0; k < j; ++k) v = fma(-x[k], s[c0 + j][c0 + k], v);
+          for (int k = 0; k < j; ++k) v = fma(-x[k], s[pb + j * PLDP + k], v);
           x[j] = v * rdiag[j];
         } else {
           x[j] = E(0);
@@ -176,31 +215,41 @@ __global__ void __launch_bounds__(256) potrf_tile(ViewT<E> L, int n, int info_ba
       }
 #pragma unroll
       for (int j = 0; j < 32; ++j)
-        if (j < w) s[r][c0 + j] = x[j];
+        if (j < w) row[j] = x[j];
     }
     __syncthreads();
     // (3) trailing update of the lower triangle rows/cols >= r1, in 4 x 4
-    // register blocks (16 independent accumulators per thread)
+    // register blocks (16 independent accumulators per thread); r1 is a
+    // multiple of 32 here, so a block's 4 columns share one panel.
     const int m = n - r1, nb4 = (m + 3) / 4, nblk4 = nb4 * (nb4 + 1) / 2;
-    for (int e = tid; e < nblk4; e += 256) {
+    for (int e = tid; e < nblk4; e += THR) {
       int bi = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
       while ((bi + 1) * (bi + 2) / 2 <= e) ++bi;
       while (bi * (bi + 1) / 2 > e) --bi;
       const int bj = e - bi * (bi + 1) / 2;
       const int ri = r1 + 4 * bi, cj = r1 + 4 * bj;
+      const int pc = panel_off<NT>(cj >> 5) + (cj & 31);  // + (row - 32*(cj>>5)) * 33
+      const int prow0 = 32 * (cj >> 5);
       E acc[4][4];
 #pragma unroll
       for (int p = 0; p < 4; ++p)
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-          acc[p][q] = (ri + p < n && cj + q < n) ? s[ri + p][cj + q] : E(0);
+          acc[p][q] = (ri + p < n && cj + q <= ri + p) ? s[pc + (ri + p - prow0) * PLDP + q] : E(0);
+      const E* ar[4];
+      const E* br[4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        ar[p] = s + pb + (min(ri + p, n - 1) - c0) * PLDP;
+        br[p] = s + pb + (min(cj + p, n - 1) - c0) * PLDP;
+      }
 #pragma unroll 4
       for (int k = 0; k < w; ++k) {
         E a4[4], b4[4];
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
-          a4[p] = (ri + p < n) ? s[ri + p][c0 + k] : E(0);
-          b4[p] = (cj + p < n) ? s[cj + p][c0 + k] : E(0);
+          a4[p] = ar[p][k];
+          b4[p] = br[p][k];
         }
 #pragma unroll
         for (int p = 0; p < 4; ++p)
@@ -211,12 +260,23 @@ __global__ void __launch_bounds__(256) potrf_tile(ViewT<E> L, int n, int info_ba
       for (int p = 0; p < 4; ++p)
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-          if (ri + p < n && cj + q <= ri + p) s[ri + p][cj + q] = acc[p][q];
+          if (ri + p < n && cj + q <= ri + p) s[pc + (ri + p - prow0) * PLDP + q] = acc[p][q];
     }
     __syncthreads();
   }
   if (fail_sh && tid == 0) atomicMin(info, info_base + fail_sh);
-  store_lower<PLD>(L, n, dyn);
+  // Store the lower triangle back (same thread mapping as the load).
+  {
+    const bool rcont = (L.cs == 1 || L.cs == -1);
+    for (int a = warp; a < n; a += NW) {
+#pragma unroll
+      for (int q = 0; q < NT / 32; ++q) {
+        const int b = lane + 32 * q;
+        const int i = rcont ? a : b, j = rcont ? b : a;
+        if (b < n && i >= j) L.p[(int64_t)i * L.rs + (int64_t)j * L.cs] = s[pidx<NT>(i, j)];
+      }
+    }
+  }
 }
 
 // Inverse of lower-triangular diagonal blocks.  Block b = blockIdx.x covers

@@ -137,8 +137,9 @@ int trmm(ExecT<T>& ex, int left, int lower, int trans, ViewT<T> Tm, ViewT<T> B, 
 template <typename T>
 int potrf_lower(ExecT<T>& ex, ViewT<T> A, int n, int info_base, int math) {
   if (n <= 0) return 0;
-  if (n <= kPotrfTile) return ex.potrf_tile(A, n, info_base);
-  int n1 = split(n, kPotrfTile), n2 = n - n1;
+  const int tile = ex.potrf_tile_rows();
+  if (n <= tile) return ex.potrf_tile(A, n, info_base);
+  int n1 = split(n, tile), n2 = n - n1;
   int rc = potrf_lower(ex, A, n1, info_base, math);
   if (rc) return rc;
   ViewT<T> A21 = sub(A, n1, 0);
