@@ -28,35 +28,20 @@ against ``torch.linalg.cholesky`` in FP64).
 
 ``math`` ("fp32" or "bf16x3") selects the contraction arithmetic of the
 factorization and of the Cholesky adjoint's triangular solves.
+
+Every library call goes through the torch extension (torch.ops.curfp_b200.*,
+curfp_b200/csrc_torch/torch_ops.cpp), on torch's current stream: the autograd
+engine runs a backward on the stream of its forward.
 """
 from __future__ import annotations
 
-import contextlib
-import ctypes
-
 import torch
 
-from . import _fill, _get_handle, _n_from_rfp, _op, _ptr, rfp_diag_indices
-from ._lib import check
+from . import _fill, _n_from_rfp, _op, rfp_diag_indices
+from ._torch_ops import ops
 from .precision import _math
 
 __all__ = ["ssfrk", "add_to_diagonal", "cholesky", "solve", "log_diag_sum", "nll"]
-
-
-@contextlib.contextmanager
-def _stream_handle():
-    """The library handle, bound to torch's current stream for the call (the
-    autograd engine runs a backward on the stream of its forward)."""
-    h = _get_handle()
-    old = h.get_stream_ptr()
-    cur = torch.cuda.current_stream().cuda_stream
-    if cur != old:
-        h.set_stream_ptr(cur)
-    try:
-        yield h
-    finally:
-        if cur != old:
-            h.set_stream_ptr(old)
 
 
 def _check_rfp(t: torch.Tensor, name: str) -> int:
@@ -89,11 +74,7 @@ class _Ssfrk(torch.autograd.Function):
         n, k = A.shape
         a = _scalar(alpha)
         C = torch.empty(n * (n + 1) // 2, device=A.device, dtype=torch.float32)
-        with _stream_handle() as h:
-            check(h._lib.curfpSsfrkEx(h.ptr, _op(transr), _fill(uplo), 1, n, k,
-                                      ctypes.byref(ctypes.c_float(a)), _ptr(A), max(k, 1),
-                                      ctypes.byref(ctypes.c_float(0.0)), _ptr(C),
-                                      _math(math)))
+        ops().ssfrk(A, C, a, 0.0, _op(transr), _fill(uplo), 1, n, k, max(k, 1), _math(math))
         ctx.save_for_backward(A)
         ctx.alpha, ctx.transr, ctx.uplo = a, transr, uplo
         ctx.alpha_is_tensor = torch.is_tensor(alpha)
@@ -109,10 +90,8 @@ class _Ssfrk(torch.autograd.Function):
         n, k = A.shape
         G = torch.empty_like(A)
         scale = 1.0 if need_alpha else ctx.alpha
-        with _stream_handle() as h:
-            check(h._lib.curfpSsfrkBackward(h.ptr, _op(ctx.transr), _fill(ctx.uplo), 1, n, k,
-                                            ctypes.byref(ctypes.c_float(scale)), _ptr(A),
-                                            max(k, 1), _ptr(Cbar), _ptr(G), max(k, 1)))
+        ops().ssfrk_backward(A, Cbar, G, scale, _op(ctx.transr), _fill(ctx.uplo), 1, n, k,
+                             max(k, 1))
         g_alpha = 0.5 * torch.sum(G * A) if need_alpha else None
         g_a = (G * ctx.alpha if need_alpha else G) if need_a else None
         return g_a, g_alpha, None, None, None
@@ -122,10 +101,8 @@ class _AddDiag(torch.autograd.Function):
     @staticmethod
     def forward(ctx, C, value, transr, uplo):
         n = _check_rfp(C, "C")
-        out = C.clone()
-        with _stream_handle() as h:
-            check(h._lib.curfpSaddToDiagonal(h.ptr, _op(transr), _fill(uplo), n,
-                                             ctypes.c_float(_scalar(value)), _ptr(out)))
+        out = C.contiguous().clone()
+        ops().add_to_diagonal(out, _scalar(value), _op(transr), _fill(uplo), n)
         ctx.n, ctx.transr, ctx.uplo = n, transr, uplo
         return out
 
@@ -143,14 +120,11 @@ class _Cholesky(torch.autograd.Function):
     def forward(ctx, C, transr, uplo, math):
         n = _check_rfp(C, "C")
         L = C.contiguous().clone()
-        info = ctypes.c_int(0)
-        with _stream_handle() as h:
-            check(h._lib.curfpSpftrfEx(h.ptr, _op(transr), _fill(uplo), n, _ptr(L),
-                                       ctypes.byref(info), _math(math)))
-        if info.value != 0:
+        info = ops().spftrf(L, _op(transr), _fill(uplo), n, _math(math))
+        if info != 0:
             raise torch.linalg.LinAlgError(
                 f"cholesky: matrix is not positive definite (leading minor of order "
-                f"{info.value} is not positive definite)")
+                f"{info} is not positive definite)")
         ctx.save_for_backward(L)
         ctx.n, ctx.transr, ctx.uplo, ctx.math = n, transr, uplo, math
         return L
@@ -160,10 +134,8 @@ class _Cholesky(torch.autograd.Function):
         (L,) = ctx.saved_tensors
         Lbar = Lbar.contiguous()
         Cbar = torch.empty_like(L)
-        with _stream_handle() as h:
-            check(h._lib.curfpSpftrfBackward(h.ptr, _op(ctx.transr), _fill(ctx.uplo), ctx.n,
-                                             _ptr(L), _ptr(Lbar), _ptr(Cbar),
-                                             _math(ctx.math)))
+        ops().spftrf_backward(L, Lbar, Cbar, _op(ctx.transr), _fill(ctx.uplo), ctx.n,
+                              _math(ctx.math))
         return Cbar, None, None, None
 
 
@@ -181,9 +153,7 @@ class _Solve(torch.autograd.Function):
         # (nrhs, n) row-major == column-major n x nrhs, always a fresh buffer
         # (for nrhs = 1, Bm.t() is already contiguous and would alias B)
         Xf = torch.empty((nrhs, n), device=B.device, dtype=torch.float32).copy_(Bm.t())
-        with _stream_handle() as h:
-            check(h._lib.curfpSpftrs(h.ptr, _op(transr), _fill(uplo), n, nrhs, _ptr(L),
-                                     _ptr(Xf), n))
+        ops().spftrs(L, Xf, _op(transr), _fill(uplo), n, nrhs, n)
         ctx.save_for_backward(L, Xf)
         ctx.n, ctx.transr, ctx.uplo, ctx.vec = n, transr, uplo, vec
         X = Xf.t()
@@ -198,10 +168,8 @@ class _Solve(torch.autograd.Function):
         Bbf = torch.empty((nrhs, n), device=Xbar.device, dtype=torch.float32).copy_(Xbm.t())
         need_l = ctx.needs_input_grad[0]
         Lbar = torch.empty_like(L) if need_l else None
-        with _stream_handle() as h:
-            check(h._lib.curfpSpftrsBackward(h.ptr, _op(ctx.transr), _fill(ctx.uplo), n, nrhs,
-                                             _ptr(L), _ptr(Xf), n, _ptr(Bbf), n, _ptr(Bbf), n,
-                                             _ptr(Lbar)))
+        ops().spftrs_backward(L, Xf, Bbf, Lbar if need_l else L.new_empty(0),
+                              _op(ctx.transr), _fill(ctx.uplo), n, nrhs)
         Bbar = None
         if ctx.needs_input_grad[1]:
             Bbar = Bbf.t()
@@ -220,24 +188,16 @@ class _GpNll(torch.autograd.Function):
         n, d = X.shape
         sv, vv = _scalar(s), _scalar(sigma2)
         C = torch.empty(n * (n + 1) // 2, device=X.device, dtype=torch.float32)
-        info = ctypes.c_int(0)
-        iters = ctypes.c_int(0)
         a = y.detach().clone().contiguous()
-        with _stream_handle() as h:
-            check(h._lib.curfpSsfrkEx(h.ptr, _op(transr), _fill(uplo), 1, n, d,
-                                      ctypes.byref(ctypes.c_float(sv)), _ptr(X), max(d, 1),
-                                      ctypes.byref(ctypes.c_float(0.0)), _ptr(C), _math(math)))
-            check(h._lib.curfpSaddToDiagonal(h.ptr, _op(transr), _fill(uplo), n,
-                                             ctypes.c_float(vv), _ptr(C)))
-            L = C.clone()
-            check(h._lib.curfpSpftrfEx(h.ptr, _op(transr), _fill(uplo), n, _ptr(L),
-                                       ctypes.byref(info), _math(math)))
-            if info.value != 0:
-                raise torch.linalg.LinAlgError(
-                    f"nll: C is not positive definite (leading minor of order {info.value})")
-            check(h._lib.curfpSpftrsRefine(h.ptr, _op(transr), _fill(uplo), n, 1, _ptr(C),
-                                           _ptr(L), _ptr(a), n, int(refine),
-                                           ctypes.byref(iters)))
+        o = ops()
+        o.ssfrk(X, C, sv, 0.0, _op(transr), _fill(uplo), 1, n, d, max(d, 1), _math(math))
+        o.add_to_diagonal(C, vv, _op(transr), _fill(uplo), n)
+        L = C.clone()
+        info = o.spftrf(L, _op(transr), _fill(uplo), n, _math(math))
+        if info != 0:
+            raise torch.linalg.LinAlgError(
+                f"nll: C is not positive definite (leading minor of order {info})")
+        o.spftrs_refine(C, L, a, _op(transr), _fill(uplo), n, 1, n, int(refine))
         del C
         idx = _diag_idx(n, transr, uplo, X.device)
         loss = (0.5 * torch.dot(y.detach().double(), a.double())
@@ -255,11 +215,8 @@ class _GpNll(torch.autograd.Function):
         gx = torch.empty_like(X)
         sums = torch.empty(2, device=X.device, dtype=torch.float64)
         g32 = g.detach().float().contiguous()
-        with _stream_handle() as h:
-            check(h._lib.curfpSgpnllBackward(h.ptr, _op(ctx.transr), _fill(ctx.uplo), n, d,
-                                             ctypes.c_float(ctx.sv), _ptr(L), _ptr(X),
-                                             max(d, 1), _ptr(a), _ptr(g32), _ptr(gx), max(d, 1),
-                                             _ptr(sums), _math(ctx.math)))
+        ops().gpnll_backward(L, X, a, g32, gx, sums, ctx.sv, _op(ctx.transr), _fill(ctx.uplo),
+                             n, d, _math(ctx.math))
         gs = sums[0].float().reshape(ctx.s_shape) if ctx.needs_input_grad[1] else None
         gv = sums[1].float().reshape(ctx.v_shape) if ctx.needs_input_grad[2] else None
         gy = a * g32 if ctx.needs_input_grad[3] else None

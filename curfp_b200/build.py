@@ -81,6 +81,27 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     return LIB
 
 
+TORCH_SRC = PKG / "csrc_torch" / "torch_ops.cpp"
+TORCH_BUILD = PKG / "_torch_build"
+TORCH_EXT = TORCH_BUILD / "curfp_torch_ops.so"
+
+
+def build_torch_ext(verbose: bool = False) -> Path:
+    """The torch extension (torch.ops.curfp_b200.*) over the C ABI, built
+    in-tree next to the library it links (rpath $ORIGIN/..)."""
+    from torch.utils import cpp_extension
+    build()
+    TORCH_BUILD.mkdir(exist_ok=True)
+    cpp_extension.load(
+        name="curfp_torch_ops", sources=[str(TORCH_SRC)],
+        extra_include_paths=[str(ROOT / "include")],
+        extra_cflags=["-O2"],
+        extra_ldflags=[f"-L{PKG}", "-lcurfp_b200", "-Wl,-rpath,'$$ORIGIN/..'"],
+        build_directory=str(TORCH_BUILD), with_cuda=True, is_python_module=False,
+        verbose=verbose)
+    return TORCH_EXT
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
@@ -88,4 +109,5 @@ if __name__ == "__main__":
     a = ap.parse_args()
     build(force=a.force or a.ptxas_v, verbose=True,
           extra=["-Xptxas", "-v"] if a.ptxas_v else None)
+    build_torch_ext()
     sys.exit(0)

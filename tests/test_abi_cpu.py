@@ -52,3 +52,17 @@ def test_python_api_surface():
                  "Handle", "set_stream"]:
         assert callable(getattr(c, name)), name
     assert (c.OP_N, c.OP_T, c.FILL_LOWER, c.FILL_UPPER) == (0, 1, 0, 1)
+
+
+def test_torch_extension_registers_ops():
+    """The torch extension (curfp_b200/csrc_torch/torch_ops.cpp) loads on a
+    machine without a GPU and registers every operator the autograd layer
+    calls."""
+    import torch
+
+    from curfp_b200._torch_ops import ops
+    o = ops()
+    for name in ("ssfrk", "add_to_diagonal", "spftrf", "spftrs", "spftrs_refine",
+                 "ssfrk_backward", "spftrf_backward", "spftrs_backward", "gpnll_backward"):
+        assert hasattr(o, name), name
+        assert "curfp_b200::" + name in str(getattr(o, name).default._schema)
