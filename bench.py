@@ -537,6 +537,9 @@ def run_ours(args, rank, world, local):
     P.profile_enable(True)
     timed_steps(step_head, prep, args.steps, world)
     prof = P.profile_read()
+    if args.dump_records and rank == 0:
+        with open(args.dump_records, "w") as f:
+            json.dump({"steps": args.steps, "records": P.profile_records()}, f)
     P.profile_enable(False)
     kernels = {k_: {"ms_per_step": round(v["ms"] / args.steps, 3),
                     "launches_per_step": v["launches"] // args.steps} for k_, v in prof.items()}
@@ -748,6 +751,8 @@ def main():
     ap.add_argument("--case", choices=CASES, default=None)
     ap.add_argument("--cpu-n", type=int, default=CPU_SAMPLE_N,
                     help="host LAPACK size (cpu_baseline and --impl reference)")
+    ap.add_argument("--dump-records", default=None,
+                    help="write the per-launch records of the profiling pass to this JSON file")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="--impl reference: skip the reference GPU build timing")
     args = ap.parse_args()

@@ -74,6 +74,7 @@ SIGNATURES = {
     "curfpSpftrsBackward": [_h, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _i, _p],
     "curfpSgpnllBackward": [_h, _i, _i, _i, _i, _f, _p, _p, _i, _p, _p, _p, _i, _p, _i],
     "curfpProfileEnable": [_h, _i],
+    "curfpProfileRecords": [_h, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong), _p],
     "curfpProfileRead": [_h, _i, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_d),
                          ctypes.POINTER(ctypes.c_longlong)],
 }

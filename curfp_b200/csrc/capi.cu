@@ -913,6 +913,27 @@ curfpStatus_t curfpProfileRead(curfpHandle_t handle, int kclass, double* ms, dou
   return CURFP_STATUS_SUCCESS;
 }
 
+// Every record since curfpProfileEnable, 8 doubles each: class, device ms,
+// flops, bytes, and the contraction shape (m, n, k, output tiles; zeros when
+// not given).  Writes at most max_records; *count receives the number held.
+curfpStatus_t curfpProfileRecords(curfpHandle_t handle, long long max_records,
+                                  long long* count, double* out) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (!count || (max_records > 0 && !out)) return CURFP_STATUS_INVALID_VALUE;
+  if (cudaStreamSynchronize(handle->stream) != cudaSuccess) return CURFP_STATUS_EXECUTION_FAILED;
+  const auto& recs = handle->prof.recs;
+  *count = (long long)recs.size();
+  for (long long i = 0; i < max_records && i < (long long)recs.size(); ++i) {
+    const auto& r = recs[(size_t)i];
+    float e = 0.f;
+    if (cudaEventElapsedTime(&e, r.e0, r.e1) != cudaSuccess) return CURFP_STATUS_EXECUTION_FAILED;
+    double* o = out + 8 * i;
+    o[0] = r.cls; o[1] = e; o[2] = r.flops; o[3] = r.bytes;
+    o[4] = r.m; o[5] = r.n; o[6] = r.k; o[7] = r.tiles;
+  }
+  return CURFP_STATUS_SUCCESS;
+}
+
 // Number of kernels this handle has launched (diagnostic counter).
 curfpStatus_t curfpGetKernelLaunchCount(curfpHandle_t handle, long long* count) {
   if (!handle) return CURFP_STATUS_NOT_INITIALIZED;

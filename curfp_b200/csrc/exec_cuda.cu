@@ -80,6 +80,7 @@ int launch_gemm(const GemmProbT<T>* p, int count, const int* abort_flag,
   b.total_tiles = tiles;
   b.abort_flag = abort_flag;
   ProfScope ps(ctx->prof, st, K_SGEMM, flops, 0);
+  ps.shape(b.p[0].m, b.p[0].n, b.p[0].k + b.p[0].k2, tiles);
   kgemm::sgemm_batch<T, BM, BN><<<tiles, kgemm::kThreads, 0, st>>>(b);
   ++ctx->launches;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
@@ -363,6 +364,7 @@ int launch_wave(curfpContext* ctx, const int* abort_flag, ViewT<T> L, int n, Vie
   const int smem_launch = nchunk <= 2 ? smem_one : smem;
   ProfScope ps(ctx->prof, ctx->stream, K_TRSV, (double)n * n * m,
                (double)n * n * sizeof(T) / 2.0);
+  ps.shape(n, m, n, nblk * nchunk);
   ktrsv::trsm_wave<T, NC><<<nblk * nchunk, 256, smem_launch, ctx->stream>>>(
       L, n, B, m, alpha, W, sync, ctx->d_info + 1, abort_flag);
   ++ctx->launches;

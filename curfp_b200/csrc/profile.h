@@ -32,6 +32,7 @@ struct ProfRec {
   int cls;
   double flops, bytes;
   cudaEvent_t e0, e1;
+  int m = 0, n = 0, k = 0, tiles = 0;  // shape of a contraction launch (0: not given)
 };
 
 struct Profiler {
@@ -72,6 +73,13 @@ struct ProfScope {
   }
   ~ProfScope() {
     if (idx >= 0) cudaEventRecord(p->recs[idx].e1, s);
+  }
+  // Shape of the bracketed contraction: output rows and columns summed over
+  // its tasks, depth, and output tiles.
+  void shape(int m, int n, int k, int tiles) {
+    if (idx < 0) return;
+    ProfRec& r = p->recs[idx];
+    r.m = m; r.n = n; r.k = k; r.tiles = tiles;
   }
 };
 

@@ -158,6 +158,11 @@ int tc_slab(curfpContext* ctx, const int* abort_flag, View A, int arows, int ama
     return 4;
   const int grid = tiles < sms ? tiles : sms;  // persistent: one CTA per SM
   ProfScope ps(ctx->prof, ctx->stream, K_TC_GEMM, flops, 0);
+  {
+    int sm = 0, sn = 0;
+    for (int i = 0; i < cnt; ++i) { sm += b.t[i].m; sn += b.t[i].n; }
+    ps.shape(sm, sn, k, tiles);
+  }
   ktc::tc_gemm_kernel<<<grid, ktc::THREADS, ktc::SMEM_BYTES, ctx->stream>>>(mA, mB, b);
   ++ctx->launches;
   ++ctx->wait_launches;

@@ -160,6 +160,21 @@ def profile_enable(on: bool = True) -> None:
     check(h._lib.curfpProfileEnable(h.ptr, 1 if on else 0))
 
 
+def profile_records() -> list:
+    """Every record since profile_enable: dicts with class, ms, flops, bytes
+    and (contractions, solves) m, n, k, tiles."""
+    import numpy as np
+    h = _get_handle()
+    n = ctypes.c_longlong(0)
+    check(h._lib.curfpProfileRecords(h.ptr, 0, ctypes.byref(n), None))
+    buf = np.zeros((max(n.value, 1), 8), np.float64)
+    check(h._lib.curfpProfileRecords(h.ptr, n.value, ctypes.byref(n),
+                                     buf.ctypes.data_as(ctypes.c_void_p)))
+    keys = ("ms", "flops", "bytes", "m", "n", "k", "tiles")
+    return [dict(cls=KERNEL_CLASSES[int(r[0])], **{k_: float(v) for k_, v in zip(keys, r[1:])})
+            for r in buf[:n.value]]
+
+
 def profile_read() -> dict:
     """{class: {ms, flops, bytes, launches}} for the records since profile_enable."""
     h = _get_handle()

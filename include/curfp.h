@@ -410,6 +410,12 @@ curfpStatus_t curfpProfileEnable(curfpHandle_t handle, int enable);
 curfpStatus_t curfpProfileRead(curfpHandle_t handle, int kclass, double *ms,
                                double *flops, double *bytes,
                                long long *launches);
+/* Every record since curfpProfileEnable, 8 doubles each: class, device
+ * milliseconds, flops, bytes, and for contractions and solves the shape
+ * (m, n, k, output tiles; zeros otherwise).  At most max_records are
+ * written; *count receives the number held.  Synchronises the stream. */
+curfpStatus_t curfpProfileRecords(curfpHandle_t handle, long long max_records,
+                                  long long *count, double *out);
 
 #ifdef __cplusplus
 }
