@@ -111,12 +111,10 @@ class BoundsExec : public Exec {
     }
     return 0;
   }
-  // The CUDA executor's FP32 tile size.
-  int potrf_tile_rows() const override { return 2 * kPotrfTile; }
   int potrf_tile(View L, int n, int info_base) override {
     (void)info_base;
     ++calls;
-    if (n > potrf_tile_rows()) return 3;
+    if (n > kPotrfTile) return 3;
     check("potrf_tile", L, n, n, 1);
     return 0;
   }
