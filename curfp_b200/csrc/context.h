@@ -12,7 +12,6 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
-#include <vector>
 
 #include "engine.h"
 #include "profile.h"
@@ -51,7 +50,6 @@ class CudaExecT : public ExecT<T> {
  public:
   explicit CudaExecT(curfpContext* ctx, const int* abort_flag = nullptr)
       : ctx_(ctx), abort_(abort_flag) {}
-  ~CudaExecT() override;
   int gemm(const GemmProbT<T>* p, int count) override;
   int potrf_tile(ViewT<T> L, int n, int info_base) override;
   // 128-row tiles.  (A 256-row FP32 tile, one CTA of 512 threads, measured
@@ -69,24 +67,11 @@ class CudaExecT : public ExecT<T> {
   int gemm_pair(ViewT<T> X, ViewT<T> Y, int rows, int k, const SharedTaskT<T>* t, int count,
                 int math) override;
   int trsm_wave(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const T* W) override;
-  int trsm_leaf(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const T* W, int math) override;
   int potrf_adj_tile(ViewT<T> L, ViewT<T> G, int n) override;
 
  protected:
   curfpContext* ctx_;
   const int* abort_;
-  // Inverses of solve leaves, kept for the executor's lifetime (one entry
-  // point call): a leaf of the factor recurs in the solves of every
-  // recursion level above it.  Keyed by the leaf's view; freed
-  // stream-ordered by the destructor.
-  struct LeafInverse {
-    const T* p;
-    int64_t rs, cs;
-    int n;
-    T* inv;
-  };
-  std::vector<LeafInverse> leaf_inv_;
-  const T* leaf_inverse(ViewT<T> L, int n, const T* W);
 };
 using CudaExec = CudaExecT<float>;
 using CudaExecD = CudaExecT<double>;

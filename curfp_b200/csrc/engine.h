@@ -110,13 +110,6 @@ class ExecT {
     (void)L; (void)n; (void)B; (void)m; (void)alpha; (void)W;
     return kNotSupported;
   }
-  // Leaf of the recursive solve (n <= kWaveLeaf rows, W its 64-block
-  // records) by a route other than the wavefront solve, for executors that
-  // have one for these sizes; kNotSupported otherwise.
-  virtual int trsm_leaf(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const T* W, int math) {
-    (void)L; (void)n; (void)B; (void)m; (void)alpha; (void)W; (void)math;
-    return kNotSupported;
-  }
   // Adjoint of the Cholesky factorization of one diagonal tile
   // (n <= kAdjTile): L is the factor (lower triangle read), G holds the
   // cotangent of L's stored lower elements on entry and that of the factored

@@ -373,80 +373,6 @@ int launch_wave(curfpContext* ctx, const int* abort_flag, ViewT<T> L, int n, Vie
 }
 }  // namespace
 
-template <typename T>
-CudaExecT<T>::~CudaExecT() {
-  for (const LeafInverse& e : leaf_inv_) cudaFreeAsync(e.inv, ctx_->stream);
-  cudaGetLastError();
-}
-
-namespace {
-template <typename T>
-__global__ void set_identity(T* X, int n) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < (int64_t)n * n) X[i] = (i / n == i % n) ? T(1) : T(0);
-}
-}  // namespace
-
-// Inverse of the leaf (n x n lower, column-major, zeros above the diagonal)
-// from the executor's cache, or computed now by the wavefront solve on the
-// identity (W: the leaf's 64-block records); nullptr on failure.
-template <typename T>
-const T* CudaExecT<T>::leaf_inverse(ViewT<T> L, int n, const T* W) {
-  for (const LeafInverse& e : leaf_inv_)
-    if (e.p == L.p && e.rs == L.rs && e.cs == L.cs && e.n == n) return e.inv;
-  void* buf = nullptr;
-  if (cudaMallocFromPoolAsync(&buf, (size_t)n * n * sizeof(T), ctx_->pool, ctx_->stream) !=
-      cudaSuccess) {
-    cudaGetLastError();
-    return nullptr;
-  }
-  T* inv = static_cast<T*>(buf);
-  set_identity<T><<<(unsigned)(((int64_t)n * n + 255) / 256), 256, 0, ctx_->stream>>>(inv, n);
-  ++ctx_->launches;
-  if (cudaGetLastError() != cudaSuccess || trsm_wave(L, n, ViewT<T>{inv, 1, n}, n, T(1), W)) {
-    cudaFreeAsync(buf, ctx_->stream);
-    cudaGetLastError();
-    return nullptr;
-  }
-  leaf_inv_.push_back(LeafInverse{L.p, L.rs, L.cs, n, inv});
-  return inv;
-}
-
-// Leaves with many right-hand sides on the tensor cores: X = alpha inv(L) B
-// as one split-BF16 product with the (lower-masked) inverse, written over B
-// (B is staged whole before the product runs).  The inverse costs one
-// wavefront solve with n right-hand sides and is reused by every later
-// solve against the same leaf in this call.
-template <>
-int CudaExecT<double>::trsm_leaf(ViewT<double> L, int n, ViewT<double> B, int m, double alpha,
-                                 const double* W, int math) {
-  (void)L; (void)n; (void)B; (void)m; (void)alpha; (void)W; (void)math;
-  return kNotSupported;
-}
-
-template <>
-int CudaExecT<float>::trsm_leaf(View L, int n, View B, int m, float alpha, const float* W,
-                                int math) {
-  if (!math || m < 2 * n || !tc_worthwhile(n, m, n) || !tc_single_slab(m > n ? m : n, n))
-    return kNotSupported;
-  const float* inv = leaf_inverse(L, n, W);
-  if (!inv) return kNotSupported;  // the wavefront solve takes the leaf
-  GemmProb p{};
-  p.A = View{const_cast<float*>(inv), 1, n};
-  p.B = B;
-  p.C = B;
-  p.A2 = p.A;
-  p.B2 = p.B;
-  p.m = n; p.n = m; p.k = n; p.k2 = 0;
-  p.alpha = alpha; p.beta = 0.0f;
-  p.c_lower = 0;
-  p.a_tri = 1;
-  p.b_tri = p.a2_tri = p.b2_tri = 0;
-  p.inplace = 1;
-  p.math = 1;
-  return gemm(&p, 1);
-}
-
 // Up to 8 right-hand sides: 8-column chunks (the per-block products of the
 // chain shrink with the chunk); otherwise 64-column chunks.
 template <typename T>
