@@ -21,8 +21,8 @@ The RFP matrix (2.1 GB) is larger than L2 (126 MB): no extra L2 flush.
   python bench.py --case NAME [--n N] [--k K] [--nrhs R]
       runs one small workload of one kernel family a few times and exits (no
       timing): the commands the ncu summaries under profiles/ were made with.
-      Cases: ssfrk-bf16, ssfrk-fp32, chol-bf16, chol-fp32, solve, refine, pack,
-      norms, rank, nll-fused.
+      Cases: ssfrk-bf16, ssfrk-fp32, ssfr2k-bf16, chol-bf16, chol-fp32, solve, refine,
+      pack, norms, rank, symv, dsfrk, nll-fused.
 
 --impl reference times the reference's algorithm on the host cores: LAPACK's
 RFP routines (spftrf/spftrs via scipy/OpenBLAS, all threads), which the
@@ -633,8 +633,8 @@ def run_ours(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
-CASES = ("ssfrk-bf16", "ssfrk-fp32", "chol-bf16", "chol-fp32", "solve", "refine", "pack",
-         "norms", "rank", "symv", "dsfrk", "nll-fused")
+CASES = ("ssfrk-bf16", "ssfrk-fp32", "ssfr2k-bf16", "chol-bf16", "chol-fp32", "solve", "refine",
+         "pack", "norms", "rank", "symv", "dsfrk", "nll-fused")
 
 
 def run_case(args):
@@ -666,6 +666,15 @@ def run_case(args):
         prof_on()
         for _ in range(reps):
             P.ssfrk(A, C, math="bf16x3" if case == "ssfrk-bf16" else "fp32")
+    elif case == "ssfr2k-bf16":
+        # two distinct operands and beta = 1: the shape class of the solves'
+        # tensor-core updates (C -= L21 X1)
+        A = torch.randn(n, k, device="cuda", generator=g) / k ** 0.5
+        B = torch.randn(n, k, device="cuda", generator=g) / k ** 0.5
+        C = torch.randn(nt, device="cuda", generator=g)
+        prof_on()
+        for _ in range(reps):
+            curfp.ssfr2k(A, B, C, alpha=-1.0, beta=1.0)
     elif case in ("chol-bf16", "chol-fp32"):
         C0 = spd()
         C = torch.empty_like(C0)
