@@ -386,32 +386,46 @@ __global__ void __launch_bounds__(THREADS, 1)
         mbar_arrive(&acc_empty[b]);
       }
       if (!ok) break;
+      // The write-back runs while the MMA warp fills the other accumulator
+      // buffer, and under that load every global round trip is slow: the
+      // task's fields are read once into registers (a store through C could
+      // otherwise force them to be re-read), the 128 column scales come in
+      // with one coalesced load (lane l holds columns l + 32 i) and are
+      // broadcast by shuffle, and the write mask is a per-row column range.
       const int r = q * 32 + lane;
       const int gi = m0 + r;
-      if (gi < T.m) {
-        const float sa = batch.a_scale[T.a_row0 + gi] * 0x1p-14f;
-        float* crow = T.C + (int64_t)gi * T.c_rs;
-        const bool rd = T.beta != 0.f;
-        // 16-column slices: all loads of a slice (C for beta != 0, column
-        // scales) are issued before its stores, so their latencies overlap.
+      const int64_t ccs = T.c_cs;
+      const float beta = T.beta;
+      const int tn = T.n, tm = T.m, cmask = T.c_mask;
+      float bsr[BN / 32];
 #pragma unroll
-        for (int j0 = 0; j0 < BN; j0 += 16) {
-          float cv[16], bs[16];
+      for (int i = 0; i < BN / 32; ++i) {
+        const int j = lane + 32 * i;
+        bsr[i] = (n0 + j < tn) ? batch.b_scale[T.b_row0 + n0 + j] : 0.f;
+      }
+      int jlo = 0, jhi = tn - n0 < BN ? tn - n0 : BN;  // columns n0 + [jlo, jhi)
+      if (cmask == 1 && gi - n0 + 1 < jhi) jhi = gi - n0 + 1;
+      if (cmask == 2 && gi - n0 > jlo) jlo = gi - n0;
+      if (gi >= tm) jhi = 0;
+      // alpha s_i 2^-14 s_j is alpha times a power of two: out rounds once.
+      const float sa = (gi < tm ? batch.a_scale[T.a_row0 + gi] : 0.f) * 0x1p-14f * T.alpha;
+      float* const crow = T.C + (int64_t)(gi < tm ? gi : 0) * T.c_rs + (int64_t)n0 * ccs;
+      const bool rd = beta != 0.f;
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int gj = n0 + j0 + j;
-            const bool v = gj < T.n && (T.c_mask != 1 || gj <= gi) && (T.c_mask != 2 || gj >= gi);
-            bs[j] = v ? batch.b_scale[T.b_row0 + gj] : 0.f;
-            cv[j] = (v && rd) ? crow[(int64_t)gj * T.c_cs] : 0.f;
-          }
+      for (int j0 = 0; j0 < BN; j0 += 16) {
+        float cv[16];
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int gj = n0 + j0 + j;
-            const bool v = gj < T.n && (T.c_mask != 1 || gj <= gi) && (T.c_mask != 2 || gj >= gi);
-            float out = T.alpha * (acc[j0 + j] * (sa * bs[j]));
-            if (rd) out = fmaf(T.beta, cv[j], out);
-            if (v) crow[(int64_t)gj * T.c_cs] = out;
-          }
+        for (int j = 0; j < 16; ++j) {
+          const int jj = j0 + j;
+          cv[j] = (rd && jj >= jlo && jj < jhi) ? crow[jj * ccs] : 0.f;
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int jj = j0 + j;
+          const float bs = __shfl_sync(0xffffffffu, bsr[jj >> 5], jj & 31);
+          float out = acc[jj] * (sa * bs);
+          if (rd) out = fmaf(beta, cv[j], out);
+          if (jj >= jlo && jj < jhi) crow[jj * ccs] = out;
         }
       }
     }
@@ -425,10 +439,6 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
 }
 
-// Row scales of an FP32 view X (rows x k): s_i = smallest power of two with
-// s_i >= max_k |X_ik| (1 for an all-zero row), for rows < rows_pad (padding
-// rows get 1).  One block of 256 threads per 32 rows; the warp runs along
-// the contiguous dimension of X.
 // Triangular operand mask of the staging kernels: element (r, c) of the
 // staged operand (c counted from column koff of the full operand) is kept
 // when mask == 0, when mask == 1 and c + koff <= r (lower, diagonal
@@ -438,89 +448,108 @@ __device__ __forceinline__ bool keep_elem(int mask, int r, int c, int koff) {
   return mask == 0 || (mask == 1 ? c + koff <= r : c + koff >= r);
 }
 
-__global__ void __launch_bounds__(256) rowscale_kernel(View X, int rows, int k,
-                                                       float* scale, int rows_pad, int mask,
-                                                       int koff) {
+// Row maxima of |X| for an FP32 view X (rows x k).  Block (blockIdx.x,
+// blockIdx.y) covers rows 32 blockIdx.x .. +31 and the columns
+// [blockIdx.y * kseg, +kseg) (kseg a multiple of 128); every thread keeps 16
+// loads in flight, the warp running along X's contiguous dimension (a warp
+// takes four rows in turn when k is contiguous).  With
+// one column segment (atomic == 0) the block stores the row maxima (0 for
+// rows >= rows, the padding); with several, each block combines its partial
+// maxima by atomicMax on the bit patterns (non-negative floats order like
+// their bits) into an array zeroed beforehand.  NaN elements are skipped
+// here as by fmaxf; they reach the digits and the products unchanged.
+__global__ void __launch_bounds__(256, 4) rowmax_kernel(View X, int rows, int k, int kseg,
+                                                     unsigned* maxbits, int mask, int koff,
+                                                     int atomic) {
   __shared__ float red[8][33];
   const int r0 = blockIdx.x * 32;
+  const int cb = blockIdx.y * kseg, ce = min(k, cb + kseg);
   const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
   const bool kcont = (X.cs == 1 || X.cs == -1);
-  float m[4] = {0.f, 0.f, 0.f, 0.f};
+  float m = 0.f;  // the maximum of row r0 + threadIdx.x, in threads < 32
   if (kcont) {
-    // warp ty handles rows r0 + ty + 8 j; lanes stride over k, 8 loads in
-    // flight per lane
-#pragma unroll
+    // warp ty: rows r0 + ty + 8 j (j < 4) in turn, lanes along k, 16
+    // columns in flight
+#pragma unroll 1
     for (int j = 0; j < 4; ++j) {
       const int r = r0 + ty + 8 * j;
+      float mj = 0.f;
       if (r < rows) {
         const float* row = X.p + (int64_t)r * X.rs;
-        for (int c = tx; c < k; c += 256) {
-          float v[8];
+        for (int c = cb + tx; c < ce; c += 512) {
+          float v[16];
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
+          for (int u = 0; u < 16; ++u) {
             const int cc = c + 32 * u;
-            v[u] = (cc < k && keep_elem(mask, r, cc, koff)) ? fabsf(row[(int64_t)cc * X.cs]) : 0.f;
+            v[u] = (cc < ce && keep_elem(mask, r, cc, koff)) ? fabsf(row[(int64_t)cc * X.cs]) : 0.f;
           }
 #pragma unroll
-          for (int u = 0; u < 8; ++u) m[j] = fmaxf(m[j], v[u]);
+          for (int u = 0; u < 16; ++u) mj = fmaxf(mj, v[u]);
         }
       }
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      for (int o = 16; o; o >>= 1) m[j] = fmaxf(m[j], __shfl_xor_sync(0xffffffffu, m[j], o));
-      if (tx == 0) red[0][ty + 8 * j] = m[j];
+      for (int o = 16; o; o >>= 1) mj = fmaxf(mj, __shfl_xor_sync(0xffffffffu, mj, o));
+      if (tx == 0) red[0][ty + 8 * j] = mj;
     }
     __syncthreads();
-    if (threadIdx.x < 32) m[0] = red[0][threadIdx.x];
+    if (threadIdx.x < 32) m = red[0][threadIdx.x];
   } else {
-    // thread (tx, ty): row r0 + tx, k in ty, ty + 8, ...; 8 loads in flight
+    // thread (tx, ty): row r0 + tx, columns ty + 8 u (u < 16) of each 128
     const int r = r0 + tx;
-    if (r < rows) {
-      const float* row = X.p + (int64_t)r * X.rs;
-      for (int c = ty; c < k; c += 64) {
-        float v[8];
+    const float* row = X.p + (int64_t)(r < rows ? r : 0) * X.rs;
+    float mt = 0.f;
+    for (int c = cb + ty; c < ce; c += 128) {
+      float v[16];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int cc = c + 8 * u;
-          v[u] = (cc < k && keep_elem(mask, r, cc, koff)) ? fabsf(row[(int64_t)cc * X.cs]) : 0.f;
-        }
-#pragma unroll
-        for (int u = 0; u < 8; ++u) m[0] = fmaxf(m[0], v[u]);
+      for (int u = 0; u < 16; ++u) {
+        const int cc = c + 8 * u;
+        v[u] = (r < rows && cc < ce && keep_elem(mask, r, cc, koff))
+                   ? fabsf(row[(int64_t)cc * X.cs])
+                   : 0.f;
       }
+#pragma unroll
+      for (int u = 0; u < 16; ++u) mt = fmaxf(mt, v[u]);
     }
-    red[ty][tx] = m[0];
+    red[ty][tx] = mt;
     __syncthreads();
     if (threadIdx.x < 32) {
-      m[0] = red[0][threadIdx.x];
-      for (int y = 1; y < 8; ++y) m[0] = fmaxf(m[0], red[y][threadIdx.x]);
+      m = red[0][threadIdx.x];
+      for (int y = 1; y < 8; ++y) m = fmaxf(m, red[y][threadIdx.x]);
     }
   }
   if (threadIdx.x < 32) {
     const int r = r0 + threadIdx.x;
-    if (r < rows_pad) {
-      float s = 1.0f;
-      if (r < rows && m[0] > 0.f) {
-        int e;
-        frexpf(m[0], &e);   // m = f * 2^e, f in [0.5, 1)  ->  2^e >= m
-        s = ldexpf(1.0f, e);
-      }
-      scale[r] = s;
+    const unsigned bits = __float_as_uint(m);
+    if (atomic) {
+      if (r < rows && bits) atomicMax(maxbits + r, bits);
+    } else {
+      maxbits[r] = r < rows ? bits : 0u;
     }
   }
 }
 
-// Digits of X (see the header): nplanes (3 or 4) BF16 planes h = d0, m = d1,
+// Row scale from the row maximum m: the smallest power of two 2^e with
+// 2^e > m/2 and 2^e >= m (frexpf: m = f 2^e, f in [0.5, 1)); 1 for m = 0.
+__device__ __forceinline__ float row_scale(unsigned maxbits) {
+  const float m = __uint_as_float(maxbits);
+  if (!(m > 0.f)) return 1.0f;
+  int e;
+  frexpf(m, &e);
+  return ldexpf(1.0f, e);
+}
+
+// Digits of X (see the header), with the row scales s_i = row_scale(max_i)
+// (block column 0 also stores them in scale[] for the contraction's
+// epilogue): nplanes (3 or 4) BF16 planes h = d0, m = d1,
 // l' = 2^-8 d2 and m' = 2^-8 d1, row-major with K contiguous, out[p][i][j],
 // plane stride rows_pad * k_pad; zero padding.  A block stages a 32 x 64 tile
 // through shared memory (the warp reads along X's contiguous dimension) and
 // writes BF16 pairs (128 bytes per warp store).  Grid (k_pad/64, rows_pad/32),
 // block (32, 8); k_pad is a multiple of 64.
 __global__ void __launch_bounds__(256) digits_kernel(View X, int rows, int k,
-                                                     const float* __restrict__ scale,
-                                                     __nv_bfloat16* out, int rows_pad,
-                                                     int k_pad, int nplanes, int mask,
-                                                     int koff) {
+                                                     const unsigned* __restrict__ maxbits,
+                                                     float* scale, __nv_bfloat16* out,
+                                                     int rows_pad, int k_pad, int nplanes,
+                                                     int mask, int koff) {
   __shared__ float t[32][65];
   const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 64;
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -540,7 +569,9 @@ __global__ void __launch_bounds__(256) digits_kernel(View X, int rows, int k,
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const int lr = ty + 8 * r;
-    const float inv = 1.0f / scale[r0 + lr];            // power of two: exact
+    const float sc = row_scale(maxbits[r0 + lr]);
+    if (blockIdx.x == 0 && tx == 0) scale[r0 + lr] = sc;  // for the contraction's epilogue
+    const float inv = 1.0f / sc;                          // power of two: exact
     float d[4][2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {

@@ -46,8 +46,19 @@ struct Staged {
   int planes;
 };
 
+int sm_count(const curfpContext* ctx) {
+  static int sms = 0;
+  if (!sms && (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) !=
+                   cudaSuccess ||
+               sms <= 0))
+    sms = 148;
+  return sms;
+}
+
 // Stage X (rows x k) as row scales + `planes` BF16 digit planes in a context
-// staging buffer (two kernels: row maxima, then digits).
+// staging buffer: row maxima (split along k into enough blocks for about
+// eight per SM; the partial maxima meet by atomicMax in a zeroed array), then
+// the digits, whose first block column also stores the scales.
 int stage(curfpContext* ctx, void** buf, size_t* cur, View X, int rows, int k, int planes,
           int mask, int koff, Staged* out) {
   out->rows_pad = (int)(round_up(rows, ktc::BN) + ktc::BN);
@@ -56,18 +67,30 @@ int stage(curfpContext* ctx, void** buf, size_t* cur, View X, int rows, int k, i
   const size_t plane_bytes =
       (size_t)planes * out->rows_pad * out->k_pad * sizeof(__nv_bfloat16);
   const size_t off = (size_t)round_up((int64_t)plane_bytes, 256);
-  void* p = grow_buffer(ctx, buf, cur, off + (size_t)out->rows_pad * sizeof(float));
+  void* p = grow_buffer(ctx, buf, cur,
+                        off + (size_t)out->rows_pad * (sizeof(float) + sizeof(unsigned)));
   if (!p) return 2;
   out->p = static_cast<__nv_bfloat16*>(p);
   out->scale = reinterpret_cast<float*>(static_cast<char*>(p) + off);
+  unsigned* maxbits = reinterpret_cast<unsigned*>(out->scale + out->rows_pad);
   ProfScope ps(ctx->prof, ctx->stream, K_TC_STAGE, 0,
                (double)rows * k * 8.0 + (double)out->rows_pad * out->k_pad * 2.0 * planes);
-  ktc::rowscale_kernel<<<out->rows_pad / 32, 256, 0, ctx->stream>>>(X, rows, k, out->scale,
-                                                                   out->rows_pad, mask, koff);
+  const int groups = out->rows_pad / 32;
+  const int kchunks = k > 0 ? (k + 127) / 128 : 1;
+  int nsplit = (8 * sm_count(ctx) + groups - 1) / groups;
+  if (nsplit > kchunks) nsplit = kchunks;
+  const int kseg = 128 * ((kchunks + nsplit - 1) / nsplit);
+  const int ksplit = k > 0 ? (k + kseg - 1) / kseg : 1;
+  if (ksplit > 1 &&
+      cudaMemsetAsync(maxbits, 0, (size_t)out->rows_pad * sizeof(unsigned), ctx->stream) !=
+          cudaSuccess)
+    return 4;
+  ktc::rowmax_kernel<<<dim3(groups, ksplit), 256, 0, ctx->stream>>>(
+      X, rows, k, kseg, maxbits, mask, koff, ksplit > 1 ? 1 : 0);
   dim3 grid(out->k_pad / 64, out->rows_pad / 32);
-  ktc::digits_kernel<<<grid, dim3(32, 8), 0, ctx->stream>>>(X, rows, k, out->scale, out->p,
-                                                            out->rows_pad, out->k_pad, planes,
-                                                            mask, koff);
+  ktc::digits_kernel<<<grid, dim3(32, 8), 0, ctx->stream>>>(X, rows, k, maxbits, out->scale,
+                                                            out->p, out->rows_pad, out->k_pad,
+                                                            planes, mask, koff);
   ctx->launches += 2;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
@@ -151,11 +174,7 @@ int tc_slab(curfpContext* ctx, const int* abort_flag, View A, int arows, int ama
       return 4;
     attr_set = true;
   }
-  static int sms = 0;
-  if (!sms && (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) !=
-                   cudaSuccess ||
-               sms <= 0))
-    return 4;
+  const int sms = sm_count(ctx);
   const int grid = tiles < sms ? tiles : sms;  // persistent: one CTA per SM
   ProfScope ps(ctx->prof, ctx->stream, K_TC_GEMM, flops, 0);
   {
