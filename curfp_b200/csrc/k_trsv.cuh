@@ -367,13 +367,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
       if (a < rows && b < cols) Bt.p[(int64_t)a * Bt.rs + (int64_t)b * Bt.cs] = Xs1[a * LX + b];
     }
   }
-  // The block's stores are ordered before thread 0's fence by the barrier;
-  // the fence and the release then publish them at GPU scope.
+  // The block's stores are ordered before thread 0's release by the
+  // barrier; a release store is cumulative (a release fence plus the flag
+  // store), so it publishes them at GPU scope without a separate
+  // sequentially consistent fence.
   __syncthreads();
-  if (tid == 0) {
-    __threadfence();
-    st_release(&flags[j * nchunk + c], 1);
-  }
+  if (tid == 0) st_release(&flags[j * nchunk + c], 1);
 }
 
 }  // namespace ktrsv
