@@ -111,7 +111,7 @@ int make_map(const Staged& s, int box_rows, CUtensorMap* map) {
 }  // namespace
 
 bool tc_worthwhile(int m, int n, int k) {
-  return m >= 128 && n >= 128 && k >= 128 && (double)m * n * k >= 6.7e7;
+  return m >= 128 && n >= 128 && k >= 128 && (double)m * n * k >= 2.7e8;
 }
 
 bool tc_single_slab(int rows, int k) {

@@ -84,7 +84,7 @@ curfpStatus_t curfpGetStream(curfpHandle_t handle, cudaStream_t *stream);
  * inside the FP32 routines; set per handle with curfpSetMathMode, or per call
  * through the *Ex entry points below.
  *   CURFP_MATH_SPLIT_BF16 (the handle's default): contractions with
- *     m, n, k >= 128 and m*n*k >= 6.7e7 run on the tcgen05 tensor cores; every
+ *     m, n, k >= 128 and m*n*k >= 2.7e8 run on the tcgen05 tensor cores; every
  *     FP32 operand row is scaled by a power of two and split into three
  *     integer BF16 digits, and the six digit products of weight >= 2^-16 are
  *     accumulated exactly per 1024-deep chunk and summed in FP32.  Measured

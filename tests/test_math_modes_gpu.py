@@ -1,6 +1,6 @@
 """The drop-in FP32 routines (ssfrk, ssfr2k, spftrf, spftrs, spftri) in both
 math modes of the handle, all 8 variants, at sizes whose contractions reach
-the tensor-core path (m, n, k >= 128 and m n k >= 6.7e7).
+the tensor-core path (m, n, k >= 128 and m n k >= 2.7e8).
 
 * "bf16x3" (the default): large contractions run as exact split-BF16
   tcgen05 products; the test checks that tc_gemm_kernel actually ran.
