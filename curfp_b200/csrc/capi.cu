@@ -54,20 +54,12 @@ inline int read_info(curfpHandle_t h, int* info, int* err) {
 int symm_launch(curfpHandle_t h, const Geometry& g, const float* A, const float* X,
                 int64_t ldx, float* Y, int64_t ldy, int nrhs, float alpha, float beta);
 
-// The dynamic shared-memory limit of the 64 x 64 or the wide kernel, set
-// once per process.
-inline bool symm_attr(bool wide) {
-  static bool done_narrow = false, done_wide = false;
-  bool& done = wide ? done_wide : done_narrow;
+inline bool symm_attr() {
+  static bool done = false;
   if (!done) {
-    const cudaError_t e =
-        wide ? cudaFuncSetAttribute(rfp::kref::symm_acc64_wide,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    rfp::kref::SYMMW_SMEM)
-             : cudaFuncSetAttribute(rfp::kref::symm_acc64,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    rfp::kref::SYMM_SMEM);
-    if (e != cudaSuccess) return false;
+    if (cudaFuncSetAttribute(rfp::kref::symm_acc64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             rfp::kref::SYMM_SMEM) != cudaSuccess)
+      return false;
     done = true;
   }
   return true;
@@ -113,26 +105,11 @@ curfpStatus_t pack(curfpHandle_t h, int transr, int lower, int n, const T* src,
 
 int symm_launch(curfpHandle_t h, const Geometry& g, const float* A, const float* X,
                 int64_t ldx, float* Y, int64_t ldy, int nrhs, float alpha, float beta) {
+  if (!symm_attr()) return 4;
   const int n = g.n;
-  // nrhs >= 32: the 128 x 64 tile of 8 x 8 accumulators per thread (two CTAs
-  // per SM), split over the column blocks so that the CTA count fills whole
-  // waves; fewer right-hand sides: the 64 x 64 tile.
-  const bool wide = nrhs >= 32;
-  if (!symm_attr(wide)) return 4;
-  const int tr = wide ? rfp::kref::WR : rfp::kref::TB, tcol = wide ? rfp::kref::WC : rfp::kref::TB;
-  const int bx = (n + tr - 1) / tr, by = (nrhs + tcol - 1) / tcol;
+  const int bx = (n + rfp::kref::TB - 1) / rfp::kref::TB, by = (nrhs + rfp::kref::TB - 1) / rfp::kref::TB;
   int split = 1;
-  if (wide) {
-    const int slots = 2 * 148, nkb = (n + rfp::kref::WK - 1) / rfp::kref::WK;
-    double best = 0;
-    for (int z = 1; z <= 16 && nkb / z >= 8; ++z) {
-      const int64_t t = (int64_t)bx * by * z;
-      const double eff = (double)t / ((double)((t + slots - 1) / slots) * slots);
-      if (eff > best + 0.02) { best = eff; split = z; }
-    }
-  } else {
-    while ((int64_t)bx * by * split < 4 * 148 && split < 16 && bx / (split * 2) >= 4) split *= 2;
-  }
+  while ((int64_t)bx * by * split < 4 * 148 && split < 16 && bx / (split * 2) >= 4) split *= 2;
   double* R = nullptr;
   if (split > 1) {
     R = static_cast<double*>(rfp::grow_buffer(h, &h->ws3, &h->ws3_bytes,
@@ -144,13 +121,8 @@ int symm_launch(curfpHandle_t h, const Geometry& g, const float* A, const float*
   {
     rfp::ProfScope ps(h->prof, h->stream, rfp::K_SYMM64, 2.0 * n * (double)n * nrhs,
                       4.0 * n * (double)n);
-    if (wide)
-      rfp::kref::symm_acc64_wide<<<dim3(bx, by, split), rfp::kref::WTHREADS,
-                                   rfp::kref::SYMMW_SMEM, h->stream>>>(g, A, X, ldx, Y, ldy,
-                                                                      nrhs, alpha, beta, R);
-    else
-      rfp::kref::symm_acc64<<<dim3(bx, by, split), 256, rfp::kref::SYMM_SMEM, h->stream>>>(
-          g, A, X, ldx, Y, ldy, nrhs, alpha, beta, R);
+    rfp::kref::symm_acc64<<<dim3(bx, by, split), 256, rfp::kref::SYMM_SMEM, h->stream>>>(
+        g, A, X, ldx, Y, ldy, nrhs, alpha, beta, R);
     ++h->launches;
     if (R) {
       rfp::kref::symm_finish<<<148 * 4, 256, 0, h->stream>>>(R, n, nrhs, Y, ldy, alpha, beta);

@@ -122,120 +122,6 @@ __global__ void __launch_bounds__(256) symm_acc64(Geometry g, const float* __res
   }
 }
 
-// The same product with a wider register tile, for nrhs >= 32: one CTA of
-// 128 threads owns a 128-row x 64-column output block, each thread 8 x 8
-// FP64 accumulators on rows {2 tr, 2 tr + 1} + 32 q and columns
-// {2 tc, 2 tc + 1} + 16 q (q < 4).  Per k the thread reads its 8 A and 8 X
-// values as eight 16-byte shared loads, all conflict-free or broadcast
-// (consecutive tr / tc read consecutive 16-byte words), for 64 DFMA: half
-// the shared-memory bytes per DFMA of the 4 x 4 tile above, which the FP64
-// pipe can consume at full rate.  A 128 x 32 block of A (addressed through
-// the RFP geometry, the upper half from the stored lower element) and a
-// 32 x 64 block of X are loaded into registers one block ahead, converted
-// to FP64 once and staged k-major.  gridDim.z splits the sum over the
-// 32-wide column blocks as in symm_acc64.
-constexpr int WR = 128, WC = 64, WK = 32, WTHREADS = 128;
-// k-major rows padded by two doubles: 16-byte aligned, and the staging
-// stores of one warp (consecutive k) spread over the banks
-constexpr int WRP = WR + 2, WCP = WC + 2;
-constexpr int SYMMW_SMEM = WK * (WRP + WCP) * 8;  // 48.5 KB
-
-__global__ void __launch_bounds__(WTHREADS, 2)
-    symm_acc64_wide(Geometry g, const float* __restrict__ arf, const float* __restrict__ X,
-                    int64_t ldx, float* Y, int64_t ldy, int nrhs, float alpha, float beta,
-                    double* R) {
-  extern __shared__ double dsw[];
-  double* As = dsw;             // [WK][WRP]: element (row, k) at As[k * WRP + row]
-  double* Xs = dsw + WK * WRP;  // [WK][WCP]
-  const int n = g.n;
-  const int i0 = blockIdx.x * WR, c0 = blockIdx.y * WC;
-  const int tid = threadIdx.x;
-  const int tr = tid / 8, tc = tid % 8;
-  const int nkb = (n + WK - 1) / WK;
-  const int per = (nkb + gridDim.z - 1) / gridDim.z;
-  const int kb0 = blockIdx.z * per, kb1 = min(nkb, kb0 + per);
-  double acc[8][8];
-#pragma unroll
-  for (int a = 0; a < 8; ++a)
-#pragma unroll
-    for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
-
-  float av[WR * WK / WTHREADS], xv[WK * WC / WTHREADS];  // 32 + 16
-  bool i_fast = true;
-  auto load = [&](int k0) {
-    // the warp runs along the RFP block's contiguous direction (see symm_load)
-    const bool lower_tile = i0 >= k0;
-    const int64_t p0 = lower_tile ? i0 : k0, q0 = lower_tile ? k0 : i0;
-    const BlockGeom& bg = q0 < g.n1 ? (p0 < g.n1 ? g.b11 : g.b21) : g.b22;
-    const bool p_cont = (bg.rs == 1 || bg.rs == -1);
-    i_fast = lower_tile ? p_cont : !p_cont;
-#pragma unroll
-    for (int r = 0; r < WR * WK / WTHREADS; ++r) {
-      const int e = tid + WTHREADS * r;
-      const int li = i_fast ? e % WR : e / WK, lk = i_fast ? e / WR : e % WK;
-      const int64_t i = i0 + li, j = k0 + lk;
-      av[r] = (i < n && j < n) ? arf[i >= j ? lower_offset(g, i, j) : lower_offset(g, j, i)]
-                               : 0.f;
-    }
-#pragma unroll
-    for (int r = 0; r < WK * WC / WTHREADS; ++r) {
-      const int e = tid + WTHREADS * r;
-      const int64_t xr = k0 + e % WK, c = c0 + e / WK;  // X column-major: rows fastest
-      xv[r] = (xr < n && c < nrhs) ? X[xr + c * ldx] : 0.f;
-    }
-  };
-  if (kb0 < kb1) load(kb0 * WK);
-  for (int kb = kb0; kb < kb1; ++kb) {
-#pragma unroll
-    for (int r = 0; r < WR * WK / WTHREADS; ++r) {
-      const int e = tid + WTHREADS * r;
-      const int li = i_fast ? e % WR : e / WK, lk = i_fast ? e / WR : e % WK;
-      As[lk * WRP + li] = (double)av[r];
-    }
-#pragma unroll
-    for (int r = 0; r < WK * WC / WTHREADS; ++r) {
-      const int e = tid + WTHREADS * r;
-      Xs[(e % WK) * WCP + e / WK] = (double)xv[r];
-    }
-    __syncthreads();
-    if (kb + 1 < kb1) load((kb + 1) * WK);
-#pragma unroll 4
-    for (int k = 0; k < WK; ++k) {
-      double a[8], x[8];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const double2 av2 = *reinterpret_cast<const double2*>(As + k * WRP + 2 * tr + 32 * q);
-        const double2 xv2 = *reinterpret_cast<const double2*>(Xs + k * WCP + 2 * tc + 16 * q);
-        a[2 * q] = av2.x; a[2 * q + 1] = av2.y;
-        x[2 * q] = xv2.x; x[2 * q + 1] = xv2.y;
-      }
-#pragma unroll
-      for (int p = 0; p < 8; ++p)
-#pragma unroll
-        for (int q = 0; q < 8; ++q) acc[p][q] = fma(a[p], x[q], acc[p][q]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int p = 0; p < 8; ++p) {
-    const int64_t i = i0 + 2 * tr + (p & 1) + 32 * (p >> 1);
-    if (i >= n) continue;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int64_t c = c0 + 2 * tc + (q & 1) + 16 * (q >> 1);
-      if (c >= nrhs) continue;
-      if (R) {
-        atomicAdd(R + i + c * (int64_t)n, acc[p][q]);
-      } else {
-        float* y = Y + i + c * ldy;
-        double v = (double)alpha * acc[p][q];
-        if (beta != 0.f) v += (double)beta * (double)*y;
-        *y = (float)v;
-      }
-    }
-  }
-}
-
 // Y := alpha * R + beta * Y (R the FP64 accumulator of a split symm_acc64).
 __global__ void symm_finish(const double* __restrict__ R, int n, int nrhs, float* Y,
                             int64_t ldy, float alpha, float beta) {
