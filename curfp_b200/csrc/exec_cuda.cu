@@ -299,10 +299,7 @@ int CudaExecT<T>::potrf_tile(ViewT<T> L, int n, int info_base) {
   if (n <= 0) return 0;
   if (n > potrf_tile_rows()) return 3;
   ProfScope ps(ctx_->prof, ctx_->stream, K_POTRF, (double)n * n * n / 3.0, 0);
-  if (n <= ktile::PT) return launch_potrf<T, ktile::PT, 256>(ctx_, L, n, info_base);
-  if constexpr (sizeof(T) == 4)
-    return launch_potrf<T, ktile::PT_BIG, 512>(ctx_, L, n, info_base);
-  return 3;
+  return launch_potrf<T, ktile::PT, 256>(ctx_, L, n, info_base);
 }
 
 template <typename T>

@@ -65,8 +65,8 @@ constexpr int LD = T + 1;    // padded shared-memory leading dimension
 
 static_assert(T == kTrsmLeaf && T == kTriTile, "tile kernels assume one tile size");
 
-// Lower-triangular Cholesky of an n x n tile (n <= NT, NT = 128 or 256), one
-// CTA of THR threads, the tile's lower triangle in shared memory.  Blocked
+// Lower-triangular Cholesky of an n x n tile (n <= NT = 128), one CTA of THR
+// threads, the tile's lower triangle in shared memory.  Blocked
 // by 32 columns:
 //   (1) warp 0 factors the 32 x 32 diagonal block in registers (lane = row;
 //       each column is broadcast through shared memory as 16-byte reads;
@@ -77,13 +77,11 @@ static_assert(T == kTrsmLeaf && T == kTriTile, "tile kernels assume one tile siz
 //       4 x 4 register blocks.
 // Shared-memory layout, panel-blocked: panel p (columns 32p .. 32p+31) holds
 // rows 32p .. NT-1 with a row stride of 33, so consecutive rows of a column
-// fall in consecutive banks and only the lower triangle is stored (NT = 256
-// in FP32: 148 KB).
+// fall in consecutive banks and only the lower triangle is stored.
 // On a pivot that is not > 0 (or NaN) the device info word becomes
 // min(info, info_base + column + 1), the partially factored tile is written
 // back and the kernel returns (LAPACK xPOTRF semantics).
-constexpr int PT = 128;           // potrf tile of the FP64 executor and the CPU planner tests
-constexpr int PT_BIG = 256;       // potrf tile of the FP32 executor
+constexpr int PT = 128;           // potrf tile (FP32 and FP64 executors, CPU planner tests)
 constexpr int PLDP = 33;          // row stride inside a panel
 template <int NT>
 __host__ __device__ constexpr int panel_off(int p) {
@@ -98,8 +96,6 @@ template <typename E, int NT>
 constexpr int potrf_smem() { return (panel_off<NT>(NT / 32) + 64) * (int)sizeof(E); }
 constexpr int POTRF_SMEM = potrf_smem<float, PT>();
 static_assert(PT == kPotrfTile, "potrf tile size");
-template <typename E>
-constexpr int potrf_threads(int nt) { return nt == PT_BIG ? 512 : 256; }
 
 // 1/sqrt(d): the hardware estimate refined by one Newton-Raphson step for
 // y = x^-1/2 (y <- y (3 - d y^2) / 2).
