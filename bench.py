@@ -14,6 +14,11 @@ One step = Cholesky of a fresh copy of C + solve of the 64 right-hand sides:
       (split-BF16 contractions, curfpSpftrf + curfpSpftrs, no refinement).
 Metric: Cholesky+solve TFLOP/s = (n^3/3 + n^2/2 + n/6 + 2 n^2 nrhs) / time.
 The RFP matrix (2.1 GB) is larger than L2 (126 MB): no extra L2 flush.
+e2e: the same step from pinned host buffers through the C ABI -- the matrix
+by curfpSpftrfFromHost (one host-to-device transfer, the array's second part
+copied while the first diagonal block is factored, the original kept on the
+device for the residuals), the right-hand sides by one copy, then
+curfpSpftrsRefine and the solution copied back.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--math bf16x3|fp32] [--n 32768] [--k 1024] [--nrhs 64]
@@ -338,6 +343,13 @@ class Lib:
                                     ctypes.byref(self.info), math)
         assert st == 0 and self.info.value == 0, (st, self.info.value)
 
+    def spftrf_from_host(self, n, C_h, C, Corig, math):
+        st = self.lib.curfpSpftrfFromHost(self.h.ptr, 1, 1, n, ctypes.c_void_p(C_h.data_ptr()),
+                                          ctypes.c_void_p(C.data_ptr()),
+                                          ctypes.c_void_p(Corig.data_ptr()),
+                                          ctypes.byref(self.info), math)
+        assert st == 0 and self.info.value == 0, (st, self.info.value)
+
     def spftrf_dropin(self, n, C):
         st = self.lib.curfpSpftrf(self.h.ptr, 1, 1, n, ctypes.c_void_p(C.data_ptr()),
                                   ctypes.byref(self.info))
@@ -582,10 +594,11 @@ def run_ours(args, rank, world, local):
 
         def step_e2e():
             if math_head:
-                Corig.copy_(C_h, non_blocking=True)
-                C.copy_(Corig)
+                # host RFP array -> device (original kept for the residuals)
+                # and factor, the copy of the array's second part overlapping
+                # the first diagonal block's factorization
                 X.copy_(B_h, non_blocking=True)
-                L.spftrf(n, C, 1)
+                L.spftrf_from_host(n, C_h, C, Corig, 1)
                 L.refine(n, nrhs, Corig, C, X, args.max_iter)
             else:
                 C.copy_(C_h, non_blocking=True)

@@ -38,6 +38,7 @@ SIGNATURES = {
     "curfpSsfrkEx": [_h, _i, _i, _i, _i, _i, ctypes.POINTER(_f), _p, _i,
                      ctypes.POINTER(_f), _p, _i],
     "curfpSpftrfEx": [_h, _i, _i, _i, _p, ctypes.POINTER(_i), _i],
+    "curfpSpftrfFromHost": [_h, _i, _i, _i, _p, _p, _p, ctypes.POINTER(_i), _i],
     "curfpSetMathMode": [_h, _i],
     "curfpGetMathMode": [_h, ctypes.POINTER(_i)],
     "curfpSpftrsRefine": [_h, _i, _i, _i, _i, _p, _p, _p, _i, _i, ctypes.POINTER(_i)],

@@ -182,6 +182,12 @@ curfpStatus_t curfpDestroy(curfpHandle_t handle) {
   if (handle->tsv) cudaFree(handle->tsv);
   if (handle->wsg) cudaFree(handle->wsg);
   if (handle->d_info) cudaFree(handle->d_info);
+  if (handle->copy_stream) {
+    cudaStreamSynchronize(handle->copy_stream);
+    cudaStreamDestroy(handle->copy_stream);
+  }
+  if (handle->ev_start) cudaEventDestroy(handle->ev_start);
+  if (handle->ev_rest) cudaEventDestroy(handle->ev_rest);
   if (handle->pool) cudaMemPoolDestroy(handle->pool);
   cudaGetLastError();
   delete handle;
@@ -360,6 +366,81 @@ curfpStatus_t curfpSpftrfEx(curfpHandle_t handle, curfpOperation_t transr,
   if (math != CURFP_MATH_FP32 && math != CURFP_MATH_SPLIT_BF16)
     return CURFP_STATUS_INVALID_VALUE;
   return spftrf_impl(handle, transr, uplo, n, A, info, (int)math);
+}
+
+// Not in the reference: the factorization of an RFP matrix held in host
+// memory.  The span of the array that the first diagonal block touches is
+// copied first, on the handle's stream; the rest is copied on an internal
+// stream (after everything already enqueued on the handle's stream) and the
+// factorization waits for it only after the first diagonal block, so that
+// for layouts where that block occupies its own part of the array (TRANSR =
+// T) the rest of the transfer overlaps its factorization.  With arf_orig the
+// host array is copied there and, region by region, on to arf (one
+// host-to-device transfer for both).
+curfpStatus_t curfpSpftrfFromHost(curfpHandle_t handle, curfpOperation_t transr,
+                                  curfpFillMode_t uplo, int n, const float* arf_host,
+                                  float* arf, float* arf_orig, int* info, curfpMath_t math) {
+  if (!handle) return CURFP_STATUS_NOT_INITIALIZED;
+  if (n < 0 || !info || (n > 0 && (!arf_host || !arf)) || (arf_orig && arf_orig == arf))
+    return CURFP_STATUS_INVALID_VALUE;
+  if (math != CURFP_MATH_FP32 && math != CURFP_MATH_SPLIT_BF16)
+    return CURFP_STATUS_INVALID_VALUE;
+  *info = 0;
+  if (n == 0) return CURFP_STATUS_SUCCESS;
+  if (!handle->copy_stream &&
+      cudaStreamCreateWithFlags(&handle->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return CURFP_STATUS_EXECUTION_FAILED;
+  if (!handle->ev_start &&
+      cudaEventCreateWithFlags(&handle->ev_start, cudaEventDisableTiming) != cudaSuccess)
+    return CURFP_STATUS_EXECUTION_FAILED;
+  if (!handle->ev_rest &&
+      cudaEventCreateWithFlags(&handle->ev_rest, cudaEventDisableTiming) != cudaSuccess)
+    return CURFP_STATUS_EXECUTION_FAILED;
+  const Geometry g = rfp::geometry(n, transr == CURFP_OP_T, uplo == CURFP_FILL_MODE_LOWER);
+  const int64_t total = (int64_t)n * (n + 1) / 2;
+  // Offsets the first diagonal block touches: [lo, hi) (its strides are
+  // positive in every variant, so (0, 0) and (n1 - 1, n1 - 1) bound it).
+  int64_t lo = 0, hi = total;
+  if (g.n1 > 0) {
+    lo = g.b11.off;
+    hi = g.b11.off + (int64_t)(g.n1 - 1) * (g.b11.rs + g.b11.cs) + 1;
+  }
+  float* first = arf_orig ? arf_orig : arf;
+  auto copy = [&](int64_t a, int64_t b, cudaStream_t st) {
+    if (b <= a) return true;
+    const size_t bytes = (size_t)(b - a) * sizeof(float);
+    if (cudaMemcpyAsync(first + a, arf_host + a, bytes, cudaMemcpyHostToDevice, st) !=
+        cudaSuccess)
+      return false;
+    return !arf_orig ||
+           cudaMemcpyAsync(arf + a, arf_orig + a, bytes, cudaMemcpyDeviceToDevice, st) ==
+               cudaSuccess;
+  };
+  cudaStream_t cs = handle->copy_stream;
+  if (cudaEventRecord(handle->ev_start, handle->stream) != cudaSuccess ||
+      cudaStreamWaitEvent(cs, handle->ev_start, 0) != cudaSuccess || !copy(lo, hi, handle->stream) ||
+      !copy(0, lo, cs) || !copy(hi, total, cs) ||
+      cudaEventRecord(handle->ev_rest, cs) != cudaSuccess) {
+    cudaGetLastError();
+    return CURFP_STATUS_EXECUTION_FAILED;
+  }
+  if (!reset_info(handle)) return CURFP_STATUS_EXECUTION_FAILED;
+  rfp::CudaExecT<float> ex(handle, handle->d_info);
+  ex.rest_ready = handle->ev_rest;
+  const int rc = rfp::plan::spftrf(ex, transr == CURFP_OP_T,
+                                   uplo == CURFP_FILL_MODE_LOWER, n, arf, (int)math);
+  // Whatever the plan enqueued, nothing later on the handle's stream may run
+  // ahead of the copy.
+  if (cudaStreamWaitEvent(handle->stream, handle->ev_rest, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return CURFP_STATUS_EXECUTION_FAILED;
+  }
+  if (rc) return status_of(rc);
+  int h = 0, err = 0;
+  if (!read_info(handle, &h, &err)) return CURFP_STATUS_EXECUTION_FAILED;
+  if (err) return CURFP_STATUS_EXECUTION_FAILED;
+  *info = (h == INT_MAX) ? 0 : h;
+  return CURFP_STATUS_SUCCESS;
 }
 
 // src/curfp_spftrs.cpp:215-302

@@ -39,6 +39,8 @@ struct curfpContext {
   size_t tsv_bytes = 0;
   void* wsg = nullptr;     // adjoint scratch (solve adjoint n x 2nrhs, NLL gradient)
   size_t wsg_bytes = 0;
+  cudaStream_t copy_stream = nullptr;  // host-input factorization: the overlapped copy
+  cudaEvent_t ev_start = nullptr, ev_rest = nullptr;
 };
 
 namespace rfp {
@@ -68,6 +70,12 @@ class CudaExecT : public ExecT<T> {
                 int math) override;
   int trsm_wave(ViewT<T> L, int n, ViewT<T> B, int m, T alpha, const T* W) override;
   int potrf_adj_tile(ViewT<T> L, ViewT<T> G, int n) override;
+  // When set, work after the first diagonal block waits for this event.
+  int after_first_block() override {
+    if (!rest_ready) return 0;
+    return cudaStreamWaitEvent(ctx_->stream, rest_ready, 0) == cudaSuccess ? 0 : 4;
+  }
+  cudaEvent_t rest_ready = nullptr;
 
  protected:
   curfpContext* ctx_;

@@ -90,6 +90,10 @@ class ExecT {
   // Largest diagonal tile potrf_tile takes (a multiple of kPotrfTile); the
   // recursive Cholesky splits down to it.
   virtual int potrf_tile_rows() const { return kPotrfTile; }
+  // Called by the RFP factorization once the first diagonal block's work is
+  // enqueued and before any work that reads the other blocks: an executor
+  // may order that work after data it is still bringing in.
+  virtual int after_first_block() { return 0; }
   // Inverses of the diagonal nb x nb blocks of lower L (n x n): block b is
   // written to W + b*nb*nb, column-major with ld nb, zeros above the diagonal.
   // (W: nblk records of kInvStride floats, see kInvStride)

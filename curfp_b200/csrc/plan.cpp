@@ -234,6 +234,7 @@ int spftrf(ExecT<T>& ex, int transr, int lower, int n, T* A, int math) {
        V22 = block_view(A, g.b22);
   int rc = potrf_lower(ex, V11, g.n1, 0, math);
   if (rc) return rc;
+  if ((rc = ex.after_first_block())) return rc;
   if (g.n2 == 0) return 0;
   if (g.n1 > 0) {
     if ((rc = trsm_lln(ex, V11, g.n1, tr(V21), g.n2, 1.0f, math))) return rc;

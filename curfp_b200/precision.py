@@ -69,6 +69,39 @@ def spftrf(C: torch.Tensor, *, n: int = None, transr: str = "T", uplo: str = "U"
     return info.value
 
 
+def spftrf_from_host(C_host: torch.Tensor, C: torch.Tensor, C_orig: torch.Tensor = None, *,
+                     n: int = None, transr: str = "T", uplo: str = "U", check: bool = True,
+                     math: str = "bf16x3") -> int:
+    """Copy the host RFP array C_host (CPU float32, contiguous; pinned for the
+    copy to overlap) to the CUDA array C and factor it in place
+    (curfpSpftrfFromHost); C_orig, if given, receives the unfactored matrix.
+    For transr = T the copy of the array's second part overlaps the
+    factorization of the first diagonal block."""
+    if C_host.device.type != "cpu" or C_host.dtype != torch.float32 or not C_host.is_contiguous():
+        raise ValueError("C_host must be a contiguous float32 CPU tensor")
+    _validate(C, "C")
+    if C_orig is not None:
+        _validate(C_orig, "C_orig")
+        if C_orig.numel() != C.numel():
+            raise ValueError("C_orig must have as many elements as C")
+    if C_host.numel() != C.numel():
+        raise ValueError("C_host must have as many elements as C")
+    if n is None:
+        n = _n_from_rfp(C.numel())
+    h = _get_handle()
+    info = ctypes.c_int(0)
+    from ._lib import check as _check
+    _check(h._lib.curfpSpftrfFromHost(h.ptr, _op(transr), _fill(uplo), n,
+                                      ctypes.c_void_p(C_host.data_ptr()), _ptr(C),
+                                      _ptr(C_orig) if C_orig is not None else None,
+                                      ctypes.byref(info), _math(math)))
+    if check and info.value != 0:
+        raise torch.linalg.LinAlgError(
+            f"spftrf: matrix is not positive definite "
+            f"(leading minor of order {info.value} is not positive definite)")
+    return info.value
+
+
 def spftrs_refined(A: torch.Tensor, F: torch.Tensor, B: torch.Tensor, *, n: int = None,
                    nrhs: int = None, transr: str = "T", uplo: str = "U",
                    max_iter: int = 3) -> int:

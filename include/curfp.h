@@ -191,6 +191,21 @@ curfpStatus_t curfpSpftrfEx(curfpHandle_t handle, curfpOperation_t transr,
                             curfpFillMode_t uplo, int n, float *A, int *info,
                             curfpMath_t math);
 
+/* Factor an RFP matrix held in HOST memory: arf_host (n(n+1)/2 floats, page-
+ * locked for the copy to overlap) is copied to the device array arf, which is
+ * then factored in place as by curfpSpftrfEx.  If arf_orig is not NULL (it
+ * must not be arf), the unfactored matrix is also left there, as the
+ * refined solve (curfpSpftrsRefine) needs it; the host array crosses the
+ * bus once.  The part of the array the first diagonal block touches is
+ * copied first; the rest is copied on an internal stream and waited for only
+ * after that block is factored, so for TRANSR = T (where that block occupies
+ * its own half of the array) the transfer overlaps the factorization.
+ * Synchronises the handle's stream once to read info.  Not in the reference. */
+curfpStatus_t curfpSpftrfFromHost(curfpHandle_t handle, curfpOperation_t transr,
+                                  curfpFillMode_t uplo, int n, const float *arf_host,
+                                  float *arf, float *arf_orig, int *info,
+                                  curfpMath_t math);
+
 /* Solve A*X = B with iterative refinement: X0 = spftrs(factor, B), then
  * repeatedly R = B - A*X with the products of the ORIGINAL matrix Aorig (RFP,
  * same transr/uplo) summed in FP64, D = spftrs(factor, R), X += D, for at most
