@@ -175,6 +175,62 @@ __device__ __forceinline__ void stage_store(const Stage<T, R, BK>& st, T (*s)[R]
   }
 }
 
+// One operand's load groups for tiles whose k-tiles are all whole and in
+// bounds (no masks): the same groups as stage_load / stage_store, each with
+// a pointer that advances one k-tile per load and a fixed shared-memory
+// offset.  The four elements of a group share one swizzle (it depends on
+// kk >> 2 only), so a k-contiguous group's transposing stores are R apart.
+template <typename T, int R, int BK>
+struct Lane {
+  static constexpr int G = Stage<T, R, BK>::G;
+  static_assert(Stage<T, R, BK>::NG % kThreads == 0, "whole groups per thread");
+  const T* p[G];
+  int off[G];
+  int64_t step, unit;
+  bool kcont, vec;
+
+  __device__ __forceinline__ Lane(const T* base, int64_t sr, int64_t sk, int flags, int r0,
+                                  int k0) {
+    constexpr int KG = BK / 4;
+    kcont = flags & 1;
+    vec = flags & 2;
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+      const int e = threadIdx.x + kThreads * u;
+      int r, kk;
+      if (kcont) { r = e / KG; kk = (e % KG) << 2; }
+      else       { r = (e % (R / 4)) << 2; kk = e / (R / 4); }
+      p[u] = base + (int64_t)(r0 + r) * sr + (int64_t)(k0 + kk) * sk;
+      off[u] = kk * R + swz<BK>(r, kk);
+    }
+    step = (int64_t)BK * sk;
+    unit = kcont ? sk : sr;
+  }
+  __device__ __forceinline__ void load(Stage<T, R, BK>& st) {
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+      if (vec) {
+        ld4(p[u], st.v[u]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) st.v[u][c] = __ldg(p[u] + c * unit);
+      }
+      p[u] += step;
+    }
+  }
+  __device__ __forceinline__ void store(const Stage<T, R, BK>& st, T* s) const {
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+      if (kcont) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) s[off[u] + c * R] = st.v[u][c];
+      } else {
+        sts4(s + off[u], st.v[u]);
+      }
+    }
+  }
+};
+
 // k range [kb, ke) of a product that the triangular masks leave non-zero for
 // the tile at (m0, n0), rounded out to BK.
 template <int BK>
@@ -256,16 +312,9 @@ __global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 && BM >= 128) ? 1 : 
     stage_store<T, BN, BK>(rb, sb[buf], (f >> 2) & 1);
   };
 
-  if (ktiles > 0) {
-    load(0);
-    store(0, 0);
-    __syncthreads();
-  }
-#pragma unroll 1
-  for (int kt = 0; kt < ktiles; ++kt) {
-    const int buf = kt & 1;
-    const bool more = kt + 1 < ktiles;
-    if (more) load(kt + 1);  // global loads in flight during the FMAs
+  // The FMAs of one k-tile from shared buffer buf.  Both main loops below
+  // run this same sequence, so a tile's result does not depend on the loop.
+  auto fmas = [&](int buf) {
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
       T a[TM], b[TN];
@@ -293,8 +342,55 @@ __global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 && BM >= 128) ? 1 : 
 #pragma unroll
         for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
-    if (more) store(kt + 1, buf ^ 1);
-    __syncthreads();
+  };
+
+  // Interior tiles of single-product problems without triangular masks (the
+  // bulk of a large update): every k-tile is whole and in bounds, so each
+  // thread's load groups advance by a fixed pointer step and land at fixed
+  // shared-memory offsets, with no bounds or mask arithmetic per k-tile.
+  // The values loaded are the ones the general loop loads.
+  const bool whole = kt2 == 0 && P.a_tri == 0 && P.b_tri == 0 && m0 + BM <= P.m &&
+                     n0 + BN <= P.n && (ke1 - kb1) % BK == 0;
+  if (whole) {
+    Lane<T, BM, BK> la(P.A, P.a_rs, P.a_cs, fl & 3, m0, kb1);
+    Lane<T, BN, BK> lb(P.B, P.b_cs, P.b_rs, (fl >> 2) & 3, n0, kb1);
+    if (ktiles > 0) {
+      la.load(ra);
+      lb.load(rb);
+      la.store(ra, &sa[0][0][0]);
+      lb.store(rb, &sb[0][0][0]);
+      __syncthreads();
+    }
+#pragma unroll 1
+    for (int kt = 0; kt < ktiles; ++kt) {
+      const int buf = kt & 1;
+      const bool more = kt + 1 < ktiles;
+      if (more) {  // global loads in flight during the FMAs
+        la.load(ra);
+        lb.load(rb);
+      }
+      fmas(buf);
+      if (more) {
+        la.store(ra, &sa[buf ^ 1][0][0]);
+        lb.store(rb, &sb[buf ^ 1][0][0]);
+      }
+      __syncthreads();
+    }
+  } else {
+    if (ktiles > 0) {
+      load(0);
+      store(0, 0);
+      __syncthreads();
+    }
+#pragma unroll 1
+    for (int kt = 0; kt < ktiles; ++kt) {
+      const int buf = kt & 1;
+      const bool more = kt + 1 < ktiles;
+      if (more) load(kt + 1);  // global loads in flight during the FMAs
+      fmas(buf);
+      if (more) store(kt + 1, buf ^ 1);
+      __syncthreads();
+    }
   }
 
   // Epilogue.
